@@ -1,0 +1,58 @@
+"""Build recipe of libhp2d.so (sm_100a), in-tree next to this file.
+
+    python -m hydropol2d_b200.build
+
+nvcc cross-compiles without a GPU.  -fmad=false keeps every multiply and add separately
+rounded so the kernels reproduce the CPU restatement bit for bit.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+SRC = PKG / "csrc"
+LIB = PKG / "libhp2d.so"
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
+    "-Xcompiler", "-fPIC", "-shared",
+]
+
+
+def sources() -> list[Path]:
+    return sorted(SRC.glob("*.cu")) + sorted(SRC.glob("*.cuh")) + [ROOT / "include" / "hp2d.h"]
+
+
+def needs_build() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in sources())
+
+
+def nvcc() -> str:
+    cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    return cand if Path(cand).exists() else "nvcc"
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and not needs_build():
+        return LIB
+    cmd = [nvcc(), *NVCC_FLAGS, f"-I{ROOT / 'include'}", f"-I{SRC}",
+           str(SRC / "hp2d_capi.cu"), "-o", str(LIB)]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd[-1] = str(tmp)
+    subprocess.run(cmd, check=True)
+    tmp.replace(LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

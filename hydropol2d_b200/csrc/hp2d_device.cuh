@@ -1,0 +1,314 @@
+// Device-side arithmetic of the surface-flow step, shared by the fused and the unfused
+// kernels.  Every function here is the per-cell or per-face form of a reference line:
+//   face_flux      Local_Inertial_Model_D4.m:31-44, :89-142 (split slope), :198,
+//                  Inertial_Solver.m:24-25, LIM_D4.m:264, :272-275, :292-294
+//   donor_scale    apply_coarse_draining_limiter, LIM_D4.m:814-829
+//   limit_face     LIM_D4.m:831-857
+//   continuity     LIM_D4.m:313-315, :389-393, :415
+//   outlet_sink    LIM_D4.m:417-498
+//   green_ampt     HydroPol2D_Main_While_Ensemble.m:274-298 with Infiltration_Module.m
+//                  :179 and :444-445 (supply and depth update)
+//   cfl_cell       refreshing_timestep.m:61-89, :139-150, :181-238
+// The whole library is compiled with -fmad=false: every a*b+c below rounds twice, so the
+// results are reproducible on any IEEE machine that evaluates the same expressions.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hp2d {
+
+constexpr double kG = 9.81;
+
+// ---------------- x^(-1/3) by a fixed Newton iteration -------------------------------
+// Seed: dividing the IEEE exponent field by three (bits(x)/3 subtracted from the bits of
+// 2^(4/3 * bias)), then r <- r + r (1 - x r^3) / 3, quadratically convergent.
+template <typename R> struct RcbrtTraits;
+template <> struct RcbrtTraits<float> {
+    static constexpr int iters = 3;
+};
+template <> struct RcbrtTraits<double> {
+    static constexpr int iters = 5;
+};
+
+__device__ __forceinline__ float bits_seed(float x) {
+    uint32_t u = __float_as_uint(x);
+    return __uint_as_float(0x54AAAAABu - u / 3u);
+}
+__device__ __forceinline__ double bits_seed(double x) {
+    unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return __longlong_as_double((long long)(0x5540000000000000ull - u / 3ull));
+}
+__device__ __forceinline__ bool below_normal(float x) { return x < 1.17549435e-38f; }
+__device__ __forceinline__ bool below_normal(double x) { return x < 2.2250738585072014e-308; }
+template <typename R> __device__ __forceinline__ R sub_up();
+template <> __device__ __forceinline__ float sub_up<float>() { return 16777216.0f; }
+template <> __device__ __forceinline__ double sub_up<double>() { return 18014398509481984.0; }
+template <typename R> __device__ __forceinline__ R sub_down();
+template <> __device__ __forceinline__ float sub_down<float>() { return 256.0f; }
+template <> __device__ __forceinline__ double sub_down<double>() { return 262144.0; }
+
+template <typename R> __device__ __forceinline__ R rcbrt(R x) {
+    R scale = R(1);
+    if (below_normal(x)) { x = x * sub_up<R>(); scale = sub_down<R>(); }
+    R r = bits_seed(x);
+    const R third = R(1.0 / 3.0);
+#pragma unroll
+    for (int it = 0; it < RcbrtTraits<R>::iters; ++it) {
+        R t = x * r;
+        t = t * r;
+        t = t * r;
+        R e = R(1) - t;
+        r = r + (r * e) * third;
+    }
+    return r * scale;
+}
+template <typename R> __device__ __forceinline__ R pow73(R x) {
+    if (!(x > R(0))) return R(0);
+    R r = rcbrt(x);
+    R c = x * (r * r);
+    return (x * x) * c;
+}
+template <typename R> __device__ __forceinline__ R pow53(R x) {
+    if (!(x > R(0))) return R(0);
+    R r = rcbrt(x);
+    R c = x * (r * r);
+    return x * (c * c);
+}
+
+// ---------------- per-step constants (computed in FP64, rounded once) ------------------
+template <typename R> struct StepConsts {
+    R dt, gdt, dt_over_dx, dx_over_dt, inv_dt, inv_dx, rain_scale, g, tol, thr;
+    __device__ __host__ void make(double dt_s, double res, double tol_mm, double thr_mm) {
+        dt = R(dt_s);
+        gdt = R(kG * dt_s);
+        dt_over_dx = R(dt_s / res);
+        dx_over_dt = R(res / dt_s);
+        inv_dt = R(1.0 / dt_s);
+        inv_dx = R(1.0 / res);
+        rain_scale = R(dt_s / 3.6e6);
+        g = R(kG);
+        tol = R(tol_mm / 1000.0);
+        thr = R(thr_mm / 1000.0);
+    }
+};
+
+// ---------------- device state of the clock and of the step reductions ----------------
+struct StepScalars {
+    double t_min;          // clock at the start of the next step [min]
+    double time_step;      // step the next step applies [min]; dt = time_step*60 s
+                           // (Local_Inertial_Model_D4.m:201)
+    double tsp;            // running_control.time_save_previous [min]
+    long long k;           // step counter (1-based)
+    int cur;               // which of the double buffers holds the state
+    int skip_clamp;        // next step skips the 1e-6 mm clamp (Hydrological_Model.m:45-50)
+    double vmax_last;      // velocities.max_velocity of the last refresh
+    double rain_vol, inf_vol, out_vol;   // cumulative [m^3]
+    long long neg_warn, unstable;
+    unsigned int status;   // bit 0: non-finite depth seen
+    unsigned int counter;  // CTAs done with the current step
+    unsigned long long acc_vmax;   // max speed of the step (ordered bits)
+    unsigned long long acc_cmax;   // max wave celerity of non-stagnant cells (ordered bits)
+    double acc_rain, acc_inf, acc_out; // step sums [m] (times cell area later)
+    int acc_neg;           // unfused path: some depth < -1e-8 mm after hydrology
+    int pad;
+};
+
+// non-negative floats/doubles order like their bit patterns
+__device__ __forceinline__ unsigned long long ord_bits(float v) { return (unsigned long long)__float_as_uint(v); }
+__device__ __forceinline__ unsigned long long ord_bits(double v) { return (unsigned long long)__double_as_longlong(v); }
+__host__ __device__ inline double from_ord(unsigned long long b, bool is_double) {
+    if (is_double) {
+        double d;
+        memcpy(&d, &b, 8);
+        return d;
+    }
+    unsigned int u = (unsigned int)b;
+    float f;
+    memcpy(&f, &u, 4);
+    return (double)f;
+}
+
+// ---------------- Green-Ampt soil class table -----------------------------------------
+template <typename R> struct SoilClass {
+    R ks, psi, dth, lu, kout, tr, minsm, pad;
+};
+
+struct OutletList {
+    const int32_t* cell;     // sorted linear indices
+    int32_t n;
+};
+
+// ---------------- rain ---------------------------------------------------------------
+struct RainDesc {
+    int n_uniform;           // entries in the uniform table (0 = none)
+    const double* t_start;   // [min]
+    const double* rate;      // [mm/h]
+    int n_maps, my, mx;
+    double map_dt;           // [min]
+    const float* maps;       // n_maps * my * mx
+};
+
+__device__ __forceinline__ double uniform_rate(const RainDesc& rd, double t) {
+    int idx = -1;
+    for (int q = 0; q < rd.n_uniform; ++q)
+        if (rd.t_start[q] <= t) idx = q;
+    return idx < 0 ? 0.0 : rd.rate[idx];
+}
+__device__ __forceinline__ int map_index(const RainDesc& rd, double t) {
+    int m = (int)floor(t / rd.map_dt);
+    return max(0, min(m, rd.n_maps - 1));
+}
+template <typename R>
+__device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i, int j, int ny, int nx) {
+    const R half = R(0.5);
+    R fy = (R(i) + half) * R(double(rd.my) / ny) - half;
+    R fx = (R(j) + half) * R(double(rd.mx) / nx) - half;
+    fy = fmin(fmax(fy, R(0)), R(rd.my - 1));
+    fx = fmin(fmax(fx, R(0)), R(rd.mx - 1));
+    int iy0 = (int)floor(fy), ix0 = (int)floor(fx);
+    int iy1 = min(iy0 + 1, rd.my - 1), ix1 = min(ix0 + 1, rd.mx - 1);
+    R wy = fy - R(iy0), wx = fx - R(ix0);
+    R f00 = R(f[iy0 * rd.mx + ix0]), f01 = R(f[iy0 * rd.mx + ix1]);
+    R f10 = R(f[iy1 * rd.mx + ix0]), f11 = R(f[iy1 * rd.mx + ix1]);
+    R top = (R(1) - wx) * f00 + wx * f01;
+    R bot = (R(1) - wx) * f10 + wx * f11;
+    return (R(1) - wy) * top + wy * bot;
+}
+
+// ---------------- Green-Ampt (one cell) -----------------------------------------------
+// h [m] after rain; I [m]; T [s]; returns infiltrated depth [m]; updates h, I, T.
+template <typename R>
+__device__ __forceinline__ R green_ampt(R& hh, R& Ic, R& Tc, const SoilClass<R>& s, const StepConsts<R>& K) {
+    R Ip = Ic;
+    R C = s.ks * (R(1) + ((hh + s.psi) * s.dth) / Ip);
+    if (Ip > s.lu) C = s.ks;
+    R ia = hh * K.inv_dt;
+    bool idxC = ia <= C;
+    R Tn = Tc - K.dt;
+    if (ia > C) Tn = s.tr;
+    bool idxT = Tn < R(0);
+    R f = fmin(C, ia);
+    R In = Ip + f * K.dt;
+    if (idxC) In = In - s.kout * K.dt;
+    In = fmax(In, s.minsm);
+    if (idxT) In = s.minsm;
+    Ic = In;
+    Tc = Tn;
+    R fd = f * K.dt;
+    hh = hh - fd;
+    if (hh < R(0)) hh = R(0);
+    return fd;
+}
+
+// ---------------- one face of the local-inertial momentum update ----------------------
+// x face: (ha, hb) = (left, right) cells, dz = z_right - z_left.
+// y face: (ha, hb) = (upper, lower) cells (row i-1, row i), dz = z_upper - z_lower.
+// dz is NaN on closed faces (domain edge, idx_nan wall).
+template <typename R, bool IS_X>
+__device__ __forceinline__ void face_flux(R ha, R hb, R dz, R qp, R n2c, const StepConsts<R>& K,
+                                          int flag_critical, R& Hf, R& q) {
+    if (isnan(dz)) { Hf = R(0); q = R(0); return; }
+    ha = fmax(ha, R(0));
+    hb = fmax(hb, R(0));
+    R S;
+    if (IS_X) {
+        Hf = fmax(fmax(ha - fmax(dz, R(0)), hb + fmin(dz, R(0))), R(0));
+        S = (dz + (hb - ha)) * K.inv_dx;
+    } else {
+        Hf = fmax(fmax(ha + fmin(dz, R(0)), hb - fmax(dz, R(0))), R(0));
+        S = (dz + (ha - hb)) * K.inv_dx;
+    }
+    if (!(Hf > R(0))) { q = R(0); return; }
+    R num = qp - (K.gdt * Hf) * S;
+    R h73 = pow73(Hf);
+    R den = h73 + (K.gdt * n2c) * fabs(qp);
+    R qq = (num * h73) / den;
+    if (!isfinite(qq)) qq = R(0);
+    if (flag_critical == 1) {
+        R crit = Hf * sqrt(K.g * Hf);
+        qq = fmin(fmax(qq, -crit), crit);
+    }
+    R thr = Hf * R(10);
+    q = fmin(fmax(qq, -thr), thr);
+}
+
+// outgoing rate of a cell over its four faces and its donor scale factor
+template <typename R>
+__device__ __forceinline__ R donor_scale(R qR, R qL, R qU, R qD, R hc, const StepConsts<R>& K) {
+    R out = fmax(qR, R(0));
+    out = out + fmax(-qL, R(0));
+    out = out + fmax(qU, R(0));
+    out = out + fmax(-qD, R(0));
+    R avail = fmax(hc, R(0)) * K.dx_over_dt;
+    R s = R(1);
+    if (out > avail && out > R(0)) s = avail / out;
+    if (!isfinite(s)) s = R(0);
+    return fmax(fmin(s, R(1)), R(0));
+}
+
+// face limited by the scale of its donor cell; s_pos = donor when q > 0
+template <typename R>
+__device__ __forceinline__ R limit_face(R q, R s_pos, R s_neg) {
+    if (q > R(0)) q = q * s_pos;
+    else if (q < R(0)) q = q * s_neg;
+    if (!isfinite(q)) q = R(0);
+    return q;
+}
+
+template <typename R>
+__device__ __forceinline__ R continuity(R htot, R qL, R qR, R qU, R qD, const StepConsts<R>& K) {
+    R hn = htot + K.dt_over_dx * (((qL - qR) - qU) + qD);
+    if (hn < R(0)) hn = R(0);
+    return hn;
+}
+
+// outlet sink; coef = sqrt|S|/(n dx) (type 1) or sqrt(g)/dx (type 2)
+template <typename R>
+__device__ __forceinline__ R outlet_sink(R& hn, R coef, int outlet_type, const StepConsts<R>& K, R& hout) {
+    hout = fmax(hn, R(0));
+    R qq = outlet_type == 1 ? coef * pow53(hout) : coef * (hout * sqrt(hout));
+    R qmax = hout * K.inv_dt;
+    qq = fmin(qq, qmax);
+    if (!isfinite(qq)) qq = R(0);
+    hn = hn - qq * K.dt;
+    return qq;
+}
+
+// CFL contribution of one cell: speed and (if not stagnant) wave celerity
+template <typename R>
+__device__ __forceinline__ void cfl_cell(R qx, R qy, R qyb, R hfx, R hfy, R hfyb, R hf3, bool first_col,
+                                         int adaptive, const StepConsts<R>& K, R& speed, R& celer) {
+    const R big = R(1e9);
+    R sx = hfx < K.tol ? big : hfx;
+    R sy = hfy < K.tol ? big : hfy;
+    R sb = hfyb < K.tol ? big : hfyb;
+    R vr = qx / sx;
+    R vu = qy / sy;
+    R vb = qyb / sb;
+    R rc = first_col ? R(0.5) * vr : vr;
+    R uc = R(0.5) * (vu + vb);
+    speed = sqrt(rc * rc + uc * uc);
+    celer = R(0);
+    if (speed >= R(0.01)) {
+        R dts = fmax(fmax(hfx, hfy), hf3);
+        R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
+        if (adaptive != 1) wc = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
+        celer = wc;
+    }
+}
+
+// binary search of a sorted outlet list; returns ordinal or -1
+__device__ __forceinline__ int find_outlet(const int32_t* cells, int n, int c) {
+    int lo = 0, hi = n - 1;
+    while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        int v = __ldg(cells + mid);
+        if (v == c) return mid;
+        if (v < c) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    return -1;
+}
+
+}  // namespace hp2d

@@ -1,0 +1,170 @@
+"""Host-side handle of one resident grid: a thin Python layer over the C ABI.
+
+Arrays cross as numpy (host) buffers; units are the reference's (mm, mm/h, min, m).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a, shape=None) -> np.ndarray:
+    out = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None and out.shape != shape:
+        out = np.ascontiguousarray(np.broadcast_to(out, shape), dtype=np.float64)
+    return out
+
+
+class SurfaceFlow:
+    """One hp2d_ctx.  ``precision`` is "fp32" or "fp64"."""
+
+    def __init__(self, ny: int, nx: int, resolution: float, precision: str = "fp32",
+                 params: _abi.Params | None = None, device: int = 0, **param_kw):
+        self._L = _abi.lib()
+        self.ny, self.nx = int(ny), int(nx)
+        self.resolution = float(resolution)
+        self.precision = precision
+        self.dtype = np.float32 if precision == "fp32" else np.float64
+        prec = _abi.HP2D_FP32 if precision == "fp32" else _abi.HP2D_FP64
+        self.params = params if params is not None else _abi.default_params(**param_kw)
+        g = _abi.Grid(self.ny, self.nx, self.resolution, prec)
+        h = C.c_void_p()
+        st = self._L.hp2d_create(C.byref(g), C.byref(self.params), int(device), C.byref(h))
+        if st != 0:
+            raise _abi.HP2DError(st, self._L.hp2d_create_error().decode())
+        self._h = h
+        self.n_outlets = 0
+
+    # ---------------------------------------------------------------- plumbing
+    def _check(self, st: int):
+        if st != 0:
+            raise _abi.HP2DError(st, self._L.hp2d_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hp2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---------------------------------------------------------------- inputs
+    def upload_static(self, z, roughness, outlet_rows, outlet_cols, slope_per_outlet=None):
+        shp = (self.ny, self.nx)
+        z = _f64(z, shp)
+        n = _f64(roughness, shp)
+        rows = np.ascontiguousarray(outlet_rows, dtype=np.int32).ravel()
+        cols = np.ascontiguousarray(outlet_cols, dtype=np.int32).ravel()
+        sl = None if slope_per_outlet is None else _f64(slope_per_outlet).ravel()
+        self._check(self._L.hp2d_upload_static(
+            self._h, _dp(z), _dp(n), rows.ctypes.data_as(C.POINTER(C.c_int32)),
+            cols.ctypes.data_as(C.POINTER(C.c_int32)), int(rows.size),
+            None if sl is None else _dp(sl)))
+        self.n_outlets = len(set(zip(rows.tolist(), cols.tolist())))
+
+    def set_soil(self, soil_class, ksat, psi, dtheta, Lu, k_out, Tr, min_soil_moisture):
+        cls = np.ascontiguousarray(soil_class, dtype=np.uint8).reshape(self.ny, self.nx)
+        tabs = [_f64(v).ravel() for v in (ksat, psi, dtheta, Lu, k_out, Tr, min_soil_moisture)]
+        ncls = tabs[0].size
+        if any(t.size != ncls for t in tabs):
+            raise ValueError("soil tables must have one entry per class")
+        self._check(self._L.hp2d_set_soil(self._h, cls.ctypes.data_as(C.POINTER(C.c_uint8)), ncls,
+                                          *[_dp(t) for t in tabs]))
+
+    def set_state(self, d, outflow=None, soil_storage=None):
+        shp = (self.ny, self.nx)
+        d = _f64(d, shp)
+        of = None
+        if outflow is not None:
+            of = np.asarray(outflow, dtype=np.float64)
+            of = np.ascontiguousarray(of[:2] if of.shape[0] >= 2 else of)
+            if of.shape != (2, self.ny, self.nx):
+                raise ValueError("outflow must be (2 or 3, ny, nx) pages [mm/h]")
+        I = None if soil_storage is None else _f64(soil_storage, shp)
+        self._check(self._L.hp2d_set_state(self._h, _dp(d), None if of is None else _dp(of),
+                                           None if I is None else _dp(I)))
+
+    def set_clock(self, t: float, time_step: float, k: int = 1):
+        self._check(self._L.hp2d_set_clock(self._h, float(t), float(time_step), int(k)))
+
+    def set_rain_uniform(self, t_start, rate):
+        t = _f64(t_start).ravel()
+        r = _f64(rate).ravel()
+        self._check(self._L.hp2d_set_rain_uniform(self._h, int(t.size), _dp(t), _dp(r)))
+
+    def set_rain_maps(self, maps, map_dt: float):
+        m = np.ascontiguousarray(maps, dtype=np.float32)
+        nm, my, mx = m.shape
+        self._check(self._L.hp2d_set_rain_maps(self._h, nm, my, mx,
+                                               m.ctypes.data_as(C.POINTER(C.c_float)), float(map_dt)))
+
+    # ---------------------------------------------------------------- stages
+    def hydrology_step(self, time_step: float):
+        self._check(self._L.hp2d_hydrology_step(self._h, float(time_step)))
+
+    def li_step(self, time_step: float):
+        self._check(self._L.hp2d_li_step(self._h, float(time_step)))
+
+    def cfl_dt(self):
+        ts = C.c_double()
+        vm = C.c_double()
+        self._check(self._L.hp2d_cfl_dt(self._h, C.byref(ts), C.byref(vm)))
+        return ts.value, vm.value
+
+    def track_maxima(self, t_end: float):
+        self._check(self._L.hp2d_track_maxima(self._h, float(t_end)))
+
+    def fused_steps(self, n: int):
+        self._check(self._L.hp2d_fused_steps(self._h, int(n)))
+
+    def fused_steps_timed(self, n: int) -> float:
+        """Runs n fused steps; returns their device time [ms] (CUDA events on the
+        library's stream)."""
+        ms = C.c_float()
+        self._check(self._L.hp2d_fused_steps_timed(self._h, int(n), C.byref(ms)))
+        return ms.value
+
+    def run(self, max_steps: int = 0) -> int:
+        done = C.c_int64()
+        self._check(self._L.hp2d_run(self._h, int(max_steps), C.byref(done)))
+        return done.value
+
+    # ---------------------------------------------------------------- outputs
+    def download(self, field: str) -> np.ndarray:
+        out = np.empty((self.ny, self.nx), dtype=np.float64)
+        self._check(self._L.hp2d_download(self._h, _abi.FIELD[field], _dp(out), out.size))
+        return out
+
+    def download_native(self, field: str) -> np.ndarray:
+        per_outlet = field in ("hf3", "qo")
+        shape = (self.n_outlets,) if per_outlet else (self.ny, self.nx)
+        out = np.empty(shape, dtype=self.dtype)
+        self._check(self._L.hp2d_download_native(self._h, _abi.NATIVE[field],
+                                                 out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def diag(self) -> dict:
+        d = _abi.Diag()
+        self._check(self._L.hp2d_get_diag(self._h, C.byref(d)))
+        return {k: getattr(d, k) for k, _ in _abi.Diag._fields_}
+
+    def stored_volume(self) -> float:
+        v = C.c_double()
+        self._check(self._L.hp2d_stored_volume(self._h, C.byref(v)))
+        return v.value

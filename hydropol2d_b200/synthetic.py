@@ -1,0 +1,178 @@
+"""Seeded synthetic inputs of the benchmark configurations (no public dataset is involved).
+
+* ``vtilt_case``    200 x 200, dx 10 m V-tilted catchment (two planes sloping 0.005 to a
+                    channel sloping 0.002), n = 0.02, 100 mm/h for 30 min, 60 min, alpha 0.7.
+                    Geometry follows Validation/Phase1_VTilted_Catchment/
+                    generate_phase1_vtilted_domain.py:87-91.
+* ``urban_case``    2048 x 2048, dx 2 m Gaussian random field (power spectrum k^-3, 40 m
+                    relief) + rectangular buildings (+10 m, 30 % of cells); Voronoi LULC
+                    (n in {0.013, 0.03, 0.05, 0.1}) and soil (Green-Ampt classes); 64 x 64
+                    rain field U(0, 120) mm/h redrawn every 5 min; 2 h.
+* ``dambreak_case`` 4096 x 8192 (ny x nx), dx 5 m fractal valley: parabolic cross-section
+                    60 m deep + GRF of 5 m std; reservoir 30 m deep behind a wall over the
+                    upstream 5 % (removed at t = 0); n = 0.035; 3 h.
+
+All fields are float64 numpy arrays in the reference's units (m, mm, mm/h); the same
+arrays feed the GPU library and the CPU restatements.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Case:
+    name: str
+    z: np.ndarray
+    roughness: np.ndarray
+    resolution: float
+    outlet_rows: np.ndarray
+    outlet_cols: np.ndarray
+    params: dict
+    d0: np.ndarray
+    rain_uniform: tuple | None = None       # (t_start [min], rate [mm/h])
+    rain_maps: np.ndarray | None = None     # (n, my, mx) float32 [mm/h]
+    rain_map_dt: float = 5.0
+    soil: dict | None = None                # set_soil kwargs
+    I0: np.ndarray | None = None            # mm
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def shape(self):
+        return self.z.shape
+
+    def apply(self, sf):
+        """Upload the case into a SurfaceFlow (or an oracle with the same surface)."""
+        sf.upload_static(self.z, self.roughness, self.outlet_rows, self.outlet_cols)
+        if self.soil is not None:
+            sf.set_soil(**self.soil)
+        sf.set_state(self.d0, None, self.I0)
+        if self.rain_uniform is not None:
+            sf.set_rain_uniform(*self.rain_uniform)
+        if self.rain_maps is not None:
+            sf.set_rain_maps(self.rain_maps, self.rain_map_dt)
+        return sf
+
+
+def gaussian_random_field(ny: int, nx: int, slope: float = -3.0, seed: int = 0) -> np.ndarray:
+    """Zero-mean, unit-std field with isotropic power spectrum P(k) ~ k^slope (FFT method)."""
+    rng = np.random.default_rng(seed)
+    noise = rng.standard_normal((ny, nx))
+    ky = np.fft.fftfreq(ny)[:, None]
+    kx = np.fft.rfftfreq(nx)[None, :]
+    k = np.sqrt(kx * kx + ky * ky)
+    k[0, 0] = np.inf
+    amp = k ** (slope / 2.0)
+    f = np.fft.irfft2(np.fft.rfft2(noise) * amp, s=(ny, nx))
+    f -= f.mean()
+    f /= f.std()
+    return f
+
+
+def voronoi_classes(ny: int, nx: int, n_seeds: int, n_classes: int, seed: int) -> np.ndarray:
+    """Class map from a Voronoi partition of seeded random sites (nearest site wins)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    sites = rng.uniform([0, 0], [ny, nx], size=(n_seeds, 2))
+    site_class = rng.integers(0, n_classes, size=n_seeds)
+    tree = cKDTree(sites)
+    out = np.empty((ny, nx), dtype=np.uint8)
+    cols = np.arange(nx) + 0.5
+    for r0 in range(0, ny, 256):
+        rr = np.arange(r0, min(ny, r0 + 256)) + 0.5
+        pts = np.stack(np.meshgrid(rr, cols, indexing="ij"), axis=-1).reshape(-1, 2)
+        _, idx = tree.query(pts)
+        out[r0:r0 + len(rr)] = site_class[idx].reshape(len(rr), nx)
+    return out
+
+
+def green_ampt_soil_tables(ksat_mmh, psi_mm, dtheta, theta_sat=0.45, theta_r=0.05, kr=0.0):
+    """Per-class Green-Ampt tables with the reference's derived parameters
+    (HydroPol2D_preprocessing.m:2250-2253: Tr = 4.5/sqrt(ksat/25.4) h,
+    Lu = 4 sqrt(ksat/25.4) in, k_out = (theta_sat - theta_r) kr Lu 1000 mm/h;
+    min_soil_moisture = eps mm, :2387-2388)."""
+    ksat = np.asarray(ksat_mmh, dtype=np.float64)
+    Tr = 4.5 / np.sqrt(ksat / 25.4)
+    Lu = 4.0 * np.sqrt(ksat / 25.4) * 2.54 / 100.0
+    k_out = (theta_sat - theta_r) * kr * Lu * 1000.0
+    return dict(ksat=ksat, psi=np.asarray(psi_mm, dtype=np.float64),
+                dtheta=np.asarray(dtheta, dtype=np.float64), Lu=Lu, k_out=k_out, Tr=Tr,
+                min_soil_moisture=np.full(ksat.shape, np.finfo(np.float64).eps))
+
+
+def vtilt_domain(ny: int, nx: int, dx: float, side_slope: float, long_slope: float,
+                 z_outlet: float = 100.0, channel_cols: int = 2):
+    """V-tilted DEM: rows run downstream toward row 0; the channel is the central
+    ``channel_cols`` columns; planes slope toward it (generate_phase1_vtilted_domain.py:87-91)."""
+    left = (nx - channel_cols) // 2
+    x = np.arange(nx, dtype=np.float64) * dx
+    y = np.arange(ny, dtype=np.float64) * dx
+    x_left_end = left * dx
+    x_channel_end = (left + channel_cols - 1) * dx
+    base = z_outlet + long_slope * y[:, None] + 0.0 * x[None, :]
+    z = base.copy()
+    lm = x[None, :] < x_left_end
+    rm = x[None, :] > x_channel_end
+    z = np.where(lm, base + side_slope * (x_left_end - x[None, :]), z)
+    z = np.where(rm, base + side_slope * (x[None, :] - x_channel_end), z)
+    ch = np.arange(left, left + channel_cols)
+    return z, ch
+
+
+def vtilt_case(ny: int = 200, nx: int = 200, dx: float = 10.0) -> Case:
+    z, ch = vtilt_domain(ny, nx, dx, 0.005, 0.002)
+    rows = np.zeros(ch.size, dtype=np.int32)
+    params = dict(routing_time=60.0, alfa_min=0.7, alfa_max=0.7, outlet_type=1, slope_outlet=0.002,
+                  min_time_step=0.01, max_time_step=10.0)
+    return Case("vtilt_200x200_dx10", z, np.full((ny, nx), 0.02), dx, rows, ch.astype(np.int32), params,
+                np.zeros((ny, nx)), rain_uniform=(np.array([0.0, 30.0]), np.array([100.0, 0.0])))
+
+
+def urban_case(n: int = 2048, dx: float = 2.0, seed: int = 7, hours: float = 2.0) -> Case:
+    rng = np.random.default_rng(seed)
+    grf = gaussian_random_field(n, n, -3.0, seed)
+    z = (grf - grf.min()) / (grf.max() - grf.min()) * 40.0
+    bld = np.zeros((n, n), dtype=bool)
+    target = 0.30 * n * n
+    while bld.sum() < target:
+        h, w = rng.integers(4, 24, size=2)
+        r, c = rng.integers(0, n - h), rng.integers(0, n - w)
+        bld[r:r + h, c:c + w] = True
+    z = z + 10.0 * bld
+    lulc = voronoi_classes(n, n, 400, 4, seed + 1)
+    nvals = np.array([0.013, 0.03, 0.05, 0.1])
+    rough = nvals[lulc]
+    soil = voronoi_classes(n, n, 300, 3, seed + 2)
+    tabs = green_ampt_soil_tables([1.0, 10.0, 30.0], [50.0, 110.0, 200.0], [0.2, 0.3, 0.4])
+    n_maps = int(np.ceil(hours * 60 / 5.0)) + 1
+    maps = rng.uniform(0.0, 120.0, size=(n_maps, 64, 64)).astype(np.float32)
+    edge_r = np.concatenate([np.zeros(n), np.full(n, n - 1), np.arange(1, n - 1), np.arange(1, n - 1)])
+    edge_c = np.concatenate([np.arange(n), np.arange(n), np.zeros(n - 2), np.full(n - 2, n - 1)])
+    params = dict(routing_time=hours * 60.0, alfa_min=0.5, alfa_max=0.7, outlet_type=2,
+                  flag_infiltration=1, min_time_step=0.01, max_time_step=10.0)
+    return Case(f"urban_{n}x{n}_dx{dx:g}", z, rough, dx, edge_r.astype(np.int32), edge_c.astype(np.int32),
+                params, np.zeros((n, n)), rain_maps=maps, rain_map_dt=5.0,
+                soil=dict(soil_class=soil, **tabs), I0=np.full((n, n), 5.0),
+                meta=dict(buildings=float(bld.mean())))
+
+
+def dambreak_case(ny: int = 4096, nx: int = 8192, dx: float = 5.0, seed: int = 11, hours: float = 3.0,
+                  long_slope: float = 0.001) -> Case:
+    """Valley along x (columns); reservoir over the first 5 % of columns."""
+    grf = gaussian_random_field(ny, nx, -3.0, seed) * 5.0
+    y = (np.arange(ny) + 0.5) / ny * 2.0 - 1.0
+    x = np.arange(nx) * dx
+    z = 60.0 * (y[:, None] ** 2) + long_slope * (x[-1] - x)[None, :] + grf + 20.0
+    x_dam = int(round(0.05 * nx))
+    thalweg = float(np.min(z[:, x_dam]))
+    wse = thalweg + 30.0
+    d0 = np.zeros((ny, nx))
+    d0[:, :x_dam] = np.maximum(wse - z[:, :x_dam], 0.0) * 1000.0
+    rows = np.arange(ny, dtype=np.int32)
+    cols = np.full(ny, nx - 1, dtype=np.int32)
+    params = dict(routing_time=hours * 60.0, alfa_min=0.5, alfa_max=0.7, outlet_type=1,
+                  slope_outlet=long_slope, min_time_step=0.01, max_time_step=10.0)
+    return Case(f"dambreak_{ny}x{nx}_dx{dx:g}", z, np.full((ny, nx), 0.035), dx, rows, cols, params, d0,
+                meta=dict(x_dam=x_dam, wse=wse))

@@ -1,0 +1,202 @@
+/*
+ * hp2d.h -- C ABI of the B200 surface-flow step for HydroPol2D.
+ *
+ * One context (hp2d_ctx) holds one grid resident in GPU memory.  The entry points
+ * replace, one for one, the MATLAB functions and scripts that HydroPol2D_Main_While
+ * calls on its surface-flow path:
+ *
+ *   hp2d_hydrology_step  rain (interception_module.m:68-71, Snow_Module.m:99), the
+ *                        Infiltration_Module script (Green-Ampt form, see below) and
+ *                        the depth clamp of Hydrological_Model.m:45-55
+ *   hp2d_li_step         Local_Inertial_Model_D4.m:1-5 (+ Inertial_Solver.m:1, scheme 1)
+ *   hp2d_cfl_dt          refreshing_timestep.m:17-359 (inertial, D4)
+ *   hp2d_track_maxima    save_output_maps.m:588-600 (running maximum depth) + arrival time
+ *   hp2d_fused_steps     all of the above, one fused kernel per accepted step, in the
+ *                        order of HydroPol2D_Main_While.m:403-782
+ *
+ * Conventions at this boundary (the MATLAB units): depths in mm, face fluxes in mm/h
+ * referenced to the cell area, time steps in minutes, the clock in minutes, elevations
+ * in m.  Arrays are row-major with x (MATLAB's column index) fastest: element (i, j) of a
+ * MATLAB ny-by-nx array is at i*nx + j.  A MEX gateway transposes column-major data on
+ * the way in and out.  Inside, the state is SI (m, m^2/s, s).
+ *
+ * Every call returns an hp2d_status; on failure hp2d_last_error() gives a message.
+ * Host pointers are borrowed for the duration of the call only.  Calls on one context
+ * are synchronous with respect to the host and must come from one host thread at a time.
+ */
+#ifndef HP2D_H
+#define HP2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hp2d_status {
+    HP2D_OK = 0,
+    HP2D_INVALID_ARG = 1,
+    HP2D_UNSUPPORTED_FLAG = 2,   /* flag_subgrid/flag_D8/flag_reservoir=1, scheme 2/3 ... */
+    HP2D_CUDA_ERROR = 3,
+    HP2D_NUMERICAL = 4,          /* NaN/Inf in the state */
+    HP2D_DT_FLOOR = 5,           /* dt hit min_time_step (refreshing_timestep.m:357-359) */
+    HP2D_TIMEOUT = 6,
+    HP2D_NO_DEVICE = 7,
+    HP2D_NOT_READY = 8           /* static data or state not uploaded yet */
+} hp2d_status;
+
+typedef enum hp2d_precision { HP2D_FP32 = 0, HP2D_FP64 = 1 } hp2d_precision;
+
+typedef struct hp2d_grid {
+    int32_t ny;            /* rows    (MATLAB size(z,1)) */
+    int32_t nx;            /* columns (MATLAB size(z,2)) */
+    double resolution;     /* Wshed_Properties.Resolution [m]; cell_area = resolution^2 */
+    int32_t precision;     /* hp2d_precision of the state and of the per-cell arithmetic */
+} hp2d_grid;
+
+/* Flags and controls the path reads (Config/input_data_bypass_script.m:160-170, :330-380,
+ * input_data_script.m:92-154).  Unsupported values are rejected, never ignored. */
+typedef struct hp2d_params {
+    int32_t flag_numerical_scheme;      /* 1 (Bates); 2 and 3 -> HP2D_UNSUPPORTED_FLAG */
+    int32_t flag_critical;              /* 0/1: critical-velocity clip (LIM_D4.m:272-275) */
+    int32_t flag_subgrid;               /* must be 0 */
+    int32_t flag_D8;                    /* must be 0 */
+    int32_t flag_reservoir;             /* must be 0 */
+    int32_t flag_infiltration;          /* 0 off, 1 Green-Ampt (hp2d_set_soil) */
+    int32_t flag_timestep;              /* 1: dt = min(dt_adv, dt_wave); 0: dt_wave */
+    int32_t flag_adaptive_timestepping; /* 1: wave celerity only; 0: celerity + speed */
+    int32_t outlet_type;                /* 1 normal-depth slope, 2 critical */
+    double slope_outlet;                /* [m/m], outlet_type 1 */
+    double min_time_step;               /* running_control.min_time_step [s] */
+    double max_time_step;               /* running_control.max_time_step [s] */
+    double time_step_increments;        /* [s] */
+    double time_step_change;            /* [s] refresh gate of HydroPol2D_Main_While.m:691-695 */
+    double routing_time;                /* [min] end of the simulation */
+    double alfa_min;                    /* Courant_Parameters.alfa_min */
+    double alfa_max;                    /* Courant_Parameters.alfa_max */
+    double depth_tolerance;             /* CA_States.depth_tolerance [mm] */
+    double arrival_threshold;           /* depth defining the arrival time [mm] */
+} hp2d_params;
+
+/* Fields for hp2d_download.  Units are the MATLAB ones. */
+typedef enum hp2d_field {
+    HP2D_FIELD_DEPTH = 0,        /* depths.d_t [mm] */
+    HP2D_FIELD_QOUT_RIGHT = 1,   /* flow_rate.qout_right_t = outflow_bates(:,:,1) [mm/h] */
+    HP2D_FIELD_QOUT_UP = 2,      /* flow_rate.qout_up_t    = outflow_bates(:,:,2) [mm/h] */
+    HP2D_FIELD_QOUT_LEFT = 3,    /* flow_rate.qout_left_t  [mm/h] (LIM_D4.m:347) */
+    HP2D_FIELD_QOUT_DOWN = 4,    /* flow_rate.qout_down_t  [mm/h] (LIM_D4.m:350) */
+    HP2D_FIELD_OUTLET_FLOW = 5,  /* outlet_states.outlet_flow = outflow_bates(:,:,3) [mm/h] */
+    HP2D_FIELD_HF_X = 6,         /* Hf(:,:,1) [m] of the last li step */
+    HP2D_FIELD_HF_Y = 7,         /* Hf(:,:,2) [m] */
+    HP2D_FIELD_HF_OUTLET = 8,    /* Hf(:,:,3) [m] */
+    HP2D_FIELD_DMAX = 9,         /* depths.dmax_final [mm] */
+    HP2D_FIELD_ARRIVAL = 10,     /* first time depth >= arrival_threshold [min]; +Inf never */
+    HP2D_FIELD_SOIL_STORAGE = 11,/* Soil_Properties.I_t [mm] */
+    HP2D_FIELD_I_TOT_END_CELL = 12 /* CA_States.I_tot_end_cell [m^3] (LIM_D4.m:512-514) */
+} hp2d_field;
+
+typedef struct hp2d_diag {
+    double t;                     /* clock [min] */
+    double time_step;             /* step the next call applies [min] */
+    int64_t k;                    /* step counter (1-based, as the reference) */
+    double max_velocity;          /* velocities.max_velocity of the last refresh [m/s] */
+    double rain_volume;           /* cumulative [m^3] */
+    double infiltration_volume;   /* cumulative [m^3] */
+    double outlet_volume;         /* cumulative [m^3] */
+    int64_t neg_depth_warnings;   /* Hydrological_Model.m:45-47 events */
+    int64_t unstable_steps;       /* refreshing_timestep.m:357-359 events */
+    int64_t status_bits;          /* bit 0: non-finite state seen */
+} hp2d_diag;
+
+typedef struct hp2d_ctx hp2d_ctx;
+
+/* ---- lifetime --------------------------------------------------------------------- */
+/* Creates a context on CUDA device `device`.  Replaces the gpuArray set-up of
+ * HydroPol2D_preprocessing.m:2754-2771 for the arrays of this path. */
+hp2d_status hp2d_create(const hp2d_grid* grid, const hp2d_params* params, int32_t device,
+                        hp2d_ctx** out);
+hp2d_status hp2d_destroy(hp2d_ctx* ctx);
+const char* hp2d_last_error(const hp2d_ctx* ctx);
+/* Library-wide message of the last failed hp2d_create (no context exists then). */
+const char* hp2d_create_error(void);
+
+/* ---- inputs ----------------------------------------------------------------------- */
+/* Elevation_Properties.elevation_cell [m] (NaN = idx_nan cell, a wall),
+ * LULC_Properties.roughness (roughness_squared = roughness.^2, Main_While.m:188),
+ * Wshed_Properties.row_outlet/col_outlet (0-based) and, optionally, one slope per outlet
+ * cell (slope_outlet given as a map); NULL uses params.slope_outlet. */
+hp2d_status hp2d_upload_static(hp2d_ctx* ctx, const double* z, const double* roughness,
+                               const int32_t* outlet_rows, const int32_t* outlet_cols,
+                               int32_t n_outlets, const double* slope_outlet_per_outlet);
+
+/* Green-Ampt soil classes: class map (255 = no soil: impervious, no infiltration) and
+ * per-class tables.  ksat [mm/h], psi [mm], dtheta = teta_sat - teta_i [-], Lu [m],
+ * k_out [mm/h], Tr [h] and min_soil_moisture [mm] as HydroPol2D_preprocessing.m:2250-2253
+ * and :2387-2388 define them. */
+hp2d_status hp2d_set_soil(hp2d_ctx* ctx, const uint8_t* soil_class, int32_t n_classes,
+                          const double* ksat, const double* psi, const double* dtheta,
+                          const double* Lu, const double* k_out, const double* Tr,
+                          const double* min_soil_moisture);
+
+/* State: depths.d_t [mm]; outflow_bates pages 1-2 [mm/h] (two ny*nx blocks, right then
+ * up; NULL = zeros); Soil_Properties.I_t [mm] (NULL = keep).  Resets dmax and arrival. */
+hp2d_status hp2d_set_state(hp2d_ctx* ctx, const double* d, const double* outflow,
+                           const double* soil_storage);
+
+/* Clock [min], the step the next call applies [min] and the step counter k (1-based). */
+hp2d_status hp2d_set_clock(hp2d_ctx* ctx, double t, double time_step, int64_t k);
+
+/* Rain forcing.  Uniform: piecewise-constant rates [mm/h] starting at t_start [min].
+ * Maps: n_maps coarse fields (my x mx, row-major) [mm/h], map m active for
+ * t in [m*map_dt, (m+1)*map_dt) [min], bilinearly interpolated to the grid. */
+hp2d_status hp2d_set_rain_uniform(hp2d_ctx* ctx, int32_t n, const double* t_start,
+                                  const double* rate);
+hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx,
+                               const float* rate, double map_dt);
+
+/* ---- unfused drop-in entry points (one reference function each) ------------------ */
+/* Hydrological_Model for this path: adds delta_p_agg = rate(t) * time_step/60 mm,
+ * runs the Infiltration_Module (Green-Ampt when flag_infiltration=1) and the clamp; the
+ * resident depth becomes d_tot. */
+hp2d_status hp2d_hydrology_step(hp2d_ctx* ctx, double time_step);
+/* Local_Inertial_Model_D4 on the resident d_tot and outflow_prev with time_step [min];
+ * the resident depth becomes d_t and the resident fluxes outflow_bates. */
+hp2d_status hp2d_li_step(hp2d_ctx* ctx, double time_step);
+/* refreshing_timestep's refresh branch on the last li step's Hf and fluxes: returns the
+ * new time_step [min] (= time_calculation_routing/60) and the maximum velocity [m/s]. */
+hp2d_status hp2d_cfl_dt(hp2d_ctx* ctx, double* time_step, double* max_velocity);
+/* save_output_maps' running maximum depth, and the arrival time t_end [min] for cells
+ * whose depth first reaches params.arrival_threshold. */
+hp2d_status hp2d_track_maxima(hp2d_ctx* ctx, double t_end);
+
+/* ---- fused path ------------------------------------------------------------------ */
+/* Runs `nsteps` accepted steps of HydroPol2D_Main_While.m:403-782 (hydrology, routing,
+ * timestep refresh, maxima, clock), one fused kernel per step, launched from a CUDA
+ * graph.  Steps after the clock passes routing_time are no-ops. */
+hp2d_status hp2d_fused_steps(hp2d_ctx* ctx, int32_t nsteps);
+/* hp2d_fused_steps bracketed by CUDA events on the context's stream; *elapsed_ms is the
+ * device time of the nsteps launches (for benchmarking). */
+hp2d_status hp2d_fused_steps_timed(hp2d_ctx* ctx, int32_t nsteps, float* elapsed_ms);
+/* Runs until the clock passes routing_time (or max_steps); returns steps executed. */
+hp2d_status hp2d_run(hp2d_ctx* ctx, int64_t max_steps, int64_t* steps_done);
+
+/* ---- outputs ---------------------------------------------------------------------- */
+hp2d_status hp2d_download(hp2d_ctx* ctx, int32_t field, double* host, size_t count);
+/* Raw copy of an internal array in the context's precision and SI units, for callers
+ * that keep the state in their own units (and for bit-level regression checks):
+ *   0 depth [m], 1 right-face discharge per width [m^2/s], 2 upper-face discharge
+ *   [m^2/s], 3 soil storage [m], 4 recovery timer [s], 5 dmax [m], 6 arrival [s],
+ *   7 Hf x [m], 8 Hf y [m] (after hp2d_li_step), 9 Hf at outlets [m] and 10 outlet
+ *   sink rate [m/s] (one value per outlet cell, in increasing linear-index order).
+ * `bytes` must equal the array size exactly. */
+hp2d_status hp2d_download_native(hp2d_ctx* ctx, int32_t field, void* host, size_t bytes);
+hp2d_status hp2d_get_diag(hp2d_ctx* ctx, hp2d_diag* out);
+/* Stored surface volume sum(d_t)*cell_area/1000 [m^3], FP64 accumulation. */
+hp2d_status hp2d_stored_volume(hp2d_ctx* ctx, double* volume);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HP2D_H */

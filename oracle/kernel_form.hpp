@@ -1,0 +1,536 @@
+// Oracle, kernel form -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of HydroPol2D's surface-flow step in the algebraically identical form
+// the CUDA kernels compute, in float or double.  The tests require the CUDA kernels to
+// reproduce this restatement bit for bit, and require this restatement (in double) to
+// agree with the literal FP64 restatement (oracle/literal.py) to round-off.
+//
+// Differences from the literal reference order, each algebraically exact:
+//   * SI state inside: h [m], face discharge per unit width q [m^2/s], I [m], T [s].
+//     The reference carries mm and mm/h (Local_Inertial_Model_D4.m:198, :309).
+//   * Split slope: S = (dz + (h_R - h_L)) / dx with dz = z_R - z_L precomputed from the
+//     FP64 DEM, and Hf = max(max(h_L - max(dz,0), h_R + min(dz,0)), 0), which equals
+//     max(max(y_L, y_R) - max(z_L, z_R), 0) (Local_Inertial_Model_D4.m:91-134).
+//   * Bates update as (num * Hf^(7/3)) / (Hf^(7/3) + g dt n^2 |q_p|), equal to
+//     num / (1 + g dt n^2 |q_p| / Hf^(7/3)) (Inertial_Solver.m:24-25), one division.
+//   * Hf^(7/3), h^(5/3): x^2 * cbrt(x) and x * cbrt(x)^2 with cbrt(x) = x * r^2 and
+//     r = x^(-1/3) from a fixed Newton iteration (no libm), so that CPU and GPU round
+//     identically.  The seed is the exponent-field division of the IEEE representation
+//     (the classic bit-level log2 approximation), refined by r <- r + r(1 - x r^3)/3.
+//   * Draining limiter compares rates per unit width (both sides divided by dx).
+//   * CFL velocities q/Hf (refreshing_timestep.m:71-77 after unit cancellation); the
+//     minimum of alfa*dx/c over cells is taken as alfa*dx/max(c), which is exact because
+//     division by a positive number is monotone.
+// Compile with -ffp-contract=off: no fused multiply-add may appear.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+#include <algorithm>
+
+#include "hp2d.h"
+
+namespace hp2d_oracle {
+
+constexpr double kG = 9.81;
+
+template <typename R> struct FloatBits;
+template <> struct FloatBits<float> {
+    using U = uint32_t;
+    static constexpr U seed = 0x54AAAAABu;                  // (4/3) * 127 * 2^23
+    static constexpr int iters = 3;
+    static float tiny() { return 1.17549435e-38f; }         // smallest normal
+    static constexpr float up = 16777216.0f;                // 2^24
+    static constexpr float down_r = 256.0f;                 // 2^8
+};
+template <> struct FloatBits<double> {
+    using U = uint64_t;
+    static constexpr U seed = 0x5540000000000000ull;        // (4/3) * 1023 * 2^52
+    static constexpr int iters = 5;
+    static double tiny() { return 2.2250738585072014e-308; }
+    static constexpr double up = 18014398509481984.0;       // 2^54
+    static constexpr double down_r = 262144.0;              // 2^18
+};
+
+// x^(-1/3) for finite x > 0.
+template <typename R> inline R rcbrt(R x) {
+    using FB = FloatBits<R>;
+    R scale = R(1);
+    if (x < FB::tiny()) { x = x * FB::up; scale = FB::down_r; }
+    typename FB::U u;
+    std::memcpy(&u, &x, sizeof(R));
+    u = FB::seed - u / 3;
+    R r;
+    std::memcpy(&r, &u, sizeof(R));
+    const R third = R(1.0 / 3.0);
+    for (int it = 0; it < FB::iters; ++it) {
+        R t = x * r;
+        t = t * r;
+        t = t * r;
+        R e = R(1) - t;
+        r = r + (r * e) * third;
+    }
+    return r * scale;
+}
+template <typename R> inline R pow73(R x) {       // x^(7/3), x >= 0
+    if (!(x > R(0))) return R(0);
+    R r = rcbrt(x);
+    R c = x * (r * r);
+    return (x * x) * c;
+}
+template <typename R> inline R pow53(R x) {       // x^(5/3), x >= 0
+    if (!(x > R(0))) return R(0);
+    R r = rcbrt(x);
+    R c = x * (r * r);
+    return x * (c * c);
+}
+
+template <typename R> inline bool finite(R v) { return std::isfinite(v); }
+
+template <typename R> struct Consts {
+    R dt, gdt, dt_over_dx, dx_over_dt, inv_dt, inv_dx, rain_scale, g, tol, thr,
+      clamp_eps, neg_eps, ten, half, stagnant, celer_floor, big_depth;
+    Consts(double dt_s, double res, double tol_mm, double thr_mm) {
+        dt = R(dt_s);
+        gdt = R(kG * dt_s);
+        dt_over_dx = R(dt_s / res);
+        dx_over_dt = R(res / dt_s);
+        inv_dt = R(1.0 / dt_s);
+        inv_dx = R(1.0 / res);
+        rain_scale = R(dt_s / 3.6e6);
+        g = R(kG);
+        tol = R(tol_mm / 1000.0);
+        thr = R(thr_mm / 1000.0);
+        clamp_eps = R(1e-9);
+        neg_eps = R(-1e-11);
+        ten = R(10);
+        half = R(0.5);
+        stagnant = R(0.01);
+        celer_floor = R(1e-10);
+        big_depth = R(1e9);
+    }
+};
+
+template <typename R> class Model {
+public:
+    int ny, nx;
+    double res;
+    hp2d_params p;
+    // static
+    std::vector<R> dzx, dzy, n2;
+    std::vector<int32_t> outlet_idx;
+    std::vector<R> outlet_coef;
+    std::vector<uint8_t> soil;          // empty or ny*nx, 255 = none
+    std::vector<R> ks, psi, dth, lu, kout, tr, minsm;   // per class
+    // rain
+    std::vector<double> rain_t, rain_r;
+    int n_maps = 0, my = 0, mx = 0;
+    double map_dt = 5.0;
+    std::vector<float> maps;
+    // state
+    std::vector<R> h, qx, qy, I, T, dmax, arrival;
+    // outputs of the last li step
+    std::vector<R> hfx, hfy, hf3, qo;    // hf3/qo per outlet entry
+    std::vector<R> qx_unl, qy_unl, scale, hn;
+    // clock
+    double t_min = 0, time_step = 0, tsp = 0;   // clock [min], step [min], time_save_previous
+    int64_t k = 1;
+    // diagnostics
+    double vmax_last = 0, rain_vol = 0, inf_vol = 0, out_vol = 0;
+    int64_t neg_warn = 0, unstable = 0;
+    int omp_threads = 1;
+
+    Model(const hp2d_grid& g, const hp2d_params& prm) : ny(g.ny), nx(g.nx), res(g.resolution), p(prm) {
+        size_t n = size_t(ny) * nx;
+        dzx.assign(n, R(0)); dzy.assign(n, R(0)); n2.assign(n, R(0));
+        h.assign(n, R(0)); qx.assign(n, R(0)); qy.assign(n, R(0));
+        I.assign(n, R(0)); T.assign(n, R(0));
+        dmax.assign(n, -std::numeric_limits<R>::infinity());
+        arrival.assign(n, std::numeric_limits<R>::infinity());
+        hfx.assign(n, R(0)); hfy.assign(n, R(0));
+        qx_unl.assign(n, R(0)); qy_unl.assign(n, R(0)); scale.assign(n, R(1));
+        time_step = p.min_time_step / 60.0;   // HydroPol2D_preprocessing.m:2469
+        t_min = p.min_time_step / 60.0;
+    }
+
+    size_t at(int i, int j) const { return size_t(i) * nx + j; }
+
+    void upload_static(const double* z, const double* n, const int32_t* rows, const int32_t* cols,
+                       int nout, const double* slopes) {
+        const double qnan = std::numeric_limits<double>::quiet_NaN();
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t c = at(i, j);
+                double dx_ = (j + 1 < nx) ? z[at(i, j + 1)] - z[c] : qnan;
+                double dy_ = (i >= 1) ? z[at(i - 1, j)] - z[c] : qnan;
+                dzx[c] = R(dx_);
+                dzy[c] = R(dy_);
+                n2[c] = R(n[c] * n[c]);
+            }
+        // outlet cells in increasing linear-index order, duplicates dropped (a repeated
+        // index in MATLAB's d_t(outlet_sub) assignment writes the same value twice)
+        std::vector<std::pair<int32_t, R>> outs;
+        for (int o = 0; o < nout; ++o) {
+            size_t c = at(rows[o], cols[o]);
+            double coef;
+            if (p.outlet_type == 1) {
+                double s = slopes ? slopes[o] : p.slope_outlet;
+                coef = std::sqrt(std::fabs(s)) / (n[c] * res);
+            } else {
+                coef = std::sqrt(kG) / res;
+            }
+            outs.emplace_back(int32_t(c), R(coef));
+        }
+        std::sort(outs.begin(), outs.end(), [](auto& a, auto& b) { return a.first < b.first; });
+        outs.erase(std::unique(outs.begin(), outs.end(), [](auto& a, auto& b) { return a.first == b.first; }),
+                   outs.end());
+        outlet_idx.resize(outs.size());
+        outlet_coef.resize(outs.size());
+        for (size_t o = 0; o < outs.size(); ++o) {
+            outlet_idx[o] = outs[o].first;
+            outlet_coef[o] = outs[o].second;
+        }
+        hf3.assign(outs.size(), R(0));
+        qo.assign(outs.size(), R(0));
+    }
+
+    void set_soil(const uint8_t* cls, int ncls, const double* ksat, const double* psi_mm,
+                  const double* dtheta, const double* Lu, const double* kout_mmh,
+                  const double* Tr_h, const double* minsm_mm) {
+        soil.assign(cls, cls + size_t(ny) * nx);
+        ks.resize(ncls); psi.resize(ncls); dth.resize(ncls); lu.resize(ncls);
+        kout.resize(ncls); tr.resize(ncls); minsm.resize(ncls);
+        for (int c = 0; c < ncls; ++c) {
+            ks[c] = R(ksat[c] / 3.6e6);
+            psi[c] = R(psi_mm[c] / 1000.0);
+            dth[c] = R(dtheta[c]);
+            lu[c] = R(Lu[c]);
+            kout[c] = R(kout_mmh[c] / 3.6e6);
+            tr[c] = R(Tr_h[c] * 3600.0);
+            minsm[c] = R(minsm_mm[c] / 1000.0);
+        }
+        reset_timer();
+    }
+
+    void set_state(const double* d_mm, const double* outflow, const double* I_mm) {
+        size_t n = size_t(ny) * nx;
+        for (size_t c = 0; c < n; ++c) {
+            h[c] = R(d_mm[c] / 1000.0);
+            // outflow_bates [mm/h] -> q [m^2/s]: mm/h / 1000 / 3600 * dx
+            qx[c] = outflow ? R(outflow[c] / 3.6e6 * res) : R(0);
+            qy[c] = outflow ? R(outflow[n + c] / 3.6e6 * res) : R(0);
+            if (I_mm) I[c] = R(I_mm[c] / 1000.0);
+            dmax[c] = -std::numeric_limits<R>::infinity();
+            arrival[c] = std::numeric_limits<R>::infinity();
+        }
+        reset_timer();
+    }
+
+    // recovery timer starts at Tr (HydroPol2D_Main_While_Ensemble.m:266)
+    void reset_timer() {
+        for (size_t c = 0; c < T.size(); ++c)
+            T[c] = (!soil.empty() && soil[c] != 255) ? tr[soil[c]] : R(0);
+    }
+
+    // test hook: overwrite the depth only [mm]
+    void set_depth(const double* d_mm) {
+        for (size_t c = 0; c < h.size(); ++c) h[c] = R(d_mm[c] / 1000.0);
+    }
+
+    // rain rate [mm/h] in R for cell (i, j) at clock t [min]
+    R rain_rate(int i, int j, double t) const {
+        if (n_maps > 0) {
+            int m = int(std::floor(t / map_dt));
+            m = std::max(0, std::min(m, n_maps - 1));
+            const float* f = maps.data() + size_t(m) * my * mx;
+            const R half = R(0.5);
+            R fy = (R(i) + half) * R(double(my) / ny) - half;
+            R fx = (R(j) + half) * R(double(mx) / nx) - half;
+            fy = std::fmin(std::fmax(fy, R(0)), R(my - 1));
+            fx = std::fmin(std::fmax(fx, R(0)), R(mx - 1));
+            int iy0 = int(std::floor(fy)), ix0 = int(std::floor(fx));
+            int iy1 = std::min(iy0 + 1, my - 1), ix1 = std::min(ix0 + 1, mx - 1);
+            R wy = fy - R(iy0), wx = fx - R(ix0);
+            R f00 = R(f[iy0 * mx + ix0]), f01 = R(f[iy0 * mx + ix1]);
+            R f10 = R(f[iy1 * mx + ix0]), f11 = R(f[iy1 * mx + ix1]);
+            R top = (R(1) - wx) * f00 + wx * f01;
+            R bot = (R(1) - wx) * f10 + wx * f11;
+            return (R(1) - wy) * top + wy * bot;
+        }
+        if (rain_r.empty()) return R(0);
+        int idx = -1;
+        for (size_t q = 0; q < rain_t.size(); ++q)
+            if (rain_t[q] <= t) idx = int(q);
+        if (idx < 0) return R(0);
+        return R(rain_r[idx]);
+    }
+
+    // ---------------- hydrology: rain + Green-Ampt + clamp ----------------
+    void hydrology(double dts) {
+        Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
+        size_t n = size_t(ny) * nx;
+        double rv = 0, iv = 0;
+        const bool ga = p.flag_infiltration == 1 && !soil.empty();
+#pragma omp parallel for schedule(static) reduction(+ : rv, iv)
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t c = at(i, j);
+                R r = rain_rate(i, j, t_min) * K.rain_scale;
+                R hh = h[c] + r;
+                if (std::isfinite(double(hh))) rv += double(r);
+                if (ga && soil[c] != 255) {
+                    int s = soil[c];
+                    R Ip = I[c];
+                    R C = ks[s] * (R(1) + ((hh + psi[s]) * dth[s]) / Ip);
+                    if (Ip > lu[s]) C = ks[s];
+                    R ia = hh * K.inv_dt;
+                    bool idxC = ia <= C;
+                    R Tn = T[c] - K.dt;
+                    if (ia > C) Tn = tr[s];
+                    bool idxT = Tn < R(0);
+                    R f = std::fmin(C, ia);
+                    R In = Ip + f * K.dt;
+                    if (idxC) In = In - kout[s] * K.dt;
+                    In = std::fmax(In, minsm[s]);
+                    if (idxT) In = minsm[s];
+                    I[c] = In;
+                    T[c] = Tn;
+                    R fd = f * K.dt;
+                    hh = hh - fd;
+                    if (hh < R(0)) hh = R(0);
+                    if (std::isfinite(double(fd))) iv += double(fd);
+                }
+                h[c] = hh;
+            }
+        rain_vol += rv * res * res;
+        inf_vol += iv * res * res;
+        bool any_neg = false;
+#pragma omp parallel for schedule(static) reduction(|| : any_neg)
+        for (size_t c = 0; c < n; ++c)
+            if (h[c] < K.neg_eps) any_neg = true;
+        if (any_neg) ++neg_warn;
+#pragma omp parallel for schedule(static)
+        for (size_t c = 0; c < n; ++c) {
+            if (!any_neg && h[c] < K.clamp_eps) h[c] = R(0);
+            if (h[c] < R(0)) h[c] = R(0);
+        }
+    }
+
+    // ---------------- Local_Inertial_Model_D4 ----------------
+    // one face: returns (Hf, q) from neighbour depths; for x faces (a, b) = (L, R);
+    // for y faces (a, b) = (U, D) and dz = z_U - z_D, so the roles of max/min swap.
+    inline void face(R ha, R hb, R dz, R qp, R n2c, bool is_x, const Consts<R>& K, R& Hf, R& q) const {
+        if (std::isnan(dz)) { Hf = R(0); q = R(0); return; }
+        ha = std::fmax(ha, R(0));
+        hb = std::fmax(hb, R(0));
+        R S;
+        if (is_x) {
+            Hf = std::fmax(std::fmax(ha - std::fmax(dz, R(0)), hb + std::fmin(dz, R(0))), R(0));
+            S = (dz + (hb - ha)) * K.inv_dx;
+        } else {
+            Hf = std::fmax(std::fmax(ha + std::fmin(dz, R(0)), hb - std::fmax(dz, R(0))), R(0));
+            S = (dz + (ha - hb)) * K.inv_dx;
+        }
+        if (!(Hf > R(0))) { q = R(0); return; }
+        R num = qp - (K.gdt * Hf) * S;
+        R h73 = pow73(Hf);
+        R den = h73 + (K.gdt * n2c) * std::fabs(qp);
+        q = (num * h73) / den;
+        if (!std::isfinite(q)) q = R(0);
+        if (p.flag_critical == 1) {
+            R crit = Hf * std::sqrt(K.g * Hf);
+            q = std::fmin(std::fmax(q, -crit), crit);
+        }
+        R thr = Hf * K.ten;
+        q = std::fmin(std::fmax(q, -thr), thr);
+    }
+
+    void li(double dts) {
+        Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
+        // faces (unlimited)
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t c = at(i, j);
+                R Hf, q;
+                R hR = (j + 1 < nx) ? h[at(i, j + 1)] : R(0);
+                face(h[c], hR, dzx[c], qx[c], n2[c], true, K, Hf, q);
+                hfx[c] = Hf; qx_unl[c] = q;
+                R hU = (i >= 1) ? h[at(i - 1, j)] : R(0);
+                face(hU, h[c], dzy[c], qy[c], n2[c], false, K, Hf, q);
+                hfy[c] = Hf; qy_unl[c] = q;
+            }
+        // donor scale
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t c = at(i, j);
+                R out = std::fmax(qx_unl[c], R(0));
+                if (j >= 1) out = out + std::fmax(-qx_unl[at(i, j - 1)], R(0));
+                out = out + std::fmax(qy_unl[c], R(0));
+                if (i + 1 < ny) out = out + std::fmax(-qy_unl[at(i + 1, j)], R(0));
+                R avail = std::fmax(h[c], R(0)) * K.dx_over_dt;
+                R s = R(1);
+                if (out > avail && out > R(0)) s = avail / out;
+                if (!std::isfinite(s)) s = R(0);
+                scale[c] = std::fmax(std::fmin(s, R(1)), R(0));
+            }
+        // limited faces
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t c = at(i, j);
+                R q = qx_unl[c];
+                if (j + 1 < nx) {
+                    if (q > R(0)) q = q * scale[c];
+                    else if (q < R(0)) q = q * scale[at(i, j + 1)];
+                } else q = R(0);
+                if (!std::isfinite(q)) q = R(0);
+                qx[c] = q;
+                q = qy_unl[c];
+                if (i >= 1) {
+                    if (q > R(0)) q = q * scale[c];
+                    else if (q < R(0)) q = q * scale[at(i - 1, j)];
+                } else q = R(0);
+                if (!std::isfinite(q)) q = R(0);
+                qy[c] = q;
+            }
+        // continuity
+        hn.resize(h.size());
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t c = at(i, j);
+                R qL = (j >= 1) ? qx[at(i, j - 1)] : R(0);
+                R qD = (i + 1 < ny) ? qy[at(i + 1, j)] : R(0);
+                R hnew = h[c] + K.dt_over_dx * (((qL - qx[c]) - qy[c]) + qD);
+                if (hnew < R(0)) hnew = R(0);
+                hn[c] = hnew;
+            }
+        h.swap(hn);
+        // outlet sink
+        double ov = 0;
+        for (size_t o = 0; o < outlet_idx.size(); ++o) {
+            size_t c = size_t(outlet_idx[o]);
+            R hc = h[c];
+            R hout = std::fmax(hc, R(0));
+            R qq;
+            if (p.outlet_type == 1) qq = outlet_coef[o] * pow53(hout);
+            else qq = outlet_coef[o] * (hout * std::sqrt(hout));
+            R qmax = hout * K.inv_dt;
+            qq = std::fmin(qq, qmax);
+            if (!std::isfinite(qq)) qq = R(0);
+            h[c] = hc - qq * K.dt;
+            hf3[o] = hout;
+            qo[o] = qq;
+            ov += double(qq * K.dt);
+        }
+        out_vol += ov * res * res;
+    }
+
+    // ---------------- refreshing_timestep (refresh branch) ----------------
+    // returns time_calculation_routing [s]; fills vmax
+    double cfl(double dts, double* vmax_out) {
+        Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
+        std::vector<R> hf3c(h.size(), R(0));
+        for (size_t o = 0; o < outlet_idx.size(); ++o) hf3c[outlet_idx[o]] = hf3[o];
+        R vmax = R(0), cmax = R(0);
+#pragma omp parallel
+        {
+        R tv = R(0), tc = R(0);
+#pragma omp for schedule(static)
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t c = at(i, j);
+                R sx = hfx[c] < K.tol ? K.big_depth : hfx[c];
+                R sy = hfy[c] < K.tol ? K.big_depth : hfy[c];
+                R vr = qx[c] / sx;
+                R vu = qy[c] / sy;
+                R vb = R(0);
+                if (i + 1 < ny) {
+                    size_t cb = at(i + 1, j);
+                    R sb = hfy[cb] < K.tol ? K.big_depth : hfy[cb];
+                    vb = qy[cb] / sb;
+                }
+                R rc = (j == 0) ? K.half * vr : vr;
+                R uc = K.half * (vu + vb);
+                R tot = std::sqrt(rc * rc + uc * uc);
+                tv = std::fmax(tv, tot);
+                if (tot >= K.stagnant) {
+                    R dts_ = std::fmax(std::fmax(hfx[c], hfy[c]), hf3c[c]);
+                    R wc = std::fmax(std::sqrt(K.g * std::fmax(dts_, R(0))), K.celer_floor);
+                    if (p.flag_adaptive_timestepping != 1) {
+                        R ras = std::fmax(std::fmax(std::fabs(vr), std::fabs(vu)), std::fabs(vb));
+                        wc = ras + wc;
+                    }
+                    tc = std::fmax(tc, wc);
+                }
+            }
+#pragma omp critical
+        {
+            vmax = std::fmax(vmax, tv);
+            cmax = std::fmax(cmax, tc);
+        }
+        }
+        *vmax_out = double(vmax);
+        return finalize_dt(double(vmax), double(cmax));
+    }
+
+    double finalize_dt(double vmax, double cmax) const {
+        double dt_adv;
+        if (vmax > 0) {
+            dt_adv = 1.0 * res / std::max(vmax, 1e-10);
+            double tsf = std::max(p.alfa_max - 2.0 * std::max(vmax - 5.0, 0.0), p.alfa_min);
+            dt_adv = std::min(dt_adv * tsf, p.max_time_step);
+        } else {
+            dt_adv = p.max_time_step;
+        }
+        double dt_wave = cmax > 0 ? (p.alfa_min * res) / cmax : p.max_time_step;
+        double nw = p.flag_timestep == 1 ? std::min(dt_adv, dt_wave) : dt_wave;
+        if (std::isnan(nw) || std::isinf(nw)) nw = p.max_time_step;
+        double tcr = std::max(p.time_step_increments * std::floor(nw / p.time_step_increments),
+                              p.min_time_step);
+        return std::min(tcr, p.max_time_step);
+    }
+
+    void track(double t_end_s) {
+        R thr = R(p.arrival_threshold / 1000.0);
+        R te = R(t_end_s);
+#pragma omp parallel for schedule(static)
+        for (size_t c = 0; c < h.size(); ++c) {
+            if (dmax[c] < thr && h[c] >= thr) arrival[c] = te;
+            dmax[c] = std::fmax(h[c], dmax[c]);
+        }
+    }
+
+    // ---------------- one accepted step (HydroPol2D_Main_While.m:403-782) ----------------
+    // The step is carried in minutes, as the reference does (time_step, min), and the
+    // seconds of the step are time_step*60 (Local_Inertial_Model_D4.m:201).
+    void step() {
+        double dts = time_step * 60.0;
+        hydrology(dts);
+        li(dts);
+        double pos_save = std::ceil((t_min * 60.0) / p.time_step_change);
+        double time_save = (pos_save - 1.0) * p.time_step_change / 60.0;
+        double delta = time_save - tsp;
+        tsp = time_save;
+        double tcr = time_step * 60.0;
+        if (delta > 0 || k == 1) {
+            double vm;
+            tcr = cfl(dts, &vm);
+            vmax_last = vm;
+            if (tcr == p.min_time_step) ++unstable;
+        }
+        track(t_min * 60.0 + dts);
+        time_step = tcr / 60.0;
+        t_min = tcr / 60.0 + t_min;
+        ++k;
+    }
+
+    bool finished() const { return !(t_min <= p.routing_time + p.min_time_step / 60.0); }
+};
+
+}  // namespace hp2d_oracle

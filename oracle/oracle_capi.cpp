@@ -1,0 +1,169 @@
+// Oracle C entry points -- TEST INFRASTRUCTURE ONLY (loaded by tests/ and bench.py's CPU
+// baseline through ctypes).  Wraps the kernel-form restatement (kernel_form.hpp) in the
+// same argument conventions as include/hp2d.h so a test can drive the CUDA library and
+// the oracle with identical calls.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "kernel_form.hpp"
+
+using hp2d_oracle::Model;
+
+struct oracle_model {
+    int precision;
+    std::unique_ptr<Model<float>> f;
+    std::unique_ptr<Model<double>> d;
+};
+
+template <typename F> static int dispatch(oracle_model* m, F&& fn) {
+    if (!m) return HP2D_INVALID_ARG;
+    if (m->precision == HP2D_FP32) return fn(*m->f);
+    return fn(*m->d);
+}
+
+extern "C" {
+
+oracle_model* oracle_create(const hp2d_grid* g, const hp2d_params* p) {
+    auto* m = new oracle_model();
+    m->precision = g->precision;
+    if (g->precision == HP2D_FP32) m->f.reset(new Model<float>(*g, *p));
+    else m->d.reset(new Model<double>(*g, *p));
+    return m;
+}
+
+void oracle_destroy(oracle_model* m) { delete m; }
+
+int oracle_upload_static(oracle_model* m, const double* z, const double* n, const int32_t* rows,
+                         const int32_t* cols, int32_t nout, const double* slopes) {
+    return dispatch(m, [&](auto& M) { M.upload_static(z, n, rows, cols, nout, slopes); return 0; });
+}
+
+int oracle_set_soil(oracle_model* m, const uint8_t* cls, int32_t ncls, const double* ksat,
+                    const double* psi, const double* dtheta, const double* Lu, const double* kout,
+                    const double* Tr, const double* minsm) {
+    return dispatch(m, [&](auto& M) {
+        M.set_soil(cls, ncls, ksat, psi, dtheta, Lu, kout, Tr, minsm);
+        return 0;
+    });
+}
+
+int oracle_set_state(oracle_model* m, const double* d, const double* outflow, const double* I) {
+    return dispatch(m, [&](auto& M) { M.set_state(d, outflow, I); return 0; });
+}
+
+int oracle_set_depth(oracle_model* m, const double* d) {
+    return dispatch(m, [&](auto& M) { M.set_depth(d); return 0; });
+}
+
+int oracle_set_clock(oracle_model* m, double t, double time_step, int64_t k) {
+    return dispatch(m, [&](auto& M) {
+        M.t_min = t;
+        M.time_step = time_step;
+        M.k = k;
+        return 0;
+    });
+}
+
+int oracle_set_rain_uniform(oracle_model* m, int32_t n, const double* t0, const double* rate) {
+    return dispatch(m, [&](auto& M) {
+        M.rain_t.assign(t0, t0 + n);
+        M.rain_r.assign(rate, rate + n);
+        M.n_maps = 0;
+        return 0;
+    });
+}
+
+int oracle_set_rain_maps(oracle_model* m, int32_t nm, int32_t my, int32_t mx, const float* rate,
+                         double map_dt) {
+    return dispatch(m, [&](auto& M) {
+        M.n_maps = nm; M.my = my; M.mx = mx; M.map_dt = map_dt;
+        M.maps.assign(rate, rate + size_t(nm) * my * mx);
+        return 0;
+    });
+}
+
+int oracle_hydrology_step(oracle_model* m, double time_step) {
+    return dispatch(m, [&](auto& M) { M.hydrology(time_step * 60.0); return 0; });
+}
+
+int oracle_li_step(oracle_model* m, double time_step) {
+    return dispatch(m, [&](auto& M) { M.li(time_step * 60.0); return 0; });
+}
+
+int oracle_cfl_dt(oracle_model* m, double time_step_applied, double* ts_out, double* vmax) {
+    return dispatch(m, [&](auto& M) {
+        double tcr = M.cfl(time_step_applied * 60.0, vmax);
+        *ts_out = tcr / 60.0;
+        return 0;
+    });
+}
+
+int oracle_track_maxima(oracle_model* m, double t_end) {
+    return dispatch(m, [&](auto& M) { M.track(t_end * 60.0); return 0; });
+}
+
+int oracle_steps(oracle_model* m, int32_t nsteps) {
+    return dispatch(m, [&](auto& M) {
+        for (int s = 0; s < nsteps; ++s) {
+            if (M.finished()) break;
+            M.step();
+        }
+        return 0;
+    });
+}
+
+int oracle_run(oracle_model* m, int64_t max_steps, int64_t* done) {
+    return dispatch(m, [&](auto& M) {
+        int64_t s = 0;
+        while (!M.finished() && (max_steps <= 0 || s < max_steps)) { M.step(); ++s; }
+        *done = s;
+        return 0;
+    });
+}
+
+// Raw state in the internal units and precision (for bit-exact comparison).
+//   0 h [m], 1 qx [m^2/s], 2 qy, 3 I [m], 4 T [s], 5 dmax [m], 6 arrival [s],
+//   7 Hf_x [m], 8 Hf_y [m], 9 Hf3 per outlet, 10 outlet rate per outlet [m/s]
+int oracle_download_native(oracle_model* m, int32_t field, void* out, size_t bytes) {
+    return dispatch(m, [&](auto& M) {
+        using R = typename std::remove_reference<decltype(M.h[0])>::type;
+        const std::vector<R>* src = nullptr;
+        switch (field) {
+            case 0: src = &M.h; break;
+            case 1: src = &M.qx; break;
+            case 2: src = &M.qy; break;
+            case 3: src = &M.I; break;
+            case 4: src = &M.T; break;
+            case 5: src = &M.dmax; break;
+            case 6: src = &M.arrival; break;
+            case 7: src = &M.hfx; break;
+            case 8: src = &M.hfy; break;
+            case 9: src = &M.hf3; break;
+            case 10: src = &M.qo; break;
+            default: return int(HP2D_INVALID_ARG);
+        }
+        if (bytes != src->size() * sizeof(R)) return int(HP2D_INVALID_ARG);
+        std::memcpy(out, src->data(), bytes);
+        return 0;
+    });
+}
+
+int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
+    return dispatch(m, [&](auto& M) {
+        o->t = M.t_min;
+        o->time_step = M.time_step;
+        o->k = M.k;
+        o->max_velocity = M.vmax_last;
+        o->rain_volume = M.rain_vol;
+        o->infiltration_volume = M.inf_vol;
+        o->outlet_volume = M.out_vol;
+        o->neg_depth_warnings = M.neg_warn;
+        o->unstable_steps = M.unstable;
+        o->status_bits = 0;
+        return 0;
+    });
+}
+
+}  // extern "C"
