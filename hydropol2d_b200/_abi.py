@@ -35,7 +35,8 @@ EXPORTS = [
     "hp2d_create", "hp2d_destroy", "hp2d_last_error", "hp2d_create_error",
     "hp2d_upload_static", "hp2d_set_soil", "hp2d_set_state", "hp2d_set_clock",
     "hp2d_set_rain_uniform", "hp2d_set_rain_maps", "hp2d_hydrology_step", "hp2d_li_step",
-    "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed", "hp2d_run",
+    "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed",
+    "hp2d_set_tuning", "hp2d_run",
     "hp2d_download",
     "hp2d_download_native", "hp2d_get_diag", "hp2d_stored_volume",
 ]
@@ -117,6 +118,7 @@ def lib() -> C.CDLL:
         "hp2d_track_maxima": ([vp, C.c_double], C.c_int),
         "hp2d_fused_steps": ([vp, C.c_int32], C.c_int),
         "hp2d_fused_steps_timed": ([vp, C.c_int32, P(C.c_float)], C.c_int),
+        "hp2d_set_tuning": ([vp, C.c_int32], C.c_int),
         "hp2d_run": ([vp, C.c_int64, P(C.c_int64)], C.c_int),
         "hp2d_download": ([vp, C.c_int32, dp, C.c_size_t], C.c_int),
         "hp2d_download_native": ([vp, C.c_int32, vp, C.c_size_t], C.c_int),

@@ -3,6 +3,15 @@
 //   nvcc -gencode arch=compute_100a,code=sm_100a -fmad=false -O3 -shared ...
 // (-fmad=false keeps every product and sum separately rounded, which the parity tests
 // against the CPU restatement rely on).
+//
+// Device layout of one context (n = ny*nx cells, R = float or double):
+//   stat      n x {dz_x, dz_y, n^2, meta}            static record (16 or 32 B)
+//   st4[2]    n x {h, q_x, q_y, dmax}                state record, double-buffered
+//   gs2[2]    n x {I, T}                             Green-Ampt record, double-buffered
+//   arrival   n x R
+//   per outlet: coefficient, Hf(:,:,3) and sink rate
+// plus, for the unfused entry points only, structure-of-arrays copies (dz_x, dz_y, n^2,
+// soil class, outlet bitmask) and scratch (h, q, dmax, I, T, Hf, unlimited q, scale).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -25,7 +34,7 @@ namespace {
 
 thread_local std::string g_create_error;
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 
 struct CudaFail {
     cudaError_t e;
@@ -42,13 +51,13 @@ struct Base {
     virtual ~Base() = default;
 };
 
-template <typename R> struct Dev {
-    R* p = nullptr;
+template <typename T> struct Dev {
+    T* p = nullptr;
     size_t n = 0;
     void alloc(size_t count) {
         free();
         if (count == 0) return;
-        HP_CK(cudaMalloc(&p, count * sizeof(R)));
+        HP_CK(cudaMalloc(&p, count * sizeof(T)));
         n = count;
     }
     void free() {
@@ -59,8 +68,32 @@ template <typename R> struct Dev {
     ~Dev() { free(); }
 };
 
-template <typename R> constexpr int fused_by() { return 16; }
-template <typename R> constexpr int fused_bx() { return sizeof(R) == 4 ? 64 : 32; }
+// smallest x >= 0 whose correctly rounded square root reaches R(0.01): the stagnant
+// test sqrt(s2) < 0.01 of refreshing_timestep.m:184 is then s2 < x exactly
+template <typename R> R stagnant_threshold() {
+    const R target = R(0.01);
+    R x = target * target;
+    while (x > R(0) && std::sqrt(std::nextafter(x, R(0))) >= target) x = std::nextafter(x, R(0));
+    while (std::sqrt(x) < target) x = std::nextafter(x, R(1));
+    return x;
+}
+
+template <typename R>
+__global__ void k_write_meta(size_t n, typename Vec<R>::V4* stat, const uint32_t* meta) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x)
+        stat[c].w = make_meta<R>(meta[c]);
+}
+
+template <typename R>
+__global__ void k_volume4(size_t n, const typename Vec<R>::V4* st, double* out) {
+    double acc = 0;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
+        const R v = st[c].x;
+        if (isfinite(v)) acc += double(v);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(out, acc);
+}
 
 }  // namespace
 
@@ -76,29 +109,42 @@ struct hp2d_ctx {
 namespace {
 
 template <typename R> struct Impl : Base {
+    using V4 = typename Vec<R>::V4;
+    using V2 = typename Vec<R>::V2;
     hp2d_ctx* ctx;
     int ny, nx;
     size_t n;
     double res;
-    Dev<R> dzx, dzy, n2;
-    Dev<uint8_t> soil;
+    // fused-path records
+    Dev<V4> stat, st4[2];
+    Dev<V2> gs2[2];
+    Dev<R> arrival;
     Dev<SoilClass<R>> classes;
     int n_classes = 0;
-    Dev<uint32_t> outlet_bits;
-    int bit_words = 0;
     Dev<int32_t> outlet_cells;
     Dev<R> outlet_coef, hf3, qo;
     int n_out = 0;
-    Dev<R> h[2], qx[2], qy[2], I[2], T[2], dmax, arrival;
+    // unfused path: structure-of-arrays copies and scratch
+    Dev<R> dzx, dzy, n2;
+    Dev<uint8_t> soil;
+    Dev<uint32_t> outlet_bits;
+    int bit_words = 0;
+    Dev<R> h, qx, qy, dmax, I, T;
     Dev<R> hfx, hfy, qxu, qyu, scale;
+    // forcing, clock
     Dev<double> rain_t, rain_r;
     Dev<float> maps;
     RainDesc rain{};
     Dev<StepScalars> sc;
     StepScalars hs{};
     Dev<double> vol;
-    bool static_ready = false, state_ready = false, dirty = true;
+    // host copies needed to rebuild records
+    std::vector<uint32_t> host_meta;
+    std::vector<uint8_t> host_soil;
+    std::vector<R> host_tr;
+    bool static_ready = false, dirty = true;
     double last_dt_s = 0;
+    int rows_per_warp = 64;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
 
@@ -107,25 +153,29 @@ template <typename R> struct Impl : Base {
         nx = c->g.nx;
         n = size_t(ny) * nx;
         res = c->g.resolution;
-        dzx.alloc(n); dzy.alloc(n); n2.alloc(n);
-        for (int b = 0; b < 2; ++b) {
-            h[b].alloc(n); qx[b].alloc(n); qy[b].alloc(n);
-            HP_CK(cudaMemset(h[b].p, 0, n * sizeof(R)));
-            HP_CK(cudaMemset(qx[b].p, 0, n * sizeof(R)));
-            HP_CK(cudaMemset(qy[b].p, 0, n * sizeof(R)));
-        }
-        dmax.alloc(n); arrival.alloc(n);
+        stat.alloc(n);
+        for (int b = 0; b < 2; ++b) st4[b].alloc(n);
+        arrival.alloc(n);
         sc.alloc(1);
         vol.alloc(1);
         bit_words = (nx + 31) / 32;
-        outlet_bits.alloc(size_t(ny) * bit_words);
-        HP_CK(cudaMemset(outlet_bits.p, 0, size_t(ny) * bit_words * sizeof(uint32_t)));
+        host_meta.assign(n, 255u);
         std::memset(&hs, 0, sizeof(hs));
         hs.t_min = c->p.min_time_step / 60.0;
         hs.time_step = c->p.min_time_step / 60.0;   // HydroPol2D_preprocessing.m:2469
         hs.k = 1;
         push_sc();
-        reset_maxima();
+        // closed faces everywhere until hp2d_upload_static, dry state
+        std::vector<V4> s(n), x(n);
+        const R qn = std::numeric_limits<R>::quiet_NaN();
+        for (size_t k = 0; k < n; ++k) {
+            s[k] = V4{qn, qn, R(0), make_meta<R>(255u)};
+            x[k] = V4{R(0), R(0), R(0), -std::numeric_limits<R>::infinity()};
+        }
+        upload(stat.p, s);
+        upload(st4[0].p, x);
+        upload(st4[1].p, x);
+        fill(arrival.p, n, std::numeric_limits<R>::infinity());
     }
     ~Impl() override {
         if (graph) cudaGraphExecDestroy(graph);
@@ -135,27 +185,20 @@ template <typename R> struct Impl : Base {
     void push_sc() { HP_CK(cudaMemcpyAsync(sc.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, st())); HP_CK(cudaStreamSynchronize(st())); }
     void pull_sc() { HP_CK(cudaMemcpyAsync(&hs, sc.p, sizeof(hs), cudaMemcpyDeviceToHost, st())); HP_CK(cudaStreamSynchronize(st())); }
 
-    void fill(R* p, size_t count, R v) {
-        std::vector<R> tmp(count, v);
-        HP_CK(cudaMemcpyAsync(p, tmp.data(), count * sizeof(R), cudaMemcpyHostToDevice, st()));
+    template <typename T> void upload(T* dst, const std::vector<T>& v) {
+        if (v.empty()) return;
+        HP_CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st()));
         HP_CK(cudaStreamSynchronize(st()));
     }
-    void reset_maxima() {
-        fill(dmax.p, n, -std::numeric_limits<R>::infinity());
-        fill(arrival.p, n, std::numeric_limits<R>::infinity());
-    }
-    void upload(R* dst, const std::vector<R>& v) {
-        HP_CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(R), cudaMemcpyHostToDevice, st()));
-        HP_CK(cudaStreamSynchronize(st()));
-    }
-    std::vector<R> fetch(const R* src, size_t count) {
-        std::vector<R> v(count);
+    template <typename T> std::vector<T> fetch(const T* src, size_t count) {
+        std::vector<T> v(count);
         if (count) {
-            HP_CK(cudaMemcpyAsync(v.data(), src, count * sizeof(R), cudaMemcpyDeviceToHost, st()));
+            HP_CK(cudaMemcpyAsync(v.data(), src, count * sizeof(T), cudaMemcpyDeviceToHost, st()));
             HP_CK(cudaStreamSynchronize(st()));
         }
         return v;
     }
+    void fill(R* p, size_t count, R v) { upload(p, std::vector<R>(count, v)); }
     GridView<R> view() const {
         GridView<R> gv;
         gv.ny = ny; gv.nx = nx; gv.res = res;
@@ -165,21 +208,22 @@ template <typename R> struct Impl : Base {
     }
     int blocks_for(size_t count) const {
         size_t b = (count + kThreads - 1) / kThreads;
-        return int(std::max<size_t>(1, std::min<size_t>(b, 148 * 16)));
+        return int(std::max<size_t>(1, std::min<size_t>(b, 148 * 32)));
+    }
+    bool ga() const { return ctx->p.flag_infiltration == 1 && n_classes > 0; }
+
+    void write_meta() {
+        Dev<uint32_t> m;
+        m.alloc(n);
+        upload(m.p, host_meta);
+        k_write_meta<R><<<blocks_for(n), kThreads, 0, st()>>>(n, stat.p, m.p);
+        HP_CK(cudaGetLastError());
+        HP_CK(cudaStreamSynchronize(st()));
     }
 
     hp2d_status upload_static(const double* z, const double* rough, const int32_t* rows, const int32_t* cols,
                               int32_t nout, const double* slopes) {
         const double qnan = std::numeric_limits<double>::quiet_NaN();
-        std::vector<R> a(n), b(n), c(n);
-        for (int i = 0; i < ny; ++i)
-            for (int j = 0; j < nx; ++j) {
-                size_t k = size_t(i) * nx + j;
-                a[k] = R((j + 1 < nx) ? z[k + 1] - z[k] : qnan);
-                b[k] = R((i >= 1) ? z[k - nx] - z[k] : qnan);
-                c[k] = R(rough[k] * rough[k]);
-            }
-        upload(dzx.p, a); upload(dzy.p, b); upload(n2.p, c);
         std::vector<std::pair<int32_t, R>> outs;
         for (int o = 0; o < nout; ++o) {
             if (rows[o] < 0 || rows[o] >= ny || cols[o] < 0 || cols[o] >= nx) {
@@ -192,31 +236,48 @@ template <typename R> struct Impl : Base {
                               : std::sqrt(kG) / res;
             outs.emplace_back(int32_t(k), R(coef));
         }
+        if (size_t(outs.size()) >= (1u << 24)) { ctx->err = "too many outlet cells"; return HP2D_INVALID_ARG; }
         std::sort(outs.begin(), outs.end(), [](auto& x, auto& y) { return x.first < y.first; });
         outs.erase(std::unique(outs.begin(), outs.end(), [](auto& x, auto& y) { return x.first == y.first; }), outs.end());
         n_out = int(outs.size());
+        for (size_t k = 0; k < n; ++k) host_meta[k] &= 255u;
         std::vector<int32_t> cells(n_out);
         std::vector<R> coefs(n_out);
         std::vector<uint32_t> bits(size_t(ny) * bit_words, 0u);
         for (int o = 0; o < n_out; ++o) {
             cells[o] = outs[o].first;
             coefs[o] = outs[o].second;
+            host_meta[cells[o]] |= uint32_t(o + 1) << 8;
             int i = cells[o] / nx, j = cells[o] % nx;
             bits[size_t(i) * bit_words + (j >> 5)] |= 1u << (j & 31);
         }
+        std::vector<V4> s(n);
+        std::vector<R> a(n), b(n), c(n);
+        for (int i = 0; i < ny; ++i)
+            for (int j = 0; j < nx; ++j) {
+                size_t k = size_t(i) * nx + j;
+                a[k] = R((j + 1 < nx) ? z[k + 1] - z[k] : qnan);
+                b[k] = R((i >= 1) ? z[k - nx] - z[k] : qnan);
+                c[k] = R(rough[k] * rough[k]);
+                s[k] = V4{a[k], b[k], c[k], make_meta<R>(host_meta[k])};
+            }
+        upload(stat.p, s);
+        // structure-of-arrays copies for the unfused entry points
+        dzx.alloc(n); dzy.alloc(n); n2.alloc(n);
+        upload(dzx.p, a); upload(dzy.p, b); upload(n2.p, c);
+        outlet_bits.alloc(bits.size());
+        upload(outlet_bits.p, bits);
         outlet_cells.alloc(std::max(n_out, 1));
         outlet_coef.alloc(std::max(n_out, 1));
         hf3.alloc(std::max(n_out, 1));
         qo.alloc(std::max(n_out, 1));
-        if (n_out) {
-            HP_CK(cudaMemcpy(outlet_cells.p, cells.data(), n_out * sizeof(int32_t), cudaMemcpyHostToDevice));
-            upload(outlet_coef.p, coefs);
-        }
+        upload(outlet_cells.p, cells);
+        upload(outlet_coef.p, coefs);
         fill(hf3.p, std::max(n_out, 1), R(0));
         fill(qo.p, std::max(n_out, 1), R(0));
-        HP_CK(cudaMemcpy(outlet_bits.p, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
         static_ready = true;
         invalidate_graph();
+        dirty = true;
         return HP2D_OK;
     }
 
@@ -237,52 +298,51 @@ template <typename R> struct Impl : Base {
             t[c].minsm = R(minsm[c] / 1000.0);
             t[c].pad = R(0);
         }
-        soil.alloc(n);
         classes.alloc(ncls);
-        HP_CK(cudaMemcpy(soil.p, cls, n, cudaMemcpyHostToDevice));
-        HP_CK(cudaMemcpy(classes.p, t.data(), ncls * sizeof(SoilClass<R>), cudaMemcpyHostToDevice));
+        upload(classes.p, t);
         n_classes = ncls;
         host_soil.assign(cls, cls + n);
         host_tr.resize(ncls);
         for (int c = 0; c < ncls; ++c) host_tr[c] = t[c].tr;
-        for (int b = 0; b < 2; ++b) {
-            if (!I[b].p) { I[b].alloc(n); fill(I[b].p, n, R(0)); }
-            if (!T[b].p) { T[b].alloc(n); fill(T[b].p, n, R(0)); }
-        }
-        reset_timer();
+        for (size_t k = 0; k < n; ++k) host_meta[k] = (host_meta[k] & ~255u) | cls[k];
+        write_meta();
+        soil.alloc(n);
+        upload(soil.p, host_soil);
+        // soil records: keep I if present, recovery timer restarts at Tr
+        std::vector<V2> g(n);
+        if (gs2[0].p) g = fetch(gs2[hs.cur].p, n);
+        else for (size_t k = 0; k < n; ++k) g[k] = V2{R(0), R(0)};
+        for (size_t k = 0; k < n; ++k) g[k].y = cls[k] != 255 ? host_tr[cls[k]] : R(0);
+        for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
+        upload(gs2[hs.cur].p, g);
         invalidate_graph();
         dirty = true;
         return HP2D_OK;
     }
 
-    // recovery timer starts at Tr (HydroPol2D_Main_While_Ensemble.m:266)
-    void reset_timer() {
-        if (!T[0].p || host_soil.empty()) return;
-        std::vector<R> v(n);
-        for (size_t k = 0; k < n; ++k) v[k] = host_soil[k] != 255 ? host_tr[host_soil[k]] : R(0);
-        upload(T[hs.cur].p, v);
-    }
-    std::vector<uint8_t> host_soil;
-    std::vector<R> host_tr;
-
     hp2d_status set_state(const double* d, const double* outflow, const double* Imm) {
-        std::vector<R> a(n), b(n), c(n);
+        pull_sc();
+        std::vector<V4> x(n);
         for (size_t k = 0; k < n; ++k) {
-            a[k] = R(d[k] / 1000.0);
-            b[k] = outflow ? R(outflow[k] / 3.6e6 * res) : R(0);
-            c[k] = outflow ? R(outflow[n + k] / 3.6e6 * res) : R(0);
+            x[k].x = R(d[k] / 1000.0);
+            // outflow_bates [mm/h] -> q [m^2/s]: mm/h / 1000 / 3600 * dx (LIM_D4.m:198)
+            x[k].y = outflow ? R(outflow[k] / 3.6e6 * res) : R(0);
+            x[k].z = outflow ? R(outflow[n + k] / 3.6e6 * res) : R(0);
+            x[k].w = -std::numeric_limits<R>::infinity();
         }
-        int cur = hs.cur;
-        upload(h[cur].p, a); upload(qx[cur].p, b); upload(qy[cur].p, c);
-        if (Imm) {
-            if (!I[0].p) for (int q = 0; q < 2; ++q) { I[q].alloc(n); T[q].alloc(n); fill(T[q].p, n, R(0)); }
-            std::vector<R> v(n);
-            for (size_t k = 0; k < n; ++k) v[k] = R(Imm[k] / 1000.0);
-            upload(I[cur].p, v);
+        upload(st4[hs.cur].p, x);
+        if (Imm || gs2[0].p) {
+            for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
+            std::vector<V2> g(n);
+            std::vector<V2> old;
+            if (!Imm) old = fetch(gs2[hs.cur].p, n);
+            for (size_t k = 0; k < n; ++k) {
+                g[k].x = Imm ? R(Imm[k] / 1000.0) : old[k].x;
+                g[k].y = (!host_soil.empty() && host_soil[k] != 255) ? host_tr[host_soil[k]] : R(0);
+            }
+            upload(gs2[hs.cur].p, g);
         }
-        reset_timer();
-        reset_maxima();
-        state_ready = true;
+        fill(arrival.p, n, std::numeric_limits<R>::infinity());
         dirty = true;
         return HP2D_OK;
     }
@@ -298,10 +358,11 @@ template <typename R> struct Impl : Base {
     }
 
     hp2d_status set_rain_uniform(int32_t cnt, const double* t0, const double* rate) {
-        rain_t.alloc(std::max(cnt, 1)); rain_r.alloc(std::max(cnt, 1));
+        rain_t.alloc(std::max(cnt, 1));
+        rain_r.alloc(std::max(cnt, 1));
         if (cnt) {
-            HP_CK(cudaMemcpy(rain_t.p, t0, cnt * sizeof(double), cudaMemcpyHostToDevice));
-            HP_CK(cudaMemcpy(rain_r.p, rate, cnt * sizeof(double), cudaMemcpyHostToDevice));
+            upload(rain_t.p, std::vector<double>(t0, t0 + cnt));
+            upload(rain_r.p, std::vector<double>(rate, rate + cnt));
         }
         rain.n_uniform = cnt;
         rain.t_start = rain_t.p;
@@ -316,15 +377,13 @@ template <typename R> struct Impl : Base {
         if (nm <= 0 || my <= 0 || mx <= 0 || !(map_dt > 0)) { ctx->err = "bad rain map shape"; return HP2D_INVALID_ARG; }
         size_t cnt = size_t(nm) * my * mx;
         maps.alloc(cnt);
-        HP_CK(cudaMemcpy(maps.p, rate, cnt * sizeof(float), cudaMemcpyHostToDevice));
+        upload(maps.p, std::vector<float>(rate, rate + cnt));
         rain.n_maps = nm; rain.my = my; rain.mx = mx; rain.map_dt = map_dt; rain.maps = maps.p;
         rain.n_uniform = 0;
         invalidate_graph();
         dirty = true;
         return HP2D_OK;
     }
-
-    bool ga() const { return ctx->p.flag_infiltration == 1 && n_classes > 0; }
 
     void fold_accumulators() {
         pull_sc();
@@ -339,17 +398,40 @@ template <typename R> struct Impl : Base {
     }
 
     // ---------------- unfused entry points ----------------
+    // each call unpacks the records of the current buffer into the SoA scratch, runs
+    // the stage kernels and packs the result back
+    void ensure_scratch() {
+        if (!h.p) {
+            h.alloc(n); qx.alloc(n); qy.alloc(n); dmax.alloc(n); I.alloc(n); T.alloc(n);
+            hfx.alloc(n); hfy.alloc(n); qxu.alloc(n); qyu.alloc(n); scale.alloc(n);
+            fill(hfx.p, n, R(0));
+            fill(hfy.p, n, R(0));
+        }
+    }
+    void unpack() {
+        ensure_scratch();
+        const int cur = hs.cur;
+        k_unpack<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[cur].p, gs2[cur].p, h.p, qx.p, qy.p, dmax.p, I.p, T.p);
+        HP_CK(cudaGetLastError());
+    }
+    void pack() {
+        const int cur = hs.cur;
+        k_pack<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[cur].p, gs2[cur].p, h.p, qx.p, qy.p, dmax.p, I.p, T.p);
+        HP_CK(cudaGetLastError());
+    }
+
     hp2d_status hydrology_step(double time_step) {
         pull_sc();
         hs.acc_neg = 0;
         push_sc();
-        int cur = hs.cur;
+        unpack();
         double dts = time_step * 60.0;
-        k_hydro_rain_ga<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), hs.t_min, dts, rain, h[cur].p,
-                                                               I[cur].p, T[cur].p, soil.p, classes.p, ga() ? 1 : 0, sc.p);
+        k_hydro_rain_ga<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), hs.t_min, dts, rain, h.p, I.p, T.p, soil.p,
+                                                               classes.p, ga() ? 1 : 0, sc.p);
         HP_CK(cudaGetLastError());
-        k_hydro_clamp<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h[cur].p, sc.p);
+        k_hydro_clamp<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h.p, sc.p);
         HP_CK(cudaGetLastError());
+        pack();
         pull_sc();
         if (hs.acc_neg) hs.neg_warn += 1;
         push_sc();
@@ -358,31 +440,27 @@ template <typename R> struct Impl : Base {
         return HP2D_OK;
     }
 
-    void ensure_scratch() {
-        if (!hfx.p) { hfx.alloc(n); hfy.alloc(n); qxu.alloc(n); qyu.alloc(n); scale.alloc(n); }
-    }
-
     hp2d_status li_step(double time_step) {
-        ensure_scratch();
         pull_sc();
-        int cur = hs.cur;
+        unpack();
         double dts = time_step * 60.0;
         auto gv = view();
         int nb = blocks_for(n);
-        k_faces<R><<<nb, kThreads, 0, st()>>>(gv, dts, h[cur].p, dzx.p, dzy.p, n2.p, qx[cur].p, qy[cur].p,
-                                            hfx.p, hfy.p, qxu.p, qyu.p, ctx->p.flag_critical);
+        k_faces<R><<<nb, kThreads, 0, st()>>>(gv, dts, h.p, dzx.p, dzy.p, n2.p, qx.p, qy.p, hfx.p, hfy.p, qxu.p,
+                                            qyu.p, ctx->p.flag_critical);
         HP_CK(cudaGetLastError());
-        k_scale<R><<<nb, kThreads, 0, st()>>>(gv, dts, h[cur].p, qxu.p, qyu.p, scale.p);
+        k_scale<R><<<nb, kThreads, 0, st()>>>(gv, dts, h.p, qxu.p, qyu.p, scale.p);
         HP_CK(cudaGetLastError());
-        k_limit<R><<<nb, kThreads, 0, st()>>>(gv, qxu.p, qyu.p, scale.p, qx[cur].p, qy[cur].p);
+        k_limit<R><<<nb, kThreads, 0, st()>>>(gv, qxu.p, qyu.p, scale.p, qx.p, qy.p);
         HP_CK(cudaGetLastError());
-        k_continuity<R><<<nb, kThreads, 0, st()>>>(gv, dts, h[cur].p, qx[cur].p, qy[cur].p);
+        k_continuity<R><<<nb, kThreads, 0, st()>>>(gv, dts, h.p, qx.p, qy.p);
         HP_CK(cudaGetLastError());
         if (n_out) {
             k_outlet<R><<<(n_out + kThreads - 1) / kThreads, kThreads, 0, st()>>>(
-                gv, dts, h[cur].p, outlet_cells.p, outlet_coef.p, n_out, ctx->p.outlet_type, hf3.p, qo.p, sc.p);
+                gv, dts, h.p, outlet_cells.p, outlet_coef.p, n_out, ctx->p.outlet_type, hf3.p, qo.p, sc.p);
             HP_CK(cudaGetLastError());
         }
+        pack();
         last_dt_s = dts;
         fold_accumulators();
         dirty = true;
@@ -390,32 +468,21 @@ template <typename R> struct Impl : Base {
     }
 
     hp2d_status cfl_dt(double* ts_out, double* vmax_out) {
-        if (!hfx.p) { ctx->err = "hp2d_cfl_dt needs a preceding hp2d_li_step"; return HP2D_NOT_READY; }
+        if (!(last_dt_s > 0)) { ctx->err = "hp2d_cfl_dt needs a preceding hp2d_li_step"; return HP2D_NOT_READY; }
         pull_sc();
         hs.acc_vmax = hs.acc_cmax = 0;
         push_sc();
-        int cur = hs.cur;
-        k_cfl<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), last_dt_s, qx[cur].p, qy[cur].p, hfx.p, hfy.p,
-                                                     outlet_bits.p, bit_words, outlet_cells.p, hf3.p, n_out,
+        unpack();
+        k_cfl<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), last_dt_s, qx.p, qy.p, hfx.p, hfy.p, outlet_bits.p,
+                                                     bit_words, outlet_cells.p, hf3.p, n_out,
                                                      ctx->p.flag_adaptive_timestepping, sc.p);
         HP_CK(cudaGetLastError());
         pull_sc();
         const bool is_d = sizeof(R) == 8;
         double vm = from_ord(hs.acc_vmax, is_d), cm = from_ord(hs.acc_cmax, is_d);
         const hp2d_params& p = ctx->p;
-        double dt_adv;
-        if (vm > 0) {
-            dt_adv = 1.0 * res / std::fmax(vm, 1e-10);
-            double tsf = std::fmax(p.alfa_max - 2.0 * std::fmax(vm - 5.0, 0.0), p.alfa_min);
-            dt_adv = std::fmin(dt_adv * tsf, p.max_time_step);
-        } else {
-            dt_adv = p.max_time_step;
-        }
-        double dt_wave = cm > 0 ? (p.alfa_min * res) / cm : p.max_time_step;
-        double nw = p.flag_timestep == 1 ? std::fmin(dt_adv, dt_wave) : dt_wave;
-        if (std::isnan(nw) || std::isinf(nw)) nw = p.max_time_step;
-        double tcr = std::fmax(p.time_step_increments * std::floor(nw / p.time_step_increments), p.min_time_step);
-        tcr = std::fmin(tcr, p.max_time_step);
+        double tcr = finalize_dt(vm, cm, res, p.alfa_min, p.alfa_max, p.min_time_step, p.max_time_step,
+                                 p.time_step_increments, p.flag_timestep);
         hs.acc_vmax = hs.acc_cmax = 0;
         hs.vmax_last = vm;
         if (tcr == p.min_time_step) hs.unstable += 1;
@@ -426,10 +493,12 @@ template <typename R> struct Impl : Base {
     }
 
     hp2d_status track_maxima(double t_end) {
-        int cur = hs.cur;
+        pull_sc();
+        unpack();
         R thr = R(ctx->p.arrival_threshold / 1000.0);
-        k_track<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h[cur].p, dmax.p, arrival.p, thr, R(t_end * 60.0));
+        k_track<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h.p, dmax.p, arrival.p, thr, R(t_end * 60.0));
         HP_CK(cudaGetLastError());
+        pack();
         HP_CK(cudaStreamSynchronize(st()));
         return HP2D_OK;
     }
@@ -445,26 +514,25 @@ template <typename R> struct Impl : Base {
         a.tsc = p.time_step_change; a.alfa_min = p.alfa_min; a.alfa_max = p.alfa_max;
         a.flag_timestep = p.flag_timestep; a.adaptive = p.flag_adaptive_timestepping;
         a.flag_critical = p.flag_critical; a.outlet_type = p.outlet_type; a.ga = ga() ? 1 : 0;
-        constexpr int BY = fused_by<R>(), BX = fused_bx<R>();
-        a.n_ctas = unsigned((nx + BX - 1) / BX) * unsigned((ny + BY - 1) / BY);
-        a.dzx = dzx.p; a.dzy = dzy.p; a.n2 = n2.p;
-        a.soil = soil.p; a.classes = classes.p;
-        a.outlet_bits = outlet_bits.p; a.bit_words = bit_words;
+        a.n_strips = (nx + kStripOut - 1) / kStripOut;
+        a.rows_per_warp = rows_per_warp;
+        a.n_warps_total = a.n_strips * ((ny + rows_per_warp - 1) / rows_per_warp);
+        a.n_ctas = unsigned((a.n_warps_total + kThreads / 32 - 1) / (kThreads / 32));
+        a.stag_s2 = stagnant_threshold<R>();
+        a.stat = stat.p;
+        a.st0 = st4[0].p; a.st1 = st4[1].p;
+        a.gs0 = gs2[0].p; a.gs1 = gs2[1].p;
+        a.classes = classes.p;
         a.outlet_cells = outlet_cells.p; a.outlet_coef = outlet_coef.p; a.n_outlets = n_out;
         a.hf3 = hf3.p; a.qo = qo.p;
-        a.h0 = h[0].p; a.h1 = h[1].p; a.qx0 = qx[0].p; a.qx1 = qx[1].p; a.qy0 = qy[0].p; a.qy1 = qy[1].p;
-        a.I0 = I[0].p; a.I1 = I[1].p; a.T0 = T[0].p; a.T1 = T[1].p;
-        a.dmax = dmax.p; a.arrival = arrival.p;
+        a.arrival = arrival.p;
         a.rain = rain;
         a.sc = sc.p;
         return a;
     }
 
     void launch_fused(const FusedArgs<R>& a) {
-        constexpr int BY = fused_by<R>(), BX = fused_bx<R>();
-        using SM = FusedSmem<R, BY, BX>;
-        dim3 grid((nx + BX - 1) / BX, (ny + BY - 1) / BY);
-        k_fused_step<R, BY, BX, kThreads><<<grid, kThreads, SM::bytes, st()>>>(a);
+        k_fused_step<R, kThreads><<<a.n_ctas, kThreads, 0, st()>>>(a);
     }
 
     void invalidate_graph() {
@@ -481,7 +549,7 @@ template <typename R> struct Impl : Base {
         hs.acc_vmax = hs.acc_cmax = 0;
         hs.acc_rain = hs.acc_inf = hs.acc_out = 0;
         push_sc();
-        k_skip_flag<R><<<blocks_for(n), kThreads, 0, st()>>>(h[hs.cur].p, ny, nx, rain, soil.p, ga() ? 1 : 0, res,
+        k_skip_flag<R><<<blocks_for(n), kThreads, 0, st()>>>(st4[hs.cur].p, stat.p, ny, nx, rain, ga() ? 1 : 0, res,
                                                            ctx->p.depth_tolerance, ctx->p.arrival_threshold, sc.p);
         HP_CK(cudaGetLastError());
         dirty = false;
@@ -548,63 +616,67 @@ template <typename R> struct Impl : Base {
     }
 
     // ---------------- outputs ----------------
+    std::vector<V4> fetch_state() {
+        pull_sc();
+        return fetch(st4[hs.cur].p, n);
+    }
+
     hp2d_status download(int32_t field, double* out, size_t count) {
         if (count != n) { ctx->err = "count must be ny*nx"; return HP2D_INVALID_ARG; }
-        pull_sc();
-        int cur = hs.cur;
         const double to_mmh = 3.6e6 / res;
-        auto per_outlet_map = [&](const Dev<R>& src, double scale) {
+        auto per_outlet_map = [&](const Dev<R>& src, double scale_) {
             std::fill(out, out + n, 0.0);
             if (!n_out) return;
-            std::vector<int32_t> cells(n_out);
-            HP_CK(cudaMemcpy(cells.data(), outlet_cells.p, n_out * sizeof(int32_t), cudaMemcpyDeviceToHost));
-            auto v = fetch(src.p, n_out);
-            for (int o = 0; o < n_out; ++o) out[cells[o]] = double(v[o]) * scale;
+            auto cells = fetch(outlet_cells.p, size_t(n_out));
+            auto v = fetch(src.p, size_t(n_out));
+            for (int o = 0; o < n_out; ++o) out[cells[o]] = double(v[o]) * scale_;
         };
         switch (field) {
-            case HP2D_FIELD_DEPTH: { auto v = fetch(h[cur].p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0; break; }
-            case HP2D_FIELD_QOUT_RIGHT: { auto v = fetch(qx[cur].p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * to_mmh; break; }
-            case HP2D_FIELD_QOUT_UP: { auto v = fetch(qy[cur].p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * to_mmh; break; }
+            case HP2D_FIELD_DEPTH: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].x) * 1000.0; break; }
+            case HP2D_FIELD_QOUT_RIGHT: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].y) * to_mmh; break; }
+            case HP2D_FIELD_QOUT_UP: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].z) * to_mmh; break; }
             case HP2D_FIELD_QOUT_LEFT: {
-                auto v = fetch(qx[cur].p, n);
+                auto v = fetch_state();
                 for (int i = 0; i < ny; ++i)
-                    for (int j = 0; j < nx; ++j) out[size_t(i) * nx + j] = j == 0 ? -0.0 : -double(v[size_t(i) * nx + j - 1]) * to_mmh;
+                    for (int j = 0; j < nx; ++j)
+                        out[size_t(i) * nx + j] = j == 0 ? -0.0 : -double(v[size_t(i) * nx + j - 1].y) * to_mmh;
                 break;
             }
             case HP2D_FIELD_QOUT_DOWN: {
-                auto v = fetch(qy[cur].p, n);
+                auto v = fetch_state();
                 for (int i = 0; i < ny; ++i)
-                    for (int j = 0; j < nx; ++j) out[size_t(i) * nx + j] = i + 1 == ny ? -0.0 : -double(v[size_t(i + 1) * nx + j]) * to_mmh;
+                    for (int j = 0; j < nx; ++j)
+                        out[size_t(i) * nx + j] = i + 1 == ny ? -0.0 : -double(v[size_t(i + 1) * nx + j].z) * to_mmh;
                 break;
             }
             case HP2D_FIELD_OUTLET_FLOW: per_outlet_map(qo, 3.6e6); break;
             case HP2D_FIELD_HF_X: case HP2D_FIELD_HF_Y: {
-                if (!hfx.p) { ctx->err = "Hf is materialised by hp2d_li_step only"; return HP2D_NOT_READY; }
+                if (!(last_dt_s > 0)) { ctx->err = "Hf is materialised by hp2d_li_step only"; return HP2D_NOT_READY; }
                 auto v = fetch(field == HP2D_FIELD_HF_X ? hfx.p : hfy.p, n);
                 for (size_t k = 0; k < n; ++k) out[k] = double(v[k]);
                 break;
             }
             case HP2D_FIELD_HF_OUTLET: per_outlet_map(hf3, 1.0); break;
-            case HP2D_FIELD_DMAX: { auto v = fetch(dmax.p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0; break; }
+            case HP2D_FIELD_DMAX: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].w) * 1000.0; break; }
             case HP2D_FIELD_ARRIVAL: { auto v = fetch(arrival.p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) / 60.0; break; }
             case HP2D_FIELD_SOIL_STORAGE: {
-                if (!I[cur].p) { ctx->err = "no soil storage (hp2d_set_soil not called)"; return HP2D_NOT_READY; }
-                auto v = fetch(I[cur].p, n);
-                for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0;
+                if (!gs2[0].p) { ctx->err = "no soil storage (hp2d_set_soil not called)"; return HP2D_NOT_READY; }
+                pull_sc();
+                auto v = fetch(gs2[hs.cur].p, n);
+                for (size_t k = 0; k < n; ++k) out[k] = double(v[k].x) * 1000.0;
                 break;
             }
             case HP2D_FIELD_I_TOT_END_CELL: {
-                auto a = fetch(qx[cur].p, n), b = fetch(qy[cur].p, n);
+                auto v = fetch_state();
                 std::vector<double> of(n, 0.0);
                 if (n_out) {
-                    std::vector<int32_t> cells(n_out);
-                    HP_CK(cudaMemcpy(cells.data(), outlet_cells.p, n_out * sizeof(int32_t), cudaMemcpyDeviceToHost));
-                    auto v = fetch(qo.p, n_out);
-                    for (int o = 0; o < n_out; ++o) of[cells[o]] = double(v[o]) * 3.6e6;
+                    auto cells = fetch(outlet_cells.p, size_t(n_out));
+                    auto q = fetch(qo.p, size_t(n_out));
+                    for (int o = 0; o < n_out; ++o) of[cells[o]] = double(q[o]) * 3.6e6;
                 }
                 double dts = last_dt_s > 0 ? last_dt_s : hs.time_step * 60.0;
                 for (size_t k = 0; k < n; ++k)
-                    out[k] = std::fabs(double(a[k]) * to_mmh + double(b[k]) * to_mmh + of[k]) * dts / 1000.0 / 3600.0 * res * res;
+                    out[k] = std::fabs(double(v[k].y) * to_mmh + double(v[k].z) * to_mmh + of[k]) * dts / 1000.0 / 3600.0 * res * res;
                 break;
             }
             default: ctx->err = "unknown field"; return HP2D_INVALID_ARG;
@@ -613,29 +685,36 @@ template <typename R> struct Impl : Base {
     }
 
     hp2d_status download_native(int32_t field, void* out, size_t bytes) {
-        pull_sc();
-        int cur = hs.cur;
-        const R* src = nullptr;
-        size_t cnt = n;
-        switch (field) {
-            case 0: src = h[cur].p; break;
-            case 1: src = qx[cur].p; break;
-            case 2: src = qy[cur].p; break;
-            case 3: src = I[cur].p; break;
-            case 4: src = T[cur].p; break;
-            case 5: src = dmax.p; break;
-            case 6: src = arrival.p; break;
-            case 7: src = hfx.p; break;
-            case 8: src = hfy.p; break;
-            case 9: src = hf3.p; cnt = size_t(n_out); break;
-            case 10: src = qo.p; cnt = size_t(n_out); break;
-            default: ctx->err = "unknown native field"; return HP2D_INVALID_ARG;
-        }
-        if (!src) { ctx->err = "field not materialised"; return HP2D_NOT_READY; }
+        size_t cnt = (field == 9 || field == 10) ? size_t(n_out) : n;
         if (bytes != cnt * sizeof(R)) { ctx->err = "byte count mismatch"; return HP2D_INVALID_ARG; }
-        if (cnt) {
-            HP_CK(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, st()));
-            HP_CK(cudaStreamSynchronize(st()));
+        R* o = static_cast<R*>(out);
+        switch (field) {
+            case 0: case 1: case 2: case 5: {
+                auto v = fetch_state();
+                for (size_t k = 0; k < n; ++k)
+                    o[k] = field == 0 ? v[k].x : field == 1 ? v[k].y : field == 2 ? v[k].z : v[k].w;
+                break;
+            }
+            case 3: case 4: {
+                if (!gs2[0].p) { ctx->err = "no soil records"; return HP2D_NOT_READY; }
+                pull_sc();
+                auto v = fetch(gs2[hs.cur].p, n);
+                for (size_t k = 0; k < n; ++k) o[k] = field == 3 ? v[k].x : v[k].y;
+                break;
+            }
+            case 6: { auto v = fetch(arrival.p, n); std::copy(v.begin(), v.end(), o); break; }
+            case 7: case 8: {
+                if (!hfx.p) { ctx->err = "Hf is materialised by hp2d_li_step only"; return HP2D_NOT_READY; }
+                auto v = fetch(field == 7 ? hfx.p : hfy.p, n);
+                std::copy(v.begin(), v.end(), o);
+                break;
+            }
+            case 9: case 10: {
+                auto v = fetch(field == 9 ? hf3.p : qo.p, cnt);
+                std::copy(v.begin(), v.end(), o);
+                break;
+            }
+            default: ctx->err = "unknown native field"; return HP2D_INVALID_ARG;
         }
         return HP2D_OK;
     }
@@ -658,7 +737,7 @@ template <typename R> struct Impl : Base {
     hp2d_status stored_volume(double* v) {
         pull_sc();
         HP_CK(cudaMemsetAsync(vol.p, 0, sizeof(double), st()));
-        k_volume<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h[hs.cur].p, vol.p);
+        k_volume4<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, vol.p);
         HP_CK(cudaGetLastError());
         double s = 0;
         HP_CK(cudaMemcpyAsync(&s, vol.p, sizeof(double), cudaMemcpyDeviceToHost, st()));
@@ -689,12 +768,6 @@ template <typename F> hp2d_status with_impl(hp2d_ctx* ctx, F&& fn) {
     });
 }
 
-template <typename R> void set_smem_attr() {
-    constexpr int BY = fused_by<R>(), BX = fused_bx<R>();
-    using SM = FusedSmem<R, BY, BX>;
-    HP_CK(cudaFuncSetAttribute(k_fused_step<R, BY, BX, kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(SM::bytes)));
-}
 
 }  // namespace
 
@@ -736,10 +809,8 @@ hp2d_status hp2d_create(const hp2d_grid* grid, const hp2d_params* params, int32_
         HP_CK(cudaSetDevice(device));
         HP_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         if (grid->precision == HP2D_FP32) {
-            set_smem_attr<float>();
             ctx->impl.reset(new Impl<float>(ctx));
         } else {
-            set_smem_attr<double>();
             ctx->impl.reset(new Impl<double>(ctx));
         }
     } catch (const CudaFail& f) {
@@ -830,6 +901,15 @@ hp2d_status hp2d_fused_steps(hp2d_ctx* ctx, int32_t nsteps) {
 hp2d_status hp2d_fused_steps_timed(hp2d_ctx* ctx, int32_t nsteps, float* elapsed_ms) {
     if (nsteps < 0 || !elapsed_ms) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.fused_steps_timed(nsteps, elapsed_ms); });
+}
+
+hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp) {
+    if (rows_per_warp < 4) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) {
+        m.rows_per_warp = rows_per_warp;
+        m.invalidate_graph();
+        return HP2D_OK;
+    });
 }
 
 hp2d_status hp2d_run(hp2d_ctx* ctx, int64_t max_steps, int64_t* steps_done) {

@@ -129,6 +129,44 @@ __host__ __device__ inline double from_ord(unsigned long long b, bool is_double)
     return (double)f;
 }
 
+// ---------------- vectorised cell records ---------------------------------------------
+// static record  {dz_x, dz_y, n^2, meta}: meta holds, in the bits of the last element,
+//                the soil class (bits 0-7, 255 = no soil) and outlet ordinal + 1 (bits
+//                8-31, 0 = not an outlet cell)
+// state record   {h, q_x, q_y, dmax}, double-buffered
+// soil record    {I, T}, double-buffered (Green-Ampt runs only)
+template <typename R> struct Vec;
+template <> struct Vec<float> {
+    using V4 = float4;
+    using V2 = float2;
+};
+template <> struct Vec<double> {
+    using V4 = double4;
+    using V2 = double2;
+};
+__host__ __device__ inline unsigned meta_bits(float v) {
+    unsigned u;
+    memcpy(&u, &v, 4);
+    return u;
+}
+__host__ __device__ inline unsigned meta_bits(double v) {
+    unsigned long long u;
+    memcpy(&u, &v, 8);
+    return unsigned(u);
+}
+template <typename R> __host__ __device__ inline R make_meta(unsigned m);
+template <> __host__ __device__ inline float make_meta<float>(unsigned m) {
+    float f;
+    memcpy(&f, &m, 4);
+    return f;
+}
+template <> __host__ __device__ inline double make_meta<double>(unsigned m) {
+    unsigned long long u = m;
+    double d;
+    memcpy(&d, &u, 8);
+    return d;
+}
+
 // ---------------- Green-Ampt soil class table -----------------------------------------
 template <typename R> struct SoilClass {
     R ks, psi, dth, lu, kout, tr, minsm, pad;

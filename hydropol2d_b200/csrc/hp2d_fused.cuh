@@ -3,13 +3,26 @@
 // continuity, outlet sink, running maximum / arrival time, CFL reductions, and the
 // timestep refresh + clock advance done by the last CTA to finish).
 //
-// Tiling: each CTA owns a BY x BX block of cells.  The draining limiter makes a cell's
-// new depth depend on cells two away (face <- donor scale <- donor's four faces <- their
-// far cells), so the CTA stages a (BY+4) x (BX+4) depth tile (hydrology applied in
-// place), computes the faces touching cells within one cell of the block, the donor
-// scales within one cell, the limited faces of the block, and the block's continuity.
-// All of that lives in shared memory; the only global traffic is one read of each input
-// field and one write of each output field (halo reads mostly hit L2).
+// Warp-streaming layout.  Each warp owns a strip of 32 columns, of which lanes 2..29
+// (28 columns) are its output, and walks down a block of rows.  The draining limiter
+// makes a cell's new depth depend on cells two away (face <- donor scale <- donor's four
+// faces <- their far cells); in x those neighbours come from other lanes by warp shuffles
+// (hence the two-lane apron on each side), in y from a rolling window of registers that
+// holds the previous two rows.  Per row a lane does: hydrology of (r, j), the x face
+// (r, j) and y face (r-1|r, j), the donor scale of (r-1, j), the limited faces of row
+// r-1 and the continuity / outlet / maxima / CFL of row r-2.  No shared memory, no
+// barrier inside the row loop.
+//
+// Memory: a cell is two 16-byte records read with one vector load each -- the static
+// {dz_x, dz_y, n^2, meta} and the state {h, q_x, q_y, dmax} -- and one state record
+// written; a warp row is 512 contiguous bytes.  The row loop is software-pipelined:
+// the records of row r+1 are requested before row r is computed.
+//
+// CFL reductions: the step needs max(speed) and, over non-stagnant cells, max of the wave
+// celerity sqrt(g*depth).  Because IEEE sqrt is correctly rounded and monotone, max of
+// sqrt(x_i) equals sqrt(max x_i) exactly, so the kernel reduces speed^2 and g*depth and
+// takes one square root at the end; the stagnant test speed < 0.01 becomes
+// speed^2 < stag_s2 with stag_s2 the smallest value whose rounded root reaches 0.01.
 //
 // The state is double-buffered (StepScalars::cur selects the read side), so a CUDA graph
 // of many launches needs no host involvement, and a launch after the end of the
@@ -20,28 +33,34 @@
 
 namespace hp2d {
 
+constexpr int kStripOut = 28;   // output columns of a 32-lane strip (lanes 2..29)
+
 template <typename R> struct FusedArgs {
+    using V4 = typename Vec<R>::V4;
+    using V2 = typename Vec<R>::V2;
     int ny, nx;
+    int n_strips, rows_per_warp, n_warps_total;
     double res;
     double tol_mm, thr_mm;
     double t_end;                // routing_time + min_time_step/60 [min]
     double min_dt, max_dt, inc, tsc, alfa_min, alfa_max;
     int flag_timestep, adaptive, flag_critical, outlet_type, ga;
     unsigned int n_ctas;
-    const R* dzx; const R* dzy; const R* n2;
-    const uint8_t* soil; const SoilClass<R>* classes;
-    const uint32_t* outlet_bits; int bit_words;   // words per row
+    R stag_s2;
+    const V4* stat;
+    V4* st0; V4* st1;            // state records, double buffer
+    V2* gs0; V2* gs1;            // soil records, double buffer
+    const SoilClass<R>* classes;
     const int32_t* outlet_cells; const R* outlet_coef; int n_outlets;
     R* hf3; R* qo;
-    R* h0; R* h1; R* qx0; R* qx1; R* qy0; R* qy1; R* I0; R* I1; R* T0; R* T1;
-    R* dmax; R* arrival;
+    R* arrival;
     RainDesc rain;
     StepScalars* sc;
 };
 
-__device__ inline double finalize_dt(double vmax, double cmax, double res, double alfa_min,
-                                     double alfa_max, double min_dt, double max_dt, double inc,
-                                     int flag_timestep) {
+__device__ __host__ inline double finalize_dt(double vmax, double cmax, double res, double alfa_min,
+                                              double alfa_max, double min_dt, double max_dt, double inc,
+                                              int flag_timestep) {
     double dt_adv;
     if (vmax > 0) {
         dt_adv = 1.0 * res / fmax(vmax, 1e-10);
@@ -62,38 +81,42 @@ template <typename R> __device__ __forceinline__ R warp_max(R v) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
+__device__ __forceinline__ unsigned long long warp_max_u(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
-template <typename R, int BY, int BX>
-struct FusedSmem {
-    static constexpr int HH = BY + 4, HW = BX + 4;   // depth tile, origin (r0-2, c0-2)
-    static constexpr int XH = BY + 2, XW = BX + 3;   // x faces, origin (r0-1, c0-2)
-    static constexpr int YH = BY + 3, YW = BX + 2;   // y faces, origin (r0-1, c0-1)
-    static constexpr int SH = BY + 2, SW = BX + 2;   // donor scale, origin (r0-1, c0-1)
-    static constexpr size_t n_elems = size_t(HH) * HW + 2 * size_t(XH) * XW + 2 * size_t(YH) * YW + size_t(SH) * SW;
-    static constexpr size_t bytes = n_elems * sizeof(R);
-};
+template <typename R> __device__ __forceinline__ R bits_to(unsigned long long b);
+template <> __device__ __forceinline__ float bits_to<float>(unsigned long long b) { return __uint_as_float((unsigned)b); }
+template <> __device__ __forceinline__ double bits_to<double>(unsigned long long b) { return __longlong_as_double((long long)b); }
 
-template <typename R, int BY, int BX, int NT>
-__global__ void __launch_bounds__(NT) k_fused_step(const FusedArgs<R> a) {
-    using SM = FusedSmem<R, BY, BX>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* sH = reinterpret_cast<R*>(smem_raw);
-    R* sQx = sH + SM::HH * SM::HW;
-    R* sHx = sQx + SM::XH * SM::XW;
-    R* sQy = sHx + SM::XH * SM::XW;
-    R* sHy = sQy + SM::YH * SM::YW;
-    R* sS = sHy + SM::YH * SM::YW;
+// resident CTAs per SM the register budget is sized for (float: 8 x 128 threads)
+#ifndef HP2D_MINB_F32
+#define HP2D_MINB_F32 7
+#endif
+template <typename R> struct FusedOcc { static constexpr int minb = HP2D_MINB_F32; };
+template <> struct FusedOcc<double> { static constexpr int minb = 3; };
 
-    __shared__ StepConsts<R> K;
+template <typename R, int NT>
+__global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const FusedArgs<R> a) {
+    using V4 = typename Vec<R>::V4;
+    using V2 = typename Vec<R>::V2;
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ StepConsts<R> s_K;
     __shared__ double s_tmin, s_dts;
     __shared__ int s_cur, s_skip, s_done, s_map, s_last;
     __shared__ R s_rain;
-    __shared__ R red_r[2][NT / 32];
+    __shared__ R red_s2[NT / 32];
+    __shared__ unsigned long long red_c[NT / 32];
     __shared__ double red_d[3][NT / 32];
 
     const int tid = threadIdx.x;
@@ -104,196 +127,214 @@ __global__ void __launch_bounds__(NT) k_fused_step(const FusedArgs<R> a) {
         s_cur = sc->cur;
         s_skip = sc->skip_clamp;
         s_done = !(s_tmin <= a.t_end);
-        K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
+        s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
         s_rain = a.rain.n_uniform ? R(uniform_rate(a.rain, s_tmin)) : R(0);
         s_map = a.rain.n_maps ? map_index(a.rain, s_tmin) : -1;
-        if (!s_done && s_skip && blockIdx.x == 0 && blockIdx.y == 0) sc->neg_warn += 1;
+        if (!s_done && s_skip && blockIdx.x == 0) sc->neg_warn += 1;
     }
     __syncthreads();
     if (s_done) return;
 
+    const StepConsts<R> K = s_K;
     const int ny = a.ny, nx = a.nx;
-    const int r0 = blockIdx.y * BY, c0 = blockIdx.x * BX;
     const int cur = s_cur;
-    const R* hin = cur ? a.h1 : a.h0;
-    const R* qxin = cur ? a.qx1 : a.qx0;
-    const R* qyin = cur ? a.qy1 : a.qy0;
-    const R* Iin = cur ? a.I1 : a.I0;
-    const R* Tin = cur ? a.T1 : a.T0;
-    R* hout = cur ? a.h0 : a.h1;
-    R* qxout = cur ? a.qx0 : a.qx1;
-    R* qyout = cur ? a.qy0 : a.qy1;
-    R* Iout = cur ? a.I0 : a.I1;
-    R* Tout = cur ? a.T0 : a.T1;
+    const bool skip = s_skip != 0;
+    const R rain_u = s_rain;
+    const V4* __restrict__ sin = cur ? a.st1 : a.st0;
+    V4* __restrict__ sout = cur ? a.st0 : a.st1;
+    const V2* __restrict__ gin = cur ? a.gs1 : a.gs0;
+    V2* __restrict__ gout = cur ? a.gs0 : a.gs1;
+    const V4* __restrict__ stat = a.stat;
     const float* map = s_map >= 0 ? a.rain.maps + size_t(s_map) * a.rain.my * a.rain.mx : nullptr;
+    const R t_arr = R(s_tmin * 60.0 + s_dts);
+    const R NaNR = R(__int_as_float(0x7fc00000));
+
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wg = blockIdx.x * (NT / 32) + warp;
 
     double rain_acc = 0.0, inf_acc = 0.0, out_acc = 0.0;
+    R s2max = R(0);
+    unsigned long long cenc = 0ull;   // 0: no non-stagnant cell; else bits(value) + 1
 
-    // ---- phase 0: depth tile with rain, Green-Ampt and the clamp ----------------------
-    for (int e = tid; e < SM::HH * SM::HW; e += NT) {
-        const int li = e / SM::HW, lj = e - li * SM::HW;
-        const int i = r0 - 2 + li, j = c0 - 2 + lj;
-        R hh = R(0);
-        if (i >= 0 && i < ny && j >= 0 && j < nx) {
-            const size_t c = size_t(i) * nx + j;
-            const bool own = li >= 2 && li < BY + 2 && lj >= 2 && lj < BX + 2;
-            hh = hin[c];
-            const R rate = map ? map_rate<R>(a.rain, map, i, j, ny, nx) : s_rain;
-            const R r = rate * K.rain_scale;
-            hh = hh + r;
-            if (own && isfinite(hh)) rain_acc += double(r);
-            if (a.ga) {
-                const uint8_t s = a.soil[c];
-                if (s != 255) {
-                    R Ic = Iin[c], Tc = Tin[c];
-                    const R fd = green_ampt(hh, Ic, Tc, a.classes[s], K);
-                    if (own) {
-                        Iout[c] = Ic;
-                        Tout[c] = Tc;
-                        if (isfinite(fd)) inf_acc += double(fd);
-                    }
-                } else if (own) {
-                    Iout[c] = Iin[c];
-                    Tout[c] = Tin[c];
+    if (wg < a.n_warps_total) {
+        const int strip = wg % a.n_strips;
+        const int rb = wg / a.n_strips;
+        const int j = strip * kStripOut - 2 + lane;
+        const bool col_ok = j >= 0 && j < nx;
+        const bool own_lane = lane >= 2 && lane < 30 && j < nx;
+        const int r0 = rb * a.rows_per_warp;
+        const int r_end = min(r0 + a.rows_per_warp, ny);
+
+        // rolling window (suffix = rows back)
+        R hT1 = R(0), hT2 = R(0);
+        R qxu1 = R(0), qyu1 = R(0);
+        R hfx1 = R(0), hfx2 = R(0), hfy1 = R(0), hfy2 = R(0);
+        R sc2 = R(1);
+        R qxl2 = R(0), qyl2 = R(0);
+        R dm1 = R(0), dm2 = R(0);
+        unsigned mt1 = 0u, mt2 = 0u;
+
+        // software pipeline: the records of row r+1 are requested before row r is computed
+        const V4 zero4 = {R(0), R(0), R(0), R(0)};
+        const V4 closed4 = {NaNR, NaNR, R(0), R(0)};
+        const V2 zero2 = {R(0), R(0)};
+        V4 nS = closed4, nX = zero4;
+        V2 nG = zero2;
+        {
+            const int rr = r0 - 2;
+            if (col_ok && rr >= 0 && rr < ny) {
+                const size_t c = size_t(rr) * nx + j;
+                nS = stat[c];
+                nX = sin[c];
+                if (a.ga) nG = gin[c];
+            }
+        }
+        for (int r = r0 - 2; r < r_end + 2; ++r) {
+            const V4 S = nS, X = nX;
+            const V2 Gs = nG;
+            {
+                const int rr = r + 1;
+                nS = closed4;
+                nX = zero4;
+                if (col_ok && rr >= 0 && rr < ny) {
+                    const size_t cn = size_t(rr) * nx + j;
+                    nS = stat[cn];
+                    nX = sin[cn];
+                    if (a.ga) nG = gin[cn];
                 }
             }
-            if (!s_skip && hh < R(1e-9)) hh = R(0);
-            if (hh < R(0)) hh = R(0);
-        }
-        sH[li * SM::HW + lj] = hh;
-    }
-    __syncthreads();
-
-    // ---- phase 1: unlimited face fluxes ----------------------------------------------
-    for (int e = tid; e < SM::XH * SM::XW; e += NT) {
-        const int li = e / SM::XW, lj = e - li * SM::XW;
-        const int i = r0 - 1 + li, j = c0 - 2 + lj;
-        R Hf = R(0), q = R(0);
-        if (i >= 0 && i < ny && j >= 0 && j < nx) {
-            const size_t c = size_t(i) * nx + j;
-            const R dz = a.dzx[c];
-            if (!isnan(dz)) {
-                const R ha = sH[(li + 1) * SM::HW + lj], hb = sH[(li + 1) * SM::HW + lj + 1];
-                face_flux<R, true>(ha, hb, dz, qxin[c], a.n2[c], K, a.flag_critical, Hf, q);
+            const bool ok = col_ok && r >= 0 && r < ny;
+            const size_t c = size_t(r) * nx + j;
+            const unsigned meta = meta_bits(S.w);
+            // (A) hydrology of (r, j)
+            R hT0 = R(0);
+            if (ok) {
+                R hh = X.x;
+                const R rate = map ? map_rate<R>(a.rain, map, r, j, ny, nx) : rain_u;
+                const R rr = rate * K.rain_scale;
+                hh = hh + rr;
+                const bool own = own_lane && r >= r0 && r < r_end;
+                if (own && isfinite(hh)) rain_acc += double(rr);
+                if (a.ga) {
+                    const unsigned s = meta & 255u;
+                    V2 go = Gs;
+                    if (s != 255u) {
+                        R Ic = Gs.x, Tc = Gs.y;
+                        const R fd = green_ampt(hh, Ic, Tc, a.classes[s], K);
+                        go.x = Ic;
+                        go.y = Tc;
+                        if (own && isfinite(fd)) inf_acc += double(fd);
+                    }
+                    if (own) gout[c] = go;
+                }
+                if (!skip && hh < R(1e-9)) hh = R(0);
+                if (hh < R(0)) hh = R(0);
+                hT0 = hh;
             }
-        }
-        sQx[e] = q;
-        sHx[e] = Hf;
-    }
-    for (int e = tid; e < SM::YH * SM::YW; e += NT) {
-        const int li = e / SM::YW, lj = e - li * SM::YW;
-        const int i = r0 - 1 + li, j = c0 - 1 + lj;
-        R Hf = R(0), q = R(0);
-        if (i >= 0 && i < ny && j >= 0 && j < nx) {
-            const size_t c = size_t(i) * nx + j;
-            const R dz = a.dzy[c];
-            if (!isnan(dz)) {
-                const R ha = sH[li * SM::HW + lj + 1], hb = sH[(li + 1) * SM::HW + lj + 1];
-                face_flux<R, false>(ha, hb, dz, qyin[c], a.n2[c], K, a.flag_critical, Hf, q);
+            // (B) x face (r, j) between (r, j) and (r, j+1)
+            const R hR = __shfl_down_sync(FULL, hT0, 1);
+            R qxu0 = R(0), hfx0 = R(0);
+            if (ok && !isnan(S.x)) face_flux<R, true>(hT0, hR, S.x, X.y, S.z, K, a.flag_critical, hfx0, qxu0);
+            // (C) y face (r, j) between (r-1, j) and (r, j)
+            R qyu0 = R(0), hfy0 = R(0);
+            if (ok && r >= r0 - 1 && !isnan(S.y))
+                face_flux<R, false>(hT1, hT0, S.y, X.z, S.z, K, a.flag_critical, hfy0, qyu0);
+            // (D) donor scale of (r-1, j)
+            const R qxu1_left = __shfl_up_sync(FULL, qxu1, 1);
+            R sc1 = R(1);
+            if (col_ok && r >= r0 && r - 1 >= 0 && r - 1 < ny) sc1 = donor_scale(qxu1, qxu1_left, qyu1, qyu0, hT1, K);
+            // (E) limited faces of row r-1
+            const R sc1_right = __shfl_down_sync(FULL, sc1, 1);
+            const R qxl1 = limit_face(qxu1, sc1, sc1_right);
+            const R qyl1 = limit_face(qyu1, sc1, sc2);
+            // (F) continuity, outlet, maxima and CFL of row r-2
+            const R qxl2_left = __shfl_up_sync(FULL, qxl2, 1);
+            const int rm2 = r - 2;
+            if (own_lane && rm2 >= r0 && rm2 < r_end) {
+                const size_t c2 = size_t(rm2) * nx + j;
+                R hn = continuity(hT2, qxl2_left, qxl2, qyl2, qyl1, K);
+                R hf3 = R(0);
+                const unsigned ord = mt2 >> 8;
+                if (ord) {
+                    const int o = int(ord) - 1;
+                    R ho;
+                    const R qq = outlet_sink(hn, a.outlet_coef[o], a.outlet_type, K, ho);
+                    hf3 = ho;
+                    a.hf3[o] = ho;
+                    a.qo[o] = qq;
+                    out_acc += double(qq * K.dt);
+                }
+                const R dm = dm2;
+                if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
+                // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
+                const R big = R(1e9);
+                const R vr = qxl2 == R(0) ? qxl2 : qxl2 / (hfx2 < K.tol ? big : hfx2);
+                const R vu = qyl2 == R(0) ? qyl2 : qyl2 / (hfy2 < K.tol ? big : hfy2);
+                const R vb = qyl1 == R(0) ? qyl1 : qyl1 / (hfy1 < K.tol ? big : hfy1);
+                const R rc = j == 0 ? R(0.5) * vr : vr;
+                const R uc = R(0.5) * (vu + vb);
+                const R s2 = rc * rc + uc * uc;
+                s2max = fmax(s2max, s2);
+                if (s2 >= a.stag_s2) {
+                    const R dts = fmax(fmax(hfx2, hfy2), hf3);
+                    R cval;
+                    if (a.adaptive == 1) {
+                        cval = K.g * fmax(dts, R(0));
+                    } else {
+                        const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
+                        cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
+                    }
+                    const unsigned long long e = ord_bits(cval) + 1ull;
+                    cenc = e > cenc ? e : cenc;
+                }
+                V4 o4;
+                o4.x = hn;
+                o4.y = qxl2;
+                o4.z = qyl2;
+                o4.w = hn > dm ? hn : dm;   // save_output_maps.m:598, max(d_t, dmax)
+                sout[c2] = o4;
             }
+            // (G) shift the window down one row
+            hT2 = hT1; hT1 = hT0;
+            qxu1 = qxu0; qyu1 = qyu0;
+            hfx2 = hfx1; hfx1 = hfx0;
+            hfy2 = hfy1; hfy1 = hfy0;
+            sc2 = sc1;
+            qxl2 = qxl1; qyl2 = qyl1;
+            dm2 = dm1; dm1 = X.w;
+            mt2 = mt1; mt1 = meta;
         }
-        sQy[e] = q;
-        sHy[e] = Hf;
-    }
-    __syncthreads();
-
-    // ---- phase 2: donor scale factors ------------------------------------------------
-    for (int e = tid; e < SM::SH * SM::SW; e += NT) {
-        const int li = e / SM::SW, lj = e - li * SM::SW;
-        const int i = r0 - 1 + li, j = c0 - 1 + lj;
-        R s = R(1);
-        if (i >= 0 && i < ny && j >= 0 && j < nx) {
-            const R qR = sQx[li * SM::XW + lj + 1];
-            const R qL = sQx[li * SM::XW + lj];
-            const R qU = sQy[li * SM::YW + lj];
-            const R qD = sQy[(li + 1) * SM::YW + lj];
-            s = donor_scale(qR, qL, qU, qD, sH[(li + 1) * SM::HW + lj + 1], K);
-        }
-        sS[e] = s;
-    }
-    __syncthreads();
-
-    // ---- phase 3: limited faces of the block (in place) ------------------------------
-    for (int e = tid; e < BY * (BX + 1); e += NT) {
-        const int ra = e / (BX + 1), cb = e - ra * (BX + 1);
-        R* q = &sQx[(ra + 1) * SM::XW + cb + 1];
-        *q = limit_face(*q, sS[(ra + 1) * SM::SW + cb], sS[(ra + 1) * SM::SW + cb + 1]);
-    }
-    for (int e = tid; e < (BY + 1) * BX; e += NT) {
-        const int ra = e / BX, cb = e - ra * BX;
-        R* q = &sQy[(ra + 1) * SM::YW + cb + 1];
-        *q = limit_face(*q, sS[(ra + 1) * SM::SW + cb + 1], sS[ra * SM::SW + cb + 1]);
-    }
-    __syncthreads();
-
-    // ---- phase 4: continuity, outlet, maxima, CFL -------------------------------------
-    R vmax = R(0), cmax = R(0);
-    const R t_arr = R(s_tmin * 60.0 + s_dts);
-    for (int e = tid; e < BY * BX; e += NT) {
-        const int ra = e / BX, cb = e - ra * BX;
-        const int i = r0 + ra, j = c0 + cb;
-        if (i >= ny || j >= nx) continue;
-        const size_t c = size_t(i) * nx + j;
-        const R htot = sH[(ra + 2) * SM::HW + cb + 2];
-        const R qR = sQx[(ra + 1) * SM::XW + cb + 2];
-        const R qL = sQx[(ra + 1) * SM::XW + cb + 1];
-        const R qU = sQy[(ra + 1) * SM::YW + cb + 1];
-        const R qD = sQy[(ra + 2) * SM::YW + cb + 1];
-        R hn = continuity(htot, qL, qR, qU, qD, K);
-        R hf3 = R(0);
-        if (a.n_outlets && ((__ldg(a.outlet_bits + size_t(i) * a.bit_words + (j >> 5)) >> (j & 31)) & 1u)) {
-            const int o = find_outlet(a.outlet_cells, a.n_outlets, int(c));
-            if (o >= 0) {
-                R ho;
-                const R qq = outlet_sink(hn, a.outlet_coef[o], a.outlet_type, K, ho);
-                hf3 = ho;
-                a.hf3[o] = ho;
-                a.qo[o] = qq;
-                out_acc += double(qq * K.dt);
-            }
-        }
-        const R dm = a.dmax[c];
-        if (dm < K.thr && hn >= K.thr) a.arrival[c] = t_arr;
-        if (hn > dm) a.dmax[c] = hn;
-        R speed, celer;
-        cfl_cell(qR, qU, qD, sHx[(ra + 1) * SM::XW + cb + 2], sHy[(ra + 1) * SM::YW + cb + 1],
-                 sHy[(ra + 2) * SM::YW + cb + 1], hf3, j == 0, a.adaptive, K, speed, celer);
-        vmax = fmax(vmax, speed);
-        cmax = fmax(cmax, celer);
-        hout[c] = hn;
-        qxout[c] = qR;
-        qyout[c] = qU;
     }
 
     // ---- CTA reductions ---------------------------------------------------------------
     // every thread publishes its stores before the CTA takes its ticket, so the last
     // CTA can read the new outlet depths
     __threadfence();
-    const int lane = tid & 31, warp = tid >> 5;
-    vmax = warp_max(vmax);
-    cmax = warp_max(cmax);
+    const int lane_ = tid & 31, warp_ = tid >> 5;
+    s2max = warp_max(s2max);
+    cenc = warp_max_u(cenc);
     rain_acc = warp_sum(rain_acc);
     inf_acc = warp_sum(inf_acc);
     out_acc = warp_sum(out_acc);
-    if (lane == 0) {
-        red_r[0][warp] = vmax;
-        red_r[1][warp] = cmax;
-        red_d[0][warp] = rain_acc;
-        red_d[1][warp] = inf_acc;
-        red_d[2][warp] = out_acc;
+    if (lane_ == 0) {
+        red_s2[warp_] = s2max;
+        red_c[warp_] = cenc;
+        red_d[0][warp_] = rain_acc;
+        red_d[1][warp_] = inf_acc;
+        red_d[2][warp_] = out_acc;
     }
     __syncthreads();
     if (tid == 0) {
         for (int w = 1; w < NT / 32; ++w) {
-            vmax = fmax(vmax, red_r[0][w]);
-            cmax = fmax(cmax, red_r[1][w]);
+            s2max = fmax(s2max, red_s2[w]);
+            cenc = red_c[w] > cenc ? red_c[w] : cenc;
             rain_acc += red_d[0][w];
             inf_acc += red_d[1][w];
             out_acc += red_d[2][w];
         }
         StepScalars* sc = a.sc;
-        if (vmax > R(0)) atomicMax(&sc->acc_vmax, ord_bits(vmax));
-        if (cmax > R(0)) atomicMax(&sc->acc_cmax, ord_bits(cmax));
+        if (s2max > R(0)) atomicMax(&sc->acc_vmax, ord_bits(s2max));
+        if (cenc) atomicMax(&sc->acc_cmax, cenc);
         if (rain_acc != 0.0) atomicAdd(&sc->acc_rain, rain_acc);
         if (inf_acc != 0.0) atomicAdd(&sc->acc_inf, inf_acc);
         if (out_acc != 0.0) atomicAdd(&sc->acc_out, out_acc);
@@ -309,9 +350,15 @@ __global__ void __launch_bounds__(NT) k_fused_step(const FusedArgs<R> a) {
     __shared__ double s_tnew, s_dtnew;
     if (tid == 0) {
         StepScalars* sc = a.sc;
-        const bool is_d = sizeof(R) == 8;
-        const double vm = from_ord(atomicAdd(&sc->acc_vmax, 0ull), is_d);
-        const double cm = from_ord(atomicAdd(&sc->acc_cmax, 0ull), is_d);
+        const unsigned long long vbits = atomicAdd(&sc->acc_vmax, 0ull);
+        const unsigned long long cbits = atomicAdd(&sc->acc_cmax, 0ull);
+        const R vR = sqrt(bits_to<R>(vbits));
+        double vm = double(vR);
+        double cm = 0.0;
+        if (cbits) {
+            const R v = bits_to<R>(cbits - 1ull);
+            cm = a.adaptive == 1 ? double(fmax(sqrt(v), R(1e-10))) : double(v);
+        }
         const double rain_s = atomicAdd(&sc->acc_rain, 0.0);
         const double inf_s = atomicAdd(&sc->acc_inf, 0.0);
         const double out_s = atomicAdd(&sc->acc_out, 0.0);
@@ -356,10 +403,10 @@ __global__ void __launch_bounds__(NT) k_fused_step(const FusedArgs<R> a) {
         const R ru = a.rain.n_uniform ? R(uniform_rate(a.rain, s_tnew)) : R(0);
         for (int o = tid; o < a.n_outlets; o += NT) {
             const int c = a.outlet_cells[o];
-            if (a.ga && a.soil[c] != 255) continue;
+            if (a.ga && (meta_bits(a.stat[c].w) & 255u) != 255u) continue;
             const int i = c / nx, j = c - (c / nx) * nx;
             const R rate = map2 ? map_rate<R>(a.rain, map2, i, j, ny, nx) : ru;
-            const R hv = __ldcg(hout + c) + rate * K2.rain_scale;
+            const R hv = __ldcg(&sout[c].x) + rate * K2.rain_scale;
             if (hv < R(-1e-11)) neg = 1;
         }
     }
@@ -370,8 +417,8 @@ __global__ void __launch_bounds__(NT) k_fused_step(const FusedArgs<R> a) {
 // Clamp-skip flag for the first fused step of a call, over every cell (the state may
 // have been set from the host).  sc->skip_clamp must be zero on entry.
 template <typename R>
-__global__ void k_skip_flag(const R* h, int ny, int nx, RainDesc rain, const uint8_t* soil, int ga,
-                            double res, double tol_mm, double thr_mm, StepScalars* sc) {
+__global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>::V4* stat, int ny, int nx,
+                            RainDesc rain, int ga, double res, double tol_mm, double thr_mm, StepScalars* sc) {
     const size_t n = size_t(ny) * nx;
     const double t = sc->t_min, dts = sc->time_step * 60.0;
     StepConsts<R> K;
@@ -381,12 +428,48 @@ __global__ void k_skip_flag(const R* h, int ny, int nx, RainDesc rain, const uin
     const R ru = rain.n_uniform ? R(uniform_rate(rain, t)) : R(0);
     int neg = 0;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
-        if (ga && soil[c] != 255) continue;
+        if (ga && (meta_bits(stat[c].w) & 255u) != 255u) continue;
         const int i = int(c / nx), j = int(c % nx);
         const R rate = map ? map_rate<R>(rain, map, i, j, ny, nx) : ru;
-        if (h[c] + rate * K.rain_scale < R(-1e-11)) neg = 1;
+        if (st[c].x + rate * K.rain_scale < R(-1e-11)) neg = 1;
     }
     if (__syncthreads_or(neg) && threadIdx.x == 0) atomicOr(&sc->skip_clamp, 1);
+}
+
+// SoA <-> record conversion for the unfused entry points
+template <typename R>
+__global__ void k_unpack(size_t n, const typename Vec<R>::V4* st, const typename Vec<R>::V2* gs, R* h, R* qx, R* qy,
+                         R* dmax, R* I, R* T) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
+        const auto v = st[c];
+        h[c] = v.x;
+        qx[c] = v.y;
+        qy[c] = v.z;
+        dmax[c] = v.w;
+        if (gs) {
+            const auto g = gs[c];
+            I[c] = g.x;
+            T[c] = g.y;
+        }
+    }
+}
+template <typename R>
+__global__ void k_pack(size_t n, typename Vec<R>::V4* st, typename Vec<R>::V2* gs, const R* h, const R* qx,
+                       const R* qy, const R* dmax, const R* I, const R* T) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
+        typename Vec<R>::V4 v;
+        v.x = h[c];
+        v.y = qx[c];
+        v.z = qy[c];
+        v.w = dmax[c];
+        st[c] = v;
+        if (gs) {
+            typename Vec<R>::V2 g;
+            g.x = I[c];
+            g.y = T[c];
+            gs[c] = g;
+        }
+    }
 }
 
 }  // namespace hp2d

@@ -140,6 +140,9 @@ class SurfaceFlow:
         self._check(self._L.hp2d_fused_steps_timed(self._h, int(n), C.byref(ms)))
         return ms.value
 
+    def set_tuning(self, rows_per_warp: int):
+        self._check(self._L.hp2d_set_tuning(self._h, int(rows_per_warp)))
+
     def run(self, max_steps: int = 0) -> int:
         done = C.c_int64()
         self._check(self._L.hp2d_run(self._h, int(max_steps), C.byref(done)))

@@ -178,6 +178,9 @@ hp2d_status hp2d_fused_steps(hp2d_ctx* ctx, int32_t nsteps);
 /* hp2d_fused_steps bracketed by CUDA events on the context's stream; *elapsed_ms is the
  * device time of the nsteps launches (for benchmarking). */
 hp2d_status hp2d_fused_steps_timed(hp2d_ctx* ctx, int32_t nsteps, float* elapsed_ms);
+/* Launch shape of the fused kernel: rows each warp streams through (>= 4).  Results do
+ * not depend on it; hp2d_autotune picks it per grid. */
+hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp);
 /* Runs until the clock passes routing_time (or max_steps); returns steps executed. */
 hp2d_status hp2d_run(hp2d_ctx* ctx, int64_t max_steps, int64_t* steps_done);
 
