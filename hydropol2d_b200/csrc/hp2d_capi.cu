@@ -532,7 +532,7 @@ template <typename R> struct Impl : Base {
     }
 
     void launch_fused(const FusedArgs<R>& a) {
-        k_fused_step<R, kThreads><<<a.n_ctas, kThreads, 0, st()>>>(a);
+        k_fused_step<R, kThreads><<<a.n_ctas, kThreads, fused_smem_bytes<R>(kThreads), st()>>>(a);
     }
 
     void invalidate_graph() {
@@ -548,6 +548,7 @@ template <typename R> struct Impl : Base {
         hs.counter = 0;
         hs.acc_vmax = hs.acc_cmax = 0;
         hs.acc_rain = hs.acc_inf = hs.acc_out = 0;
+        hs.n_finite = 0;
         push_sc();
         k_skip_flag<R><<<blocks_for(n), kThreads, 0, st()>>>(st4[hs.cur].p, stat.p, ny, nx, rain, ga() ? 1 : 0, res,
                                                            ctx->p.depth_tolerance, ctx->p.arrival_threshold, sc.p);
@@ -582,6 +583,10 @@ template <typename R> struct Impl : Base {
         HP_CK(cudaGetLastError());
         if (after) HP_CK(cudaEventRecord(after, st()));
         pull_sc();
+        if (hs.status & 2u) {
+            ctx->err = "a row copy into shared memory did not complete within its wait limit";
+            return HP2D_TIMEOUT;
+        }
         return HP2D_OK;
     }
 

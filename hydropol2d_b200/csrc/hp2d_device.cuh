@@ -112,6 +112,7 @@ struct StepScalars {
     double acc_rain, acc_inf, acc_out; // step sums [m] (times cell area later)
     int acc_neg;           // unfused path: some depth < -1e-8 mm after hydrology
     int pad;
+    unsigned long long n_finite;   // cells with a finite depth (walls excluded)
 };
 
 // non-negative floats/doubles order like their bit patterns
@@ -165,6 +166,52 @@ template <> __host__ __device__ inline double make_meta<double>(unsigned m) {
     double d;
     memcpy(&d, &u, 8);
     return d;
+}
+
+// ---------------- bulk async copies (TMA, 1-D) into shared memory ----------------------
+// Local-memory sources only (this GPU's global memory); no cluster multicast anywhere.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: false when the phase did not complete within `limit` polls
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// generic-proxy reads of a shared buffer complete before the async proxy rewrites it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// bulk copy global -> shared, completion counted in bytes on `bar`; 16-byte aligned
+// addresses, size a multiple of 16
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
 
 // ---------------- Green-Ampt soil class table -----------------------------------------
@@ -283,6 +330,24 @@ __device__ __forceinline__ R donor_scale(R qR, R qL, R qU, R qD, R hc, const Ste
     if (out > avail && out > R(0)) s = avail / out;
     if (!isfinite(s)) s = R(0);
     return fmax(fmin(s, R(1)), R(0));
+}
+
+// donor_scale without the checks that cannot fire when the four faces are finite:
+// avail >= 0, so out > avail implies out > 0 and 0 <= avail/out <= 1 (a finite value
+// that the clamps and the NaN test of donor_scale leave unchanged)
+template <typename R>
+__device__ __forceinline__ R donor_scale_finite(R qR, R qL, R qU, R qD, R hc, const StepConsts<R>& K) {
+    R out = fmax(qR, R(0));
+    out = out + fmax(-qL, R(0));
+    out = out + fmax(qU, R(0));
+    out = out + fmax(-qD, R(0));
+    const R avail = fmax(hc, R(0)) * K.dx_over_dt;
+    return out > avail ? avail / out : R(1);
+}
+// limit_face for a finite q and scales in [0, 1] (the product is finite)
+template <typename R>
+__device__ __forceinline__ R limit_face_finite(R q, R s_pos, R s_neg) {
+    return q > R(0) ? q * s_pos : (q < R(0) ? q * s_neg : q);
 }
 
 // face limited by the scale of its donor cell; s_pos = donor when q > 0

@@ -34,6 +34,12 @@
 namespace hp2d {
 
 constexpr int kStripOut = 28;   // output columns of a 32-lane strip (lanes 2..29)
+constexpr int kStages = 4;      // shared-memory ring depth of the row pipeline
+
+// dynamic shared memory of k_fused_step: per warp kStages x 64 records
+template <typename R> constexpr size_t fused_smem_bytes(int nt) {
+    return size_t(nt / 32) * kStages * 64 * sizeof(typename Vec<R>::V4);
+}
 
 template <typename R> struct FusedArgs {
     using V4 = typename Vec<R>::V4;
@@ -118,6 +124,10 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     __shared__ R red_s2[NT / 32];
     __shared__ unsigned long long red_c[NT / 32];
     __shared__ double red_d[3][NT / 32];
+    __shared__ int red_to[NT / 32];
+    __shared__ __align__(8) unsigned long long s_bar[NT / 32][kStages];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    bool timed_out = false;
 
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -153,6 +163,8 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     const int wg = blockIdx.x * (NT / 32) + warp;
 
     double rain_acc = 0.0, inf_acc = 0.0, out_acc = 0.0;
+    R rain_acc_r = R(0), inf_acc_r = R(0);   // per-lane partial sums (ledger only)
+    unsigned dry = 0u;                        // bit i: row r-i dry across the strip
     R s2max = R(0);
     unsigned long long cenc = 0ull;   // 0: no non-stagnant cell; else bits(value) + 1
 
@@ -174,35 +186,60 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
         R dm1 = R(0), dm2 = R(0);
         unsigned mt1 = 0u, mt2 = 0u;
 
-        // software pipeline: the records of row r+1 are requested before row r is computed
-        const V4 zero4 = {R(0), R(0), R(0), R(0)};
-        const V4 closed4 = {NaNR, NaNR, R(0), R(0)};
-        const V2 zero2 = {R(0), R(0)};
-        V4 nS = closed4, nX = zero4;
-        V2 nG = zero2;
-        {
-            const int rr = r0 - 2;
-            if (col_ok && rr >= 0 && rr < ny) {
-                const size_t c = size_t(rr) * nx + j;
-                nS = stat[c];
-                nX = sin[c];
-                if (a.ga) nG = gin[c];
+        // TMA pipeline: the warp's two row records (static, state) of rows k+1..k+kStages-1
+        // are in flight in a ring of kStages shared-memory stages while row k is
+        // computed.  Lane 0 issues one 1-D bulk copy per record row (the strip's cells
+        // are contiguous), the stage's mbarrier counts the bytes.
+        const int j_first = strip * kStripOut - 2;
+        const int seg_j0 = max(j_first, 0);
+        const int seg_n = min(j_first + 32, nx) - seg_j0;
+        const int seg_off = seg_j0 - j_first;
+        const int last_k = (r_end + 1) - (r0 - 2);
+        V4* ring = reinterpret_cast<V4*>(smem_dyn) + size_t(warp) * kStages * 64;
+        const uint32_t bar0 = smem_addr(&s_bar[warp][0]);
+        auto issue = [&](int k) {
+            const int s = k % kStages;
+            const uint32_t bar = bar0 + 8u * s;
+            const int rr = r0 - 2 + k;
+            if (rr >= 0 && rr < ny && seg_n > 0) {
+                const uint32_t bytes = uint32_t(seg_n) * uint32_t(sizeof(V4));
+                mbar_expect_tx(bar, 2u * bytes);
+                const size_t g = size_t(rr) * nx + seg_j0;
+                bulk_g2s(smem_addr(ring + s * 64 + seg_off), stat + g, bytes, bar);
+                bulk_g2s(smem_addr(ring + s * 64 + 32 + seg_off), sin + g, bytes, bar);
+            } else {
+                mbar_arrive(bar);
             }
+        };
+        if (lane == 0) {
+            for (int s = 0; s < kStages; ++s) mbar_init(bar0 + 8u * s, 1u);
+            mbar_fence_init();
         }
-        for (int r = r0 - 2; r < r_end + 2; ++r) {
-            const V4 S = nS, X = nX;
-            const V2 Gs = nG;
-            {
-                const int rr = r + 1;
-                nS = closed4;
-                nX = zero4;
-                if (col_ok && rr >= 0 && rr < ny) {
-                    const size_t cn = size_t(rr) * nx + j;
-                    nS = stat[cn];
-                    nX = sin[cn];
-                    if (a.ga) nG = gin[cn];
-                }
+        __syncwarp();
+        if (lane == 0)
+            for (int k = 0; k < kStages && k <= last_k; ++k) issue(k);
+        const V2 zero2 = {R(0), R(0)};
+        V2 nG = zero2;
+        if (a.ga && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
+        for (int k = 0; k <= last_k; ++k) {
+            const int r = r0 - 2 + k;
+            const int s = k % kStages;
+            if (!mbar_wait_bounded(bar0 + 8u * s, uint32_t((k / kStages) & 1), 1u << 22)) {
+                timed_out = true;
+                // let the copies still in flight land before the CTA leaves
+                for (int kk = k + 1; kk < k + kStages && kk <= last_k; ++kk)
+                    mbar_wait_bounded(bar0 + 8u * (kk % kStages), uint32_t((kk / kStages) & 1), 1u << 22);
+                break;
             }
+            const V4 S = ring[s * 64 + lane];
+            const V4 X = ring[s * 64 + 32 + lane];
+            __syncwarp();
+            if (lane == 0 && k + kStages <= last_k) {
+                fence_proxy_async_smem();
+                issue(k + kStages);
+            }
+            const V2 Gs = nG;
+            if (a.ga && col_ok && r + 1 >= 0 && r + 1 < ny) nG = gin[size_t(r + 1) * nx + j];
             const bool ok = col_ok && r >= 0 && r < ny;
             const size_t c = size_t(r) * nx + j;
             const unsigned meta = meta_bits(S.w);
@@ -214,7 +251,8 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                 const R rr = rate * K.rain_scale;
                 hh = hh + rr;
                 const bool own = own_lane && r >= r0 && r < r_end;
-                if (own && isfinite(hh)) rain_acc += double(rr);
+                // uniform rain volume comes from the count of finite cells at the end
+                if (map && own && isfinite(hh)) rain_acc_r += rr;
                 if (a.ga) {
                     const unsigned s = meta & 255u;
                     V2 go = Gs;
@@ -223,7 +261,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                         const R fd = green_ampt(hh, Ic, Tc, a.classes[s], K);
                         go.x = Ic;
                         go.y = Tc;
-                        if (own && isfinite(fd)) inf_acc += double(fd);
+                        if (own && isfinite(fd)) inf_acc_r += fd;
                     }
                     if (own) gout[c] = go;
                 }
@@ -231,22 +269,27 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                 if (hh < R(0)) hh = R(0);
                 hT0 = hh;
             }
-            // (B) x face (r, j) between (r, j) and (r, j+1)
-            const R hR = __shfl_down_sync(FULL, hT0, 1);
-            R qxu0 = R(0), hfx0 = R(0);
-            if (ok && !isnan(S.x)) face_flux<R, true>(hT0, hR, S.x, X.y, S.z, K, a.flag_critical, hfx0, qxu0);
-            // (C) y face (r, j) between (r-1, j) and (r, j)
-            R qyu0 = R(0), hfy0 = R(0);
-            if (ok && r >= r0 - 1 && !isnan(S.y))
-                face_flux<R, false>(hT1, hT0, S.y, X.z, S.z, K, a.flag_critical, hfy0, qyu0);
-            // (D) donor scale of (r-1, j)
-            const R qxu1_left = __shfl_up_sync(FULL, qxu1, 1);
-            R sc1 = R(1);
-            if (col_ok && r >= r0 && r - 1 >= 0 && r - 1 < ny) sc1 = donor_scale(qxu1, qxu1_left, qyu1, qyu0, hT1, K);
-            // (E) limited faces of row r-1
-            const R sc1_right = __shfl_down_sync(FULL, sc1, 1);
-            const R qxl1 = limit_face(qxu1, sc1, sc1_right);
-            const R qyl1 = limit_face(qyu1, sc1, sc2);
+            // rows r-2..r dry across the whole strip: every face flux of row r and r-1 is
+            // zero (Hf = 0), the donor scale of row r-1 is one and its limited faces are
+            // zero, so (B)-(E) are skipped; the values below are what they would compute
+            dry = (dry << 1) | (__all_sync(FULL, hT0 == R(0)) ? 1u : 0u);
+            R qxu0 = R(0), hfx0 = R(0), qyu0 = R(0), hfy0 = R(0), sc1 = R(1), qxl1 = R(0), qyl1 = R(0);
+            if ((dry & 7u) != 7u) {
+                // (B) x face (r, j) between (r, j) and (r, j+1)
+                const R hR = __shfl_down_sync(FULL, hT0, 1);
+                if (ok && !isnan(S.x)) face_flux<R, true>(hT0, hR, S.x, X.y, S.z, K, a.flag_critical, hfx0, qxu0);
+                // (C) y face (r, j) between (r-1, j) and (r, j)
+                if (ok && r >= r0 - 1 && !isnan(S.y))
+                    face_flux<R, false>(hT1, hT0, S.y, X.z, S.z, K, a.flag_critical, hfy0, qyu0);
+                // (D) donor scale of (r-1, j)
+                const R qxu1_left = __shfl_up_sync(FULL, qxu1, 1);
+                if (col_ok && r >= r0 && r - 1 >= 0 && r - 1 < ny)
+                    sc1 = donor_scale_finite(qxu1, qxu1_left, qyu1, qyu0, hT1, K);
+                // (E) limited faces of row r-1
+                const R sc1_right = __shfl_down_sync(FULL, sc1, 1);
+                qxl1 = limit_face_finite(qxu1, sc1, sc1_right);
+                qyl1 = limit_face_finite(qyu1, sc1, sc2);
+            }
             // (F) continuity, outlet, maxima and CFL of row r-2
             const R qxl2_left = __shfl_up_sync(FULL, qxl2, 1);
             const int rm2 = r - 2;
@@ -310,21 +353,28 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     // every thread publishes its stores before the CTA takes its ticket, so the last
     // CTA can read the new outlet depths
     __threadfence();
+    rain_acc += double(rain_acc_r);
+    inf_acc += double(inf_acc_r);
     const int lane_ = tid & 31, warp_ = tid >> 5;
     s2max = warp_max(s2max);
     cenc = warp_max_u(cenc);
     rain_acc = warp_sum(rain_acc);
     inf_acc = warp_sum(inf_acc);
     out_acc = warp_sum(out_acc);
+    const int to_any = __any_sync(0xffffffffu, timed_out);
     if (lane_ == 0) {
         red_s2[warp_] = s2max;
         red_c[warp_] = cenc;
         red_d[0][warp_] = rain_acc;
         red_d[1][warp_] = inf_acc;
         red_d[2][warp_] = out_acc;
+        red_to[warp_] = to_any;
     }
     __syncthreads();
     if (tid == 0) {
+        int to = 0;
+        for (int w = 0; w < NT / 32; ++w) to |= red_to[w];
+        if (to) atomicOr(&a.sc->status, 2u);   // a row copy did not arrive in time
         for (int w = 1; w < NT / 32; ++w) {
             s2max = fmax(s2max, red_s2[w]);
             cenc = red_c[w] > cenc ? red_c[w] : cenc;
@@ -359,7 +409,9 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
             const R v = bits_to<R>(cbits - 1ull);
             cm = a.adaptive == 1 ? double(fmax(sqrt(v), R(1e-10))) : double(v);
         }
-        const double rain_s = atomicAdd(&sc->acc_rain, 0.0);
+        double rain_s = atomicAdd(&sc->acc_rain, 0.0);
+        // uniform rain: the same depth on every cell with a finite depth
+        if (a.rain.n_uniform) rain_s += double(s_rain * s_K.rain_scale) * double(sc->n_finite);
         const double inf_s = atomicAdd(&sc->acc_inf, 0.0);
         const double out_s = atomicAdd(&sc->acc_out, 0.0);
         const double t = s_tmin;
@@ -427,12 +479,17 @@ __global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>
     const float* map = m >= 0 ? rain.maps + size_t(m) * rain.my * rain.mx : nullptr;
     const R ru = rain.n_uniform ? R(uniform_rate(rain, t)) : R(0);
     int neg = 0;
+    unsigned long long fin = 0;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
+        const R hc = st[c].x;
+        if (isfinite(hc)) ++fin;
         if (ga && (meta_bits(stat[c].w) & 255u) != 255u) continue;
         const int i = int(c / nx), j = int(c % nx);
         const R rate = map ? map_rate<R>(rain, map, i, j, ny, nx) : ru;
-        if (st[c].x + rate * K.rain_scale < R(-1e-11)) neg = 1;
+        if (hc + rate * K.rain_scale < R(-1e-11)) neg = 1;
     }
+    for (int o = 16; o > 0; o >>= 1) fin += __shfl_xor_sync(0xffffffffu, fin, o);
+    if ((threadIdx.x & 31) == 0 && fin) atomicAdd(&sc->n_finite, fin);
     if (__syncthreads_or(neg) && threadIdx.x == 0) atomicOr(&sc->skip_clamp, 1);
 }
 

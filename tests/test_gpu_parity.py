@@ -38,8 +38,11 @@ def assert_same_clock(g, o):
     dg, do = g.diag(), o.diag()
     for k in ("t", "time_step", "k", "max_velocity", "neg_depth_warnings", "unstable_steps"):
         assert dg[k] == do[k], f"{k}: gpu {dg[k]} oracle {do[k]}"
+    # the volume ledger is a diagnostic: per-lane partial sums are kept in the state
+    # precision and summed in a different order than the oracle's sequential FP64 sum
+    rel = 1e-5 if g.precision == "fp32" else 1e-9
     for k in ("rain_volume", "infiltration_volume", "outlet_volume"):
-        assert dg[k] == pytest.approx(do[k], rel=1e-9, abs=1e-9), k
+        assert dg[k] == pytest.approx(do[k], rel=rel, abs=1e-9), k
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
