@@ -35,6 +35,10 @@ namespace hp2d {
 
 constexpr int kStripOut = 28;   // output columns of a 32-lane strip (lanes 2..29)
 constexpr int kStages = 4;      // shared-memory ring depth of the row pipeline
+#ifndef HP2D_ROW_UNROLL
+#define HP2D_ROW_UNROLL 1
+#endif
+constexpr int kRowUnroll = HP2D_ROW_UNROLL;   // row-loop unroll (register renaming of the window)
 
 // dynamic shared memory of k_fused_step: per warp kStages x 64 records
 template <typename R> constexpr size_t fused_smem_bytes(int nt) {
@@ -221,6 +225,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
         const V2 zero2 = {R(0), R(0)};
         V2 nG = zero2;
         if (a.ga && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
+#pragma unroll kRowUnroll
         for (int k = 0; k <= last_k; ++k) {
             const int r = r0 - 2 + k;
             const int s = k % kStages;
