@@ -39,6 +39,7 @@ EXPORTS = [
     "hp2d_set_tuning", "hp2d_run",
     "hp2d_download",
     "hp2d_download_native", "hp2d_get_diag", "hp2d_stored_volume",
+    "hp2d_cfl_dt_noalloc", "hp2d_noalloc_error",
 ]
 
 
@@ -124,6 +125,8 @@ def lib() -> C.CDLL:
         "hp2d_download_native": ([vp, C.c_int32, vp, C.c_size_t], C.c_int),
         "hp2d_get_diag": ([vp, P(Diag)], C.c_int),
         "hp2d_stored_volume": ([vp, dp], C.c_int),
+        "hp2d_cfl_dt_noalloc": ([C.c_int32, C.c_int32, C.c_double, P(Params), vp, vp, vp, vp, dp, dp], C.c_int),
+        "hp2d_noalloc_error": ([], C.c_char_p),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -44,7 +44,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
         return LIB
     cmd = [nvcc(), *NVCC_FLAGS, f"-I{ROOT / 'include'}", f"-I{SRC}",
-           str(SRC / "hp2d_capi.cu"), "-o", str(LIB)]
+           *[str(p) for p in sorted(SRC.glob("*.cu"))], "-o", str(LIB)]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     tmp = LIB.with_suffix(".so.tmp")

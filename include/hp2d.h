@@ -198,6 +198,26 @@ hp2d_status hp2d_get_diag(hp2d_ctx* ctx, hp2d_diag* out);
 /* Stored surface volume sum(d_t)*cell_area/1000 [m^3], FP64 accumulation. */
 hp2d_status hp2d_stored_volume(hp2d_ctx* ctx, double* volume);
 
+/* ---- allocation-free timestep (no counterpart in the reference) -------------------- */
+/* refreshing_timestep's refresh branch (as hp2d_cfl_dt) on caller-owned FP32 device
+ * arrays, for callers that may not allocate GPU memory while they run: a MEX gateway
+ * inside MATLAB whose GPU memory pool owns the device, code inside a CUDA stream capture,
+ * real-time drivers that allocate only at start-up.  Nothing is allocated: the reduction
+ * scratch is a fixed 64 KB array inside the library, resident on every GPU that loads it
+ * until the process exits, which limits grids to ny <= 65536 rows (larger grids are
+ * rejected with HP2D_INVALID_ARG).  The first call on each device (with that device
+ * current) resolves the array's device address and should come before any stream
+ * capture.  Calls that overlap on the GPU share the scratch and race.
+ *   q_x, q_y   ny*nx limited face discharge per unit width [m^2/s] (native fields 1, 2)
+ *   hf         3*ny*nx face flow depth [m]: pages x, y and outlet, as Hf(:,:,1:3)
+ *   stream     cudaStream_t to run on (NULL = default stream); the call synchronises it
+ *   time_step  [out] new time step [min]; max_velocity [out, nullable] [m/s]
+ * On failure hp2d_noalloc_error() gives the message. */
+hp2d_status hp2d_cfl_dt_noalloc(int32_t ny, int32_t nx, double resolution, const hp2d_params* params,
+                                const float* q_x, const float* q_y, const float* hf, void* stream,
+                                double* time_step, double* max_velocity);
+const char* hp2d_noalloc_error(void);
+
 #ifdef __cplusplus
 }
 #endif
