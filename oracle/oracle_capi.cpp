@@ -150,6 +150,19 @@ int oracle_download_native(oracle_model* m, int32_t field, void* out, size_t byt
     });
 }
 
+// x^(7/3), x^(5/3) of the deterministic Newton iteration, for accuracy tests
+void oracle_pow_check(int32_t precision, int32_t n, const double* x, double* p73, double* p53) {
+    for (int i = 0; i < n; ++i) {
+        if (precision == 0) {
+            p73[i] = double(hp2d_oracle::pow73<float>(float(x[i])));
+            p53[i] = double(hp2d_oracle::pow53<float>(float(x[i])));
+        } else {
+            p73[i] = hp2d_oracle::pow73<double>(x[i]);
+            p53[i] = hp2d_oracle::pow53<double>(x[i]);
+        }
+    }
+}
+
 int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
     return dispatch(m, [&](auto& M) {
         o->t = M.t_min;

@@ -1,0 +1,128 @@
+"""The kernel-form restatement (oracle/kernel_form.hpp, FP64) against the literal one
+(oracle/literal.py): the rewrites listed in kernel_form.hpp are algebraically exact, so the two
+agree to round-off; the full loop agrees until a timestep-snapping tie (floor(dt/inc)) flips.
+"""
+import numpy as np
+import pytest
+
+from oracle import literal as L
+from tests.cases import random_terrain, small_urban, small_vtilt
+
+
+def literal_cfg(case):
+    p = case.params
+    kw = dict(z=case.z, roughness=case.roughness, resolution=case.resolution, outlet_rows=case.outlet_rows,
+              outlet_cols=case.outlet_cols, outlet_type=p.get("outlet_type", 1),
+              slope_outlet=p.get("slope_outlet", 0.0), d0=case.d0, routing_time=p["routing_time"],
+              alfa_min=p["alfa_min"], alfa_max=p["alfa_max"])
+    if case.rain_uniform is not None:
+        kw["rain_times_min"], kw["rain_rates_mmh"] = case.rain_uniform
+    if case.rain_maps is not None:
+        kw["rain_maps_mmh"] = case.rain_maps.astype(np.float64)
+        kw["rain_map_dt_min"] = case.rain_map_dt
+    if case.soil is not None:
+        s = case.soil
+        cls = s["soil_class"]
+        act = cls != 255
+        c = np.where(act, cls, 0)
+        kw["ga"] = L.GAParams(ksat=s["ksat"][c], psi=s["psi"][c], dtheta=s["dtheta"][c], Lu=s["Lu"][c],
+                              k_out=s["k_out"][c], Tr=s["Tr"][c], min_sm=s["min_soil_moisture"][c], active=act)
+        kw["I0"] = case.I0
+    return L.RunConfig(**kw)
+
+
+def kernel_form(case):
+    import oracle
+    o = oracle.KernelFormOracle(*case.shape, case.resolution, "fp64", **case.params)
+    case.apply(o)
+    return o
+
+
+def test_full_loop_vtilt_agrees(oracle_lib):
+    case = small_vtilt(40, 40)
+    cfg = literal_cfg(case)
+    st = L.init_state(cfg)
+    o = kernel_form(case)
+    for k in range(200):
+        L.step(cfg, st)
+        o.fused_steps(1)
+        d = o.diag()
+        assert d["time_step"] == pytest.approx(st.time_step, rel=1e-12)
+        assert d["t"] == pytest.approx(st.t, rel=1e-12)
+        h = o.download_native("h") * 1000
+        assert np.allclose(h, st.d, rtol=1e-9, atol=1e-9), k
+    dm = o.download_native("dmax") * 1000
+    assert np.allclose(dm, st.dmax, rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_li_step_agrees_on_random_states(oracle_lib, seed):
+    """One Local_Inertial_Model_D4 call on a random wet state with random prior fluxes."""
+    case = random_terrain(23, 37, seed=seed, walls=False)
+    rng = np.random.default_rng(seed)
+    ny, nx = case.shape
+    outflow = np.zeros((3, ny, nx))
+    outflow[0] = rng.normal(0, 50, (ny, nx))
+    outflow[1] = rng.normal(0, 50, (ny, nx))
+    outflow[0][:, -1] = 0
+    outflow[1][0, :] = 0
+    d = np.where(rng.random((ny, nx)) < 0.7, rng.uniform(0, 500, (ny, nx)), 0.0)
+    ts = 0.5 / 60
+    lit = L.local_inertial_model_d4(case.z, d, case.roughness, case.roughness ** 2, case.resolution ** 2, ts,
+                                    case.resolution, case.outlet_rows, case.outlet_cols, 1,
+                                    case.params["slope_outlet"], outflow)
+    o = kernel_form(case)
+    o.set_state(d, outflow)
+    o.li_step(ts)
+    h = o.download_native("h") * 1000
+    assert np.allclose(h, lit.d_t, rtol=1e-12, atol=1e-12)
+    qr = o.download_native("qx") * 3.6e6 / case.resolution
+    qu = o.download_native("qy") * 3.6e6 / case.resolution
+    assert np.allclose(qr, lit.qout_right, rtol=1e-11, atol=1e-9)
+    assert np.allclose(qu, lit.qout_up, rtol=1e-11, atol=1e-9)
+    assert np.allclose(o.download_native("hfx"), lit.Hf[0], rtol=1e-12, atol=1e-14)
+    assert np.allclose(o.download_native("hfy"), lit.Hf[1], rtol=1e-12, atol=1e-14)
+    # refreshing_timestep on that state
+    cfl = L.refreshing_timestep(lit.Hf, lit.qout_right, lit.qout_up, case.resolution, 1.0, 0.5, 0.7, 10.0,
+                                0.01, 0.001)
+    ts_k, vm_k = o.cfl_dt()
+    assert vm_k == pytest.approx(cfl.max_velocity, rel=1e-12)
+    assert ts_k == pytest.approx(cfl.time_step, rel=1e-12)
+
+
+def test_green_ampt_step_agrees(oracle_lib):
+    case = small_urban(48, seed=5)
+    cfg = literal_cfg(case)
+    st = L.init_state(cfg)
+    o = kernel_form(case)
+    ts = 2.0 / 60
+    d = np.random.default_rng(0).uniform(0, 30, case.shape)
+    o.set_state(d, None, case.I0)
+    o.hydrology_step(ts)
+    dl, Il, Tl, f = L.green_ampt_infiltration(d + L.rain_rate_at(cfg, st.t, *case.shape) * (ts / 60), st.I, st.T,
+                                              ts, cfg.ga, case.resolution)
+    dl[dl < 1e-6] = 0
+    assert np.allclose(o.download_native("h") * 1000, dl, rtol=1e-10, atol=1e-9)
+    assert np.allclose(o.download_native("I") * 1000, Il, rtol=1e-10, atol=1e-9)
+    assert np.allclose(o.download_native("T") / 3600, Tl, rtol=1e-12)
+
+
+def test_rcbrt_accuracy(oracle_lib):
+    """x^(7/3) and x^(5/3) of the Newton iteration against libm in double: within 3e-6 in
+    float (~50 ulp: the iteration's residual 1 - x r^3 is formed from rounded products) and
+    1e-13 in double.  Both are far below the FP32-vs-FP64 differences the accuracy tests bound."""
+    import ctypes as C
+    import oracle
+    L_ = oracle._load()
+    f = L_.oracle_pow_check
+    f.argtypes = [C.c_int32, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    xs = np.concatenate([np.logspace(-30, 5, 4000), [1e-38, 3e-39, 1.0, 2.0, 1e-320]])
+    for prec, tol in ((0, 3e-6), (1, 1e-13)):
+        a = np.empty_like(xs)
+        b = np.empty_like(xs)
+        f(prec, xs.size, xs.ctypes.data_as(C.POINTER(C.c_double)), a.ctypes.data_as(C.POINTER(C.c_double)),
+          b.ctypes.data_as(C.POINTER(C.c_double)))
+        xr = xs.astype(np.float32).astype(np.float64) if prec == 0 else xs
+        ok = xr > (1e-15 if prec == 0 else 1e-130)   # results above the smallest normal
+        assert np.all(np.abs(a[ok] / xr[ok] ** (7 / 3) - 1) < tol)
+        assert np.all(np.abs(b[ok] / xr[ok] ** (5 / 3) - 1) < tol)
