@@ -35,8 +35,9 @@ NY, NX, DX = 4096, 8192, 5.0
 WORKLOAD = "dambreak_4096x8192_dx5_fp32"
 METRIC = "GCell-updates/s"
 # algorithmic bytes per cell-update of the fused FP32 step without infiltration and rain:
-# read h, qx, qy, dz_x, dz_y, n^2, dmax (7 x 4 B) + write h, qx, qy, dmax (4 x 4 B)
-BYTES_PER_CELL = 44.0
+# read the static record {dz_x, dz_y, n^2, meta} and the state record {h, q_x, q_y, dmax}
+# (2 x 16 B), write the state record (16 B)
+BYTES_PER_CELL = 48.0
 
 
 def dist_env():
@@ -244,7 +245,7 @@ def main():
     # ---- end to end through the C ABI with host buffers ------------------------------
     # host arrays -> hp2d_upload_static/hp2d_set_state -> K steps, reading the outlet
     # hydrograph and the clock back every step -> final depth and dmax back to the host
-    e2e_steps = min(args.steps, 500)
+    e2e_steps = args.steps
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sf = SurfaceFlow(ny, nx, DX, "fp32", device=local, **case.params)
@@ -258,11 +259,12 @@ def main():
     e2e_s = time.perf_counter() - t0
     n_out = sf.n_outlets
     sf.close()
-    # H2D: dz_x, dz_y, n^2, h, qx, qy, dmax, arrival (8 x 4 B per cell), once per run;
-    # D2H: outlet hydrograph (4 B per outlet) + the clock block every step, then
-    # depth and dmax (2 x 4 B per cell) once
-    h2d_per_step = 8 * 4 * cells / e2e_steps
-    d2h_per_step = n_out * 4 + 168 + 2 * 4 * cells / e2e_steps
+    # H2D per run: context set-up (static + 2 state records + arrival, 52 B/cell), static
+    # upload (record + unfused-path copies, 28 B/cell), state upload (record + arrival,
+    # 20 B/cell); D2H: outlet hydrograph (4 B per outlet) and the clock block every step,
+    # then the depth and dmax (state record twice, 32 B/cell) once
+    h2d_per_step = 100 * cells / e2e_steps
+    d2h_per_step = n_out * 4 + 2 * 184 + 32 * cells / e2e_steps
     e2e = cells * e2e_steps / e2e_s / 1e9
     if dist is not None:
         t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
