@@ -295,12 +295,15 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                 qxl1 = limit_face_finite(qxu1, sc1, sc1_right);
                 qyl1 = limit_face_finite(qyu1, sc1, sc2);
             }
-            // (F) continuity, outlet, maxima and CFL of row r-2
-            const R qxl2_left = __shfl_up_sync(FULL, qxl2, 1);
+            // (F) continuity, outlet, maxima and CFL of row r-2.  When rows r-3..r-1 are dry
+            // across the strip every flux into row r-2 is +0 (and so are its face depths):
+            // continuity gives hT2 + 0 and the cell adds nothing to the CFL reductions.
+            const bool quiet = (dry & 14u) == 14u;
+            const R qxl2_left = quiet ? R(0) : __shfl_up_sync(FULL, qxl2, 1);
             const int rm2 = r - 2;
             if (own_lane && rm2 >= r0 && rm2 < r_end) {
                 const size_t c2 = size_t(rm2) * nx + j;
-                R hn = continuity(hT2, qxl2_left, qxl2, qyl2, qyl1, K);
+                R hn = quiet ? hT2 + R(0) : continuity(hT2, qxl2_left, qxl2, qyl2, qyl1, K);
                 R hf3 = R(0);
                 const unsigned ord = mt2 >> 8;
                 if (ord) {
@@ -315,25 +318,27 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                 const R dm = dm2;
                 if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
                 // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
-                const R big = R(1e9);
-                const R vr = qxl2 == R(0) ? qxl2 : qxl2 / (hfx2 < K.tol ? big : hfx2);
-                const R vu = qyl2 == R(0) ? qyl2 : qyl2 / (hfy2 < K.tol ? big : hfy2);
-                const R vb = qyl1 == R(0) ? qyl1 : qyl1 / (hfy1 < K.tol ? big : hfy1);
-                const R rc = j == 0 ? R(0.5) * vr : vr;
-                const R uc = R(0.5) * (vu + vb);
-                const R s2 = rc * rc + uc * uc;
-                s2max = fmax(s2max, s2);
-                if (s2 >= a.stag_s2) {
-                    const R dts = fmax(fmax(hfx2, hfy2), hf3);
-                    R cval;
-                    if (a.adaptive == 1) {
-                        cval = K.g * fmax(dts, R(0));
-                    } else {
-                        const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
-                        cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
+                if (!quiet) {
+                    const R big = R(1e9);
+                    const R vr = qxl2 == R(0) ? qxl2 : qxl2 / (hfx2 < K.tol ? big : hfx2);
+                    const R vu = qyl2 == R(0) ? qyl2 : qyl2 / (hfy2 < K.tol ? big : hfy2);
+                    const R vb = qyl1 == R(0) ? qyl1 : qyl1 / (hfy1 < K.tol ? big : hfy1);
+                    const R rc = j == 0 ? R(0.5) * vr : vr;
+                    const R uc = R(0.5) * (vu + vb);
+                    const R s2 = rc * rc + uc * uc;
+                    s2max = fmax(s2max, s2);
+                    if (s2 >= a.stag_s2) {
+                        const R dts = fmax(fmax(hfx2, hfy2), hf3);
+                        R cval;
+                        if (a.adaptive == 1) {
+                            cval = K.g * fmax(dts, R(0));
+                        } else {
+                            const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
+                            cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
+                        }
+                        const unsigned long long e = ord_bits(cval) + 1ull;
+                        cenc = e > cenc ? e : cenc;
                     }
-                    const unsigned long long e = ord_bits(cval) + 1ull;
-                    cenc = e > cenc ? e : cenc;
                 }
                 V4 o4;
                 o4.x = hn;
