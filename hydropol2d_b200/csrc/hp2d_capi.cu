@@ -532,7 +532,15 @@ template <typename R> struct Impl : Base {
     }
 
     void launch_fused(const FusedArgs<R>& a) {
-        k_fused_step<R, kThreads><<<a.n_ctas, kThreads, fused_smem_bytes<R>(kThreads), st()>>>(a);
+        const size_t sm = fused_smem_bytes<R>(kThreads);
+        const bool map = rain.n_maps > 0;
+        if (a.ga) {
+            if (map) k_fused_step<R, kThreads, true, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
+            else k_fused_step<R, kThreads, true, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+        } else {
+            if (map) k_fused_step<R, kThreads, false, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
+            else k_fused_step<R, kThreads, false, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+        }
     }
 
     void invalidate_graph() {

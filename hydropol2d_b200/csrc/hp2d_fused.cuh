@@ -34,7 +34,10 @@
 namespace hp2d {
 
 constexpr int kStripOut = 28;   // output columns of a 32-lane strip (lanes 2..29)
-constexpr int kStages = 4;      // shared-memory ring depth of the row pipeline
+#ifndef HP2D_STAGES
+#define HP2D_STAGES 4
+#endif
+constexpr int kStages = HP2D_STAGES;   // shared-memory ring depth of the row pipeline
 #ifndef HP2D_ROW_UNROLL
 #define HP2D_ROW_UNROLL 1
 #endif
@@ -111,12 +114,13 @@ template <> __device__ __forceinline__ double bits_to<double>(unsigned long long
 
 // resident CTAs per SM the register budget is sized for (float: 8 x 128 threads)
 #ifndef HP2D_MINB_F32
-#define HP2D_MINB_F32 7
+#define HP2D_MINB_F32 8
 #endif
 template <typename R> struct FusedOcc { static constexpr int minb = HP2D_MINB_F32; };
 template <> struct FusedOcc<double> { static constexpr int minb = 3; };
 
-template <typename R, int NT>
+// GA: Green-Ampt infiltration on; MAP: rain from coarse maps (else a uniform rate)
+template <typename R, int NT, bool GA, bool MAP>
 __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const FusedArgs<R> a) {
     using V4 = typename Vec<R>::V4;
     using V2 = typename Vec<R>::V2;
@@ -159,7 +163,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     const V2* __restrict__ gin = cur ? a.gs1 : a.gs0;
     V2* __restrict__ gout = cur ? a.gs0 : a.gs1;
     const V4* __restrict__ stat = a.stat;
-    const float* map = s_map >= 0 ? a.rain.maps + size_t(s_map) * a.rain.my * a.rain.mx : nullptr;
+    const float* map = (MAP && s_map >= 0) ? a.rain.maps + size_t(s_map) * a.rain.my * a.rain.mx : nullptr;
     const R t_arr = R(s_tmin * 60.0 + s_dts);
     const R NaNR = R(__int_as_float(0x7fc00000));
 
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
             for (int k = 0; k < kStages && k <= last_k; ++k) issue(k);
         const V2 zero2 = {R(0), R(0)};
         V2 nG = zero2;
-        if (a.ga && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
+        if (GA && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
 #pragma unroll kRowUnroll
         for (int k = 0; k <= last_k; ++k) {
             const int r = r0 - 2 + k;
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                 issue(k + kStages);
             }
             const V2 Gs = nG;
-            if (a.ga && col_ok && r + 1 >= 0 && r + 1 < ny) nG = gin[size_t(r + 1) * nx + j];
+            if (GA && col_ok && r + 1 >= 0 && r + 1 < ny) nG = gin[size_t(r + 1) * nx + j];
             const bool ok = col_ok && r >= 0 && r < ny;
             const size_t c = size_t(r) * nx + j;
             const unsigned meta = meta_bits(S.w);
@@ -257,8 +261,8 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                 hh = hh + rr;
                 const bool own = own_lane && r >= r0 && r < r_end;
                 // uniform rain volume comes from the count of finite cells at the end
-                if (map && own && isfinite(hh)) rain_acc_r += rr;
-                if (a.ga) {
+                if (MAP && map && own && isfinite(hh)) rain_acc_r += rr;
+                if (GA) {
                     const unsigned s = meta & 255u;
                     V2 go = Gs;
                     if (s != 255u) {
