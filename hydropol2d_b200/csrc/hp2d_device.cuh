@@ -22,7 +22,9 @@ constexpr double kG = 9.81;
 
 // ---------------- x^(-1/3) by a fixed Newton iteration -------------------------------
 // Seed: dividing the IEEE exponent field by three (bits(x)/3 subtracted from the bits of
-// 2^(4/3 * bias)), then r <- r + r (1 - x r^3) / 3, quadratically convergent.
+// 2^(4/3 * bias)), then r <- r + r (1 - x r^3) / 3, quadratically convergent.  The residual
+// and the update are single fused multiply-adds (correctly rounded on every IEEE machine,
+// so the CPU restatement reproduces them exactly).
 template <typename R> struct RcbrtTraits;
 template <> struct RcbrtTraits<float> {
     static constexpr int iters = 3;
@@ -57,9 +59,8 @@ template <typename R> __device__ __forceinline__ R rcbrt(R x) {
     for (int it = 0; it < RcbrtTraits<R>::iters; ++it) {
         R t = x * r;
         t = t * r;
-        t = t * r;
-        R e = R(1) - t;
-        r = r + (r * e) * third;
+        const R e = fma(-t, r, R(1));
+        r = fma(r * e, third, r);
     }
     return r * scale;
 }

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     const int wg = blockIdx.x * (NT / 32) + warp;
 
     double rain_acc = 0.0, inf_acc = 0.0, out_acc = 0.0;
-    R rain_acc_r = R(0), inf_acc_r = R(0);   // per-lane partial sums (ledger only)
+    R rain_acc_r = R(0), inf_acc_r = R(0), out_acc_r = R(0);   // per-lane partial sums (ledger only)
     unsigned dry = 0u;                        // bit i: row r-i dry across the strip
     R s2max = R(0);
     unsigned long long cenc = 0ull;   // 0: no non-stagnant cell; else bits(value) + 1
@@ -205,17 +205,23 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
         const int last_k = (r_end + 1) - (r0 - 2);
         V4* ring = reinterpret_cast<V4*>(smem_dyn) + size_t(warp) * kStages * 64;
         const uint32_t bar0 = smem_addr(&s_bar[warp][0]);
+        // lane 0 arms the stage's barrier (arrive + expected bytes) and copies the static
+        // row, lane 1 copies the state row; a copy that lands before the arming only makes
+        // the transaction count negative for a moment, and the phase cannot complete
+        // before lane 0's arrival
+        const uint32_t ring_base = smem_addr(ring + seg_off);
+        const uint32_t bytes = uint32_t(seg_n) * uint32_t(sizeof(V4));
+        const V4* src_base = lane == 0 ? stat : sin;
+        const uint32_t dst_half = lane == 0 ? 0u : uint32_t(32 * sizeof(V4));
         auto issue = [&](int k) {
             const int s = k % kStages;
             const uint32_t bar = bar0 + 8u * s;
             const int rr = r0 - 2 + k;
             if (rr >= 0 && rr < ny && seg_n > 0) {
-                const uint32_t bytes = uint32_t(seg_n) * uint32_t(sizeof(V4));
-                mbar_expect_tx(bar, 2u * bytes);
-                const size_t g = size_t(rr) * nx + seg_j0;
-                bulk_g2s(smem_addr(ring + s * 64 + seg_off), stat + g, bytes, bar);
-                bulk_g2s(smem_addr(ring + s * 64 + 32 + seg_off), sin + g, bytes, bar);
-            } else {
+                if (lane == 0) mbar_expect_tx(bar, 2u * bytes);
+                bulk_g2s(ring_base + uint32_t(s) * uint32_t(64 * sizeof(V4)) + dst_half,
+                         src_base + (size_t(rr) * nx + seg_j0), bytes, bar);
+            } else if (lane == 0) {
                 mbar_arrive(bar);
             }
         };
@@ -224,7 +230,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
             mbar_fence_init();
         }
         __syncwarp();
-        if (lane == 0)
+        if (lane < 2)
             for (int k = 0; k < kStages && k <= last_k; ++k) issue(k);
         const V2 zero2 = {R(0), R(0)};
         V2 nG = zero2;
@@ -243,7 +249,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
             const V4 S = ring[s * 64 + lane];
             const V4 X = ring[s * 64 + 32 + lane];
             __syncwarp();
-            if (lane == 0 && k + kStages <= last_k) {
+            if (lane < 2 && k + kStages <= last_k) {
                 fence_proxy_async_smem();
                 issue(k + kStages);
             }
@@ -317,7 +323,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
                     hf3 = ho;
                     a.hf3[o] = ho;
                     a.qo[o] = qq;
-                    out_acc += double(qq * K.dt);
+                    out_acc_r += qq * K.dt;
                 }
                 const R dm = dm2;
                 if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
@@ -369,6 +375,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     __threadfence();
     rain_acc += double(rain_acc_r);
     inf_acc += double(inf_acc_r);
+    out_acc += double(out_acc_r);
     const int lane_ = tid & 31, warp_ = tid >> 5;
     s2max = warp_max(s2max);
     cenc = warp_max_u(cenc);

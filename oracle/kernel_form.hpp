@@ -16,7 +16,9 @@
 //   * Hf^(7/3), h^(5/3): x^2 * cbrt(x) and x * cbrt(x)^2 with cbrt(x) = x * r^2 and
 //     r = x^(-1/3) from a fixed Newton iteration (no libm), so that CPU and GPU round
 //     identically.  The seed is the exponent-field division of the IEEE representation
-//     (the classic bit-level log2 approximation), refined by r <- r + r(1 - x r^3)/3.
+//     (the classic bit-level log2 approximation), refined by r <- r + r(1 - x r^3)/3 with
+//     the residual and the update as explicit fused multiply-adds (std::fma here, fma on
+//     the GPU: both correctly rounded).
 //   * Draining limiter compares rates per unit width (both sides divided by dx).
 //   * CFL velocities q/Hf (refreshing_timestep.m:71-77 after unit cancellation); the
 //     minimum of alfa*dx/c over cells is taken as alfa*dx/max(c), which is exact because
@@ -69,9 +71,8 @@ template <typename R> inline R rcbrt(R x) {
     for (int it = 0; it < FB::iters; ++it) {
         R t = x * r;
         t = t * r;
-        t = t * r;
-        R e = R(1) - t;
-        r = r + (r * e) * third;
+        const R e = std::fma(-t, r, R(1));
+        r = std::fma(r * e, third, r);
     }
     return r * scale;
 }
