@@ -40,6 +40,10 @@ EXPORTS = [
     "hp2d_download",
     "hp2d_download_native", "hp2d_get_diag", "hp2d_stored_volume",
     "hp2d_cfl_dt_noalloc", "hp2d_noalloc_error",
+    "hp2d_autotune",
+    "hp2d_ensemble_create", "hp2d_ensemble_destroy", "hp2d_ensemble_last_error",
+    "hp2d_ensemble_add", "hp2d_ensemble_set_tuning", "hp2d_ensemble_autotune",
+    "hp2d_ensemble_steps", "hp2d_ensemble_steps_timed", "hp2d_ensemble_run",
 ]
 
 
@@ -127,6 +131,16 @@ def lib() -> C.CDLL:
         "hp2d_stored_volume": ([vp, dp], C.c_int),
         "hp2d_cfl_dt_noalloc": ([C.c_int32, C.c_int32, C.c_double, P(Params), vp, vp, vp, vp, dp, dp], C.c_int),
         "hp2d_noalloc_error": ([], C.c_char_p),
+        "hp2d_autotune": ([vp, C.c_int32, P(C.c_int32)], C.c_int),
+        "hp2d_ensemble_create": ([C.c_int32, P(vp)], C.c_int),
+        "hp2d_ensemble_destroy": ([vp], C.c_int),
+        "hp2d_ensemble_last_error": ([vp], C.c_char_p),
+        "hp2d_ensemble_add": ([vp, vp], C.c_int),
+        "hp2d_ensemble_set_tuning": ([vp, C.c_int32], C.c_int),
+        "hp2d_ensemble_autotune": ([vp, C.c_int32, P(C.c_int32)], C.c_int),
+        "hp2d_ensemble_steps": ([vp, C.c_int32, P(C.c_int32)], C.c_int),
+        "hp2d_ensemble_steps_timed": ([vp, C.c_int32, P(C.c_int32), P(C.c_float)], C.c_int),
+        "hp2d_ensemble_run": ([vp, C.c_int64, P(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

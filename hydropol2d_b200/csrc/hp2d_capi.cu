@@ -223,7 +223,7 @@ template <typename R> struct Impl : Base {
 
     hp2d_status upload_static(const double* z, const double* rough, const int32_t* rows, const int32_t* cols,
                               int32_t nout, const double* slopes) {
-        const double qnan = std::numeric_limits<double>::quiet_NaN();
+        const double edge = std::numeric_limits<double>::infinity();   // closed domain-edge face
         std::vector<std::pair<int32_t, R>> outs;
         for (int o = 0; o < nout; ++o) {
             if (rows[o] < 0 || rows[o] >= ny || cols[o] < 0 || cols[o] >= nx) {
@@ -256,8 +256,8 @@ template <typename R> struct Impl : Base {
         for (int i = 0; i < ny; ++i)
             for (int j = 0; j < nx; ++j) {
                 size_t k = size_t(i) * nx + j;
-                a[k] = R((j + 1 < nx) ? z[k + 1] - z[k] : qnan);
-                b[k] = R((i >= 1) ? z[k - nx] - z[k] : qnan);
+                a[k] = R((j + 1 < nx) ? z[k + 1] - z[k] : edge);
+                b[k] = R((i >= 1) ? z[k - nx] - z[k] : edge);
                 c[k] = R(rough[k] * rough[k]);
                 s[k] = V4{a[k], b[k], c[k], make_meta<R>(host_meta[k])};
             }
@@ -614,6 +614,87 @@ template <typename R> struct Impl : Base {
         return s;
     }
 
+    // ---------------- autotuning ----------------
+    // Copies of everything a fused step writes, so that trial steps can be undone.
+    struct Snapshot {
+        Dev<V4> st[2];
+        Dev<V2> gs[2];
+        Dev<R> arr, hf3s, qos;
+        Dev<StepScalars> scs;
+    };
+    template <typename T> void copy_dev(T* dst, const T* src, size_t count) {
+        if (count) HP_CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToDevice, st()));
+    }
+    void take(Snapshot& s) {
+        for (int b = 0; b < 2; ++b) {
+            s.st[b].alloc(n);
+            copy_dev(s.st[b].p, st4[b].p, n);
+            if (gs2[b].p) { s.gs[b].alloc(n); copy_dev(s.gs[b].p, gs2[b].p, n); }
+        }
+        s.arr.alloc(n);
+        copy_dev(s.arr.p, arrival.p, n);
+        if (n_out) {
+            s.hf3s.alloc(n_out); copy_dev(s.hf3s.p, hf3.p, n_out);
+            s.qos.alloc(n_out); copy_dev(s.qos.p, qo.p, n_out);
+        }
+        s.scs.alloc(1);
+        copy_dev(s.scs.p, sc.p, 1);
+        HP_CK(cudaStreamSynchronize(st()));
+    }
+    void put_back(const Snapshot& s) {
+        for (int b = 0; b < 2; ++b) {
+            copy_dev(st4[b].p, s.st[b].p, n);
+            if (gs2[b].p) copy_dev(gs2[b].p, s.gs[b].p, n);
+        }
+        copy_dev(arrival.p, s.arr.p, n);
+        if (n_out) { copy_dev(hf3.p, s.hf3s.p, n_out); copy_dev(qo.p, s.qos.p, n_out); }
+        copy_dev(sc.p, s.scs.p, 1);
+        HP_CK(cudaStreamSynchronize(st()));
+        pull_sc();
+    }
+
+    // Times `trial` fused steps per launch shape (rows each warp streams) from the current
+    // state, undoes them, and keeps the fastest shape.  Results never depend on the shape.
+    hp2d_status autotune(int32_t trial, int32_t* chosen) {
+        if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
+        if (ctx->p.flag_infiltration == 1 && n_classes == 0) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil"; return HP2D_NOT_READY; }
+        prologue();
+        Snapshot snap;
+        take(snap);
+        const int cands[] = {16, 24, 32, 48, 64, 96, 128};
+        const int keep = rows_per_warp;
+        int best = keep;
+        float best_ms = std::numeric_limits<float>::infinity();
+        bool timed_out = false;
+        cudaEvent_t e0, e1;
+        HP_CK(cudaEventCreate(&e0));
+        HP_CK(cudaEventCreate(&e1));
+        for (int c : cands) {
+            if (c > std::max(ny, 4) && c != 16) continue;
+            rows_per_warp = c;
+            const FusedArgs<R> a = fused_args();
+            launch_fused(a);   // warm-up
+            HP_CK(cudaEventRecord(e0, st()));
+            for (int s = 0; s < trial; ++s) launch_fused(a);
+            HP_CK(cudaEventRecord(e1, st()));
+            HP_CK(cudaGetLastError());
+            HP_CK(cudaEventSynchronize(e1));
+            float ms = 0;
+            HP_CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best_ms) { best_ms = ms; best = c; }
+            pull_sc();
+            timed_out = timed_out || (hs.status & 2u) != 0;
+            put_back(snap);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        rows_per_warp = best;
+        invalidate_graph();
+        if (timed_out) { ctx->err = "a row copy did not complete within its wait limit"; return HP2D_TIMEOUT; }
+        if (chosen) *chosen = best;
+        return HP2D_OK;
+    }
+
     hp2d_status run(int64_t max_steps, int64_t* done) {
         const double t_end = ctx->p.routing_time + ctx->p.min_time_step / 60.0;
         int64_t k0 = hs.k;
@@ -784,6 +865,206 @@ template <typename F> hp2d_status with_impl(hp2d_ctx* ctx, F&& fn) {
 
 }  // namespace
 
+// Batched ensemble: FP32 member contexts on one device advanced together, one persistent
+// launch per step (k_ens_plan + k_ens_step), chunks of steps captured in a CUDA graph.
+struct hp2d_ensemble {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::vector<hp2d_ctx*> members;
+    Dev<FusedArgs<float>> args;
+    Dev<unsigned> prefix;
+    Dev<EnsQueue> queue;
+    int rows_per_warp = 32;
+    int ga = -1, map = -1;
+    int grid = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_members = -1, graph_rpw = -1;
+
+    Impl<float>& impl(int m) { return *static_cast<Impl<float>*>(members[m]->impl.get()); }
+
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+
+    template <bool GA, bool MAP> void launch_t(int nm) {
+        const size_t smem = fused_smem_bytes<float>(kThreads);
+        if (grid == 0) {
+            int per_sm = 0, sms = 0;
+            HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<float, kThreads, GA, MAP>,
+                                                                kThreads, smem));
+            HP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+            grid = std::max(1, per_sm) * sms;
+        }
+        k_ens_plan<float><<<1, 1024, 0, stream>>>(args.p, nm, prefix.p, queue.p);
+        k_ens_step<float, kThreads, GA, MAP><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p, queue.p);
+    }
+    void launch(int nm) {
+        if (ga) {
+            if (map) launch_t<true, true>(nm); else launch_t<true, false>(nm);
+        } else {
+            if (map) launch_t<false, true>(nm); else launch_t<false, false>(nm);
+        }
+    }
+
+    // members' pending work done, their first-step prologues run, argument table current
+    hp2d_status prepare() {
+        const int nm = int(members.size());
+        if (nm == 0) { err = "the ensemble has no members"; return HP2D_NOT_READY; }
+        std::vector<FusedArgs<float>> host(nm);
+        for (int m = 0; m < nm; ++m) {
+            Impl<float>& im = impl(m);
+            if (!im.static_ready) { err = "member " + std::to_string(m) + ": hp2d_upload_static not called"; return HP2D_NOT_READY; }
+            if (members[m]->p.flag_infiltration == 1 && im.n_classes == 0) {
+                err = "member " + std::to_string(m) + ": flag_infiltration=1 needs hp2d_set_soil";
+                return HP2D_NOT_READY;
+            }
+            const int mga = im.ga() ? 1 : 0, mmap = im.rain.n_maps > 0 ? 1 : 0;
+            if (m == 0) { ga = mga; map = mmap; }
+            if (mga != ga || mmap != map) {
+                err = "members must agree on Green-Ampt infiltration and on the kind of rain forcing";
+                return HP2D_INVALID_ARG;
+            }
+            HP_CK(cudaSetDevice(device));
+            if (im.rows_per_warp != rows_per_warp) {
+                im.rows_per_warp = rows_per_warp;
+                im.invalidate_graph();
+            }
+            im.prologue();
+            HP_CK(cudaStreamSynchronize(im.st()));
+            host[m] = im.fused_args();
+        }
+        // a captured graph holds these pointers: reallocate (and recapture) only on a size change
+        if (args.n != size_t(nm)) {
+            drop_graph();
+            args.alloc(size_t(nm));
+            prefix.alloc(size_t(nm) + 1);
+        }
+        HP_CK(cudaMemcpyAsync(args.p, host.data(), host.size() * sizeof(FusedArgs<float>), cudaMemcpyHostToDevice, stream));
+        if (!queue.p) queue.alloc(1);
+        HP_CK(cudaStreamSynchronize(stream));
+        return HP2D_OK;
+    }
+
+    static constexpr int kChunk = 32;
+
+    hp2d_status steps(int32_t nsteps, int32_t* n_active) {
+        hp2d_status s = prepare();
+        if (s != HP2D_OK) return s;
+        const int nm = int(members.size());
+        int remaining = nsteps;
+        if (remaining >= kChunk) {
+            if (graph && (graph_members != nm || graph_rpw != rows_per_warp)) drop_graph();
+            if (!graph) {
+                cudaGraph_t gr;
+                HP_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                for (int k = 0; k < kChunk; ++k) launch(nm);
+                HP_CK(cudaStreamEndCapture(stream, &gr));
+                HP_CK(cudaGraphInstantiate(&graph, gr, 0));
+                HP_CK(cudaGraphDestroy(gr));
+                graph_members = nm;
+                graph_rpw = rows_per_warp;
+            }
+            while (remaining >= kChunk) {
+                HP_CK(cudaGraphLaunch(graph, stream));
+                remaining -= kChunk;
+            }
+        }
+        for (int k = 0; k < remaining; ++k) launch(nm);
+        HP_CK(cudaGetLastError());
+        // one more plan pass counts the members still running after these steps
+        k_ens_plan<float><<<1, 1024, 0, stream>>>(args.p, nm, prefix.p, queue.p);
+        EnsQueue q{};
+        HP_CK(cudaMemcpyAsync(&q, queue.p, sizeof(q), cudaMemcpyDeviceToHost, stream));
+        HP_CK(cudaStreamSynchronize(stream));
+        for (int m = 0; m < nm; ++m) impl(m).pull_sc();
+        if (n_active) *n_active = int32_t(q.n_active);
+        if (q.stalled) {
+            err = std::to_string(q.stalled) + " member(s) stopped: a row copy did not complete within its wait limit";
+            return HP2D_TIMEOUT;
+        }
+        return HP2D_OK;
+    }
+
+    hp2d_status run(int64_t max_steps, int64_t* launches) {
+        int64_t done = 0;
+        int32_t active = 1;
+        while (active > 0 && (max_steps <= 0 || done < max_steps)) {
+            const int64_t left = max_steps > 0 ? max_steps - done : int64_t(1) << 40;
+            const int32_t chunk = int32_t(std::min<int64_t>(left, 256));
+            hp2d_status s = steps(chunk, &active);
+            if (s != HP2D_OK) return s;
+            done += chunk;
+        }
+        if (launches) *launches = done;
+        return HP2D_OK;
+    }
+
+    // every member's state copied aside, trial steps per launch shape, state put back
+    hp2d_status autotune(int32_t trial, int32_t* chosen) {
+        const int cands[] = {8, 16, 24, 32, 48, 64};
+        const int nm = int(members.size());
+        std::vector<std::unique_ptr<Impl<float>::Snapshot>> snaps;
+        hp2d_status s = prepare();
+        if (s != HP2D_OK) return s;
+        for (int m = 0; m < nm; ++m) {
+            snaps.emplace_back(new Impl<float>::Snapshot());
+            impl(m).take(*snaps.back());
+        }
+        const int keep = rows_per_warp;
+        int best = keep;
+        float best_ms = std::numeric_limits<float>::infinity();
+        cudaEvent_t e0, e1;
+        HP_CK(cudaEventCreate(&e0));
+        HP_CK(cudaEventCreate(&e1));
+        bool stalled = false;
+        for (int c : cands) {
+            rows_per_warp = c;
+            s = prepare();
+            if (s != HP2D_OK) break;
+            launch(nm);   // warm-up
+            HP_CK(cudaEventRecord(e0, stream));
+            for (int k = 0; k < trial; ++k) launch(nm);
+            HP_CK(cudaEventRecord(e1, stream));
+            HP_CK(cudaGetLastError());
+            HP_CK(cudaEventSynchronize(e1));
+            float ms = 0;
+            HP_CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best_ms) { best_ms = ms; best = c; }
+            for (int m = 0; m < nm; ++m) {
+                impl(m).pull_sc();
+                stalled = stalled || (impl(m).hs.status & 2u) != 0;
+                impl(m).put_back(*snaps[m]);
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        rows_per_warp = best;
+        drop_graph();
+        if (s != HP2D_OK) return s;
+        if (stalled) { err = "a row copy did not complete within its wait limit"; return HP2D_TIMEOUT; }
+        if (chosen) *chosen = best;
+        return prepare();
+    }
+};
+
+namespace {
+template <typename F> hp2d_status ens_guarded(hp2d_ensemble* e, F&& fn) {
+    if (!e) return HP2D_INVALID_ARG;
+    try {
+        HP_CK(cudaSetDevice(e->device));
+        return fn();
+    } catch (const CudaFail& f) {
+        e->err = std::string(f.what) + ": " + cudaGetErrorString(f.e);
+        return HP2D_CUDA_ERROR;
+    } catch (const std::exception& ex) {
+        e->err = ex.what();
+        return HP2D_INVALID_ARG;
+    }
+}
+}  // namespace
+
 extern "C" {
 
 const char* hp2d_create_error(void) { return g_create_error.c_str(); }
@@ -947,6 +1228,107 @@ hp2d_status hp2d_get_diag(hp2d_ctx* ctx, hp2d_diag* out) {
 hp2d_status hp2d_stored_volume(hp2d_ctx* ctx, double* volume) {
     if (!volume) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.stored_volume(volume); });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+hp2d_status hp2d_autotune(hp2d_ctx* ctx, int32_t trial_steps, int32_t* rows_per_warp) {
+    if (trial_steps < 1) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) { return m.autotune(trial_steps, rows_per_warp); });
+}
+
+hp2d_status hp2d_ensemble_create(int32_t device, hp2d_ensemble** out) {
+    if (!out) return HP2D_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_create_error = "no CUDA device";
+        return HP2D_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) { g_create_error = "device index out of range"; return HP2D_INVALID_ARG; }
+    auto* e = new hp2d_ensemble();
+    e->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        g_create_error = "cannot create the ensemble's stream";
+        delete e;
+        return HP2D_CUDA_ERROR;
+    }
+    *out = e;
+    return HP2D_OK;
+}
+
+hp2d_status hp2d_ensemble_destroy(hp2d_ensemble* e) {
+    if (!e) return HP2D_INVALID_ARG;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    e->drop_graph();
+    e->args.free();
+    e->prefix.free();
+    e->queue.free();
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return HP2D_OK;
+}
+
+const char* hp2d_ensemble_last_error(const hp2d_ensemble* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+hp2d_status hp2d_ensemble_add(hp2d_ensemble* e, hp2d_ctx* member) {
+    return ens_guarded(e, [&]() -> hp2d_status {
+        if (!member || !member->impl) { e->err = "null member"; return HP2D_INVALID_ARG; }
+        if (member->g.precision != HP2D_FP32) { e->err = "ensemble members must be FP32 contexts"; return HP2D_INVALID_ARG; }
+        if (member->device != e->device) { e->err = "member lives on another device"; return HP2D_INVALID_ARG; }
+        for (auto* m : e->members)
+            if (m == member) { e->err = "member added twice"; return HP2D_INVALID_ARG; }
+        e->members.push_back(member);
+        e->drop_graph();
+        return HP2D_OK;
+    });
+}
+
+hp2d_status hp2d_ensemble_set_tuning(hp2d_ensemble* e, int32_t rows_per_warp) {
+    if (rows_per_warp < 4) return HP2D_INVALID_ARG;
+    return ens_guarded(e, [&]() -> hp2d_status {
+        e->rows_per_warp = rows_per_warp;
+        e->drop_graph();
+        return HP2D_OK;
+    });
+}
+
+hp2d_status hp2d_ensemble_autotune(hp2d_ensemble* e, int32_t trial_steps, int32_t* rows_per_warp) {
+    if (trial_steps < 1) return HP2D_INVALID_ARG;
+    return ens_guarded(e, [&]() { return e->autotune(trial_steps, rows_per_warp); });
+}
+
+hp2d_status hp2d_ensemble_steps(hp2d_ensemble* e, int32_t nsteps, int32_t* n_active) {
+    if (nsteps < 0) return HP2D_INVALID_ARG;
+    return ens_guarded(e, [&]() { return e->steps(nsteps, n_active); });
+}
+
+hp2d_status hp2d_ensemble_steps_timed(hp2d_ensemble* e, int32_t nsteps, int32_t* n_active, float* elapsed_ms) {
+    if (nsteps < 0 || !elapsed_ms) return HP2D_INVALID_ARG;
+    return ens_guarded(e, [&]() -> hp2d_status {
+        hp2d_status s = e->prepare();
+        if (s != HP2D_OK) return s;
+        cudaEvent_t e0, e1;
+        HP_CK(cudaEventCreate(&e0));
+        HP_CK(cudaEventCreate(&e1));
+        HP_CK(cudaEventRecord(e0, e->stream));
+        s = e->steps(nsteps, n_active);
+        HP_CK(cudaEventRecord(e1, e->stream));
+        HP_CK(cudaEventSynchronize(e1));
+        HP_CK(cudaEventElapsedTime(elapsed_ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return s;
+    });
+}
+
+hp2d_status hp2d_ensemble_run(hp2d_ensemble* e, int64_t max_steps, int64_t* steps_done) {
+    return ens_guarded(e, [&]() { return e->run(max_steps, steps_done); });
 }
 
 }  // extern "C"

@@ -177,6 +177,10 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
+// retire a barrier whose every phase has completed, before its word is initialised again
+__device__ __forceinline__ void mbar_inval(uint32_t bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ void mbar_fence_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -290,11 +294,19 @@ __device__ __forceinline__ R green_ampt(R& hh, R& Ic, R& Tc, const SoilClass<R>&
 // ---------------- one face of the local-inertial momentum update ----------------------
 // x face: (ha, hb) = (left, right) cells, dz = z_right - z_left.
 // y face: (ha, hb) = (upper, lower) cells (row i-1, row i), dz = z_upper - z_lower.
-// dz is NaN on closed faces (domain edge, idx_nan wall).
+// Closed faces carry a non-finite dz: +inf on the domain edge (Hf(:,end) = 0 and
+// Hf(1,:) = 0, Local_Inertial_Model_D4.m:139-140) and NaN next to a cell outside the
+// domain (idx_nan, NaN elevation).  There MATLAB's max ignores the NaN, so the face depth
+// is the inside cell's depth (:133-134) while the NaN slope sends q to 0 (:264); that
+// depth still enters the wave celerity of refreshing_timestep.
 template <typename R, bool IS_X>
 __device__ __forceinline__ void face_flux(R ha, R hb, R dz, R qp, R n2c, const StepConsts<R>& K,
                                           int flag_critical, R& Hf, R& q) {
-    if (isnan(dz)) { Hf = R(0); q = R(0); return; }
+    if (!(fabs(dz) <= R(3.0e38))) {
+        Hf = isnan(dz) ? fmax(fmax(ha, hb), R(0)) : R(0);
+        q = R(0);
+        return;
+    }
     ha = fmax(ha, R(0));
     hb = fmax(hb, R(0));
     R S;

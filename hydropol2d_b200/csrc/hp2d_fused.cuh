@@ -119,9 +119,14 @@ template <> __device__ __forceinline__ double bits_to<double>(unsigned long long
 template <typename R> struct FusedOcc { static constexpr int minb = HP2D_MINB_F32; };
 template <> struct FusedOcc<double> { static constexpr int minb = 3; };
 
+// One CTA-sized work item of the fused step: warps blk*NT/32 .. of the grid described by
+// `a`.  k_fused_step runs item blockIdx.x of one grid; k_ens_step runs items of many grids
+// pulled from a queue.  Every thread of the CTA calls it; it may return early for all of
+// them together.  Returns false when a row copy timed out (the CTA must stop using its
+// shared-memory ring).
 // GA: Green-Ampt infiltration on; MAP: rain from coarse maps (else a uniform rate)
 template <typename R, int NT, bool GA, bool MAP>
-__global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const FusedArgs<R> a) {
+__device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned blk) {
     using V4 = typename Vec<R>::V4;
     using V2 = typename Vec<R>::V2;
     constexpr unsigned FULL = 0xffffffffu;
@@ -148,10 +153,10 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
         s_rain = a.rain.n_uniform ? R(uniform_rate(a.rain, s_tmin)) : R(0);
         s_map = a.rain.n_maps ? map_index(a.rain, s_tmin) : -1;
-        if (!s_done && s_skip && blockIdx.x == 0) sc->neg_warn += 1;
+        if (!s_done && s_skip && blk == 0) sc->neg_warn += 1;
     }
     __syncthreads();
-    if (s_done) return;
+    if (s_done) return true;
 
     const StepConsts<R> K = s_K;
     const int ny = a.ny, nx = a.nx;
@@ -168,7 +173,7 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     const R NaNR = R(__int_as_float(0x7fc00000));
 
     const int lane = tid & 31, warp = tid >> 5;
-    const int wg = blockIdx.x * (NT / 32) + warp;
+    const int wg = int(blk) * (NT / 32) + warp;
 
     double rain_acc = 0.0, inf_acc = 0.0, out_acc = 0.0;
     R rain_acc_r = R(0), inf_acc_r = R(0), out_acc_r = R(0);   // per-lane partial sums (ledger only)
@@ -230,8 +235,10 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
             mbar_fence_init();
         }
         __syncwarp();
-        if (lane < 2)
+        if (lane < 2) {
+            fence_proxy_async_smem();   // reads of the ring by an earlier item come first
             for (int k = 0; k < kStages && k <= last_k; ++k) issue(k);
+        }
         const V2 zero2 = {R(0), R(0)};
         V2 nG = zero2;
         if (GA && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
@@ -239,7 +246,8 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
         for (int k = 0; k <= last_k; ++k) {
             const int r = r0 - 2 + k;
             const int s = k % kStages;
-            if (!mbar_wait_bounded(bar0 + 8u * s, uint32_t((k / kStages) & 1), 1u << 22)) {
+            const bool landed = mbar_wait_bounded(bar0 + 8u * s, uint32_t((k / kStages) & 1), 1u << 22);
+            if (__any_sync(FULL, !landed)) {   // the whole warp leaves the loop together
                 timed_out = true;
                 // let the copies still in flight land before the CTA leaves
                 for (int kk = k + 1; kk < k + kStages && kk <= last_k; ++kk)
@@ -292,9 +300,9 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
             if ((dry & 7u) != 7u) {
                 // (B) x face (r, j) between (r, j) and (r, j+1)
                 const R hR = __shfl_down_sync(FULL, hT0, 1);
-                if (ok && !isnan(S.x)) face_flux<R, true>(hT0, hR, S.x, X.y, S.z, K, a.flag_critical, hfx0, qxu0);
+                if (ok) face_flux<R, true>(hT0, hR, S.x, X.y, S.z, K, a.flag_critical, hfx0, qxu0);
                 // (C) y face (r, j) between (r-1, j) and (r, j)
-                if (ok && r >= r0 - 1 && !isnan(S.y))
+                if (ok && r >= r0 - 1)
                     face_flux<R, false>(hT1, hT0, S.y, X.z, S.z, K, a.flag_critical, hfy0, qyu0);
                 // (D) donor scale of (r-1, j)
                 const R qxu1_left = __shfl_up_sync(FULL, qxu1, 1);
@@ -367,6 +375,11 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
             dm2 = dm1; dm1 = X.w;
             mt2 = mt1; mt1 = meta;
         }
+        // every phase of the ring's barriers has completed: retire them so that the next
+        // item of a persistent CTA can initialise them again
+        __syncwarp();
+        if (lane == 0 && !timed_out)
+            for (int s = 0; s < kStages; ++s) mbar_inval(bar0 + 8u * s);
     }
 
     // ---- CTA reductions ---------------------------------------------------------------
@@ -414,7 +427,10 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
         s_last = (ticket == a.n_ctas - 1);
     }
     __syncthreads();
-    if (!s_last) return;
+    bool cta_ok = true;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) cta_ok = cta_ok && red_to[w] == 0;
+    if (!s_last) return cta_ok;
 
     // ---- last CTA: refreshing_timestep + clock (HydroPol2D_Main_While.m:691-705, :779)
     __threadfence();
@@ -485,6 +501,106 @@ __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const Fuse
     }
     neg = __syncthreads_or(neg);
     if (tid == 0) a.sc->skip_clamp = neg;
+    return cta_ok;
+}
+
+template <typename R, int NT, bool GA, bool MAP>
+__global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const FusedArgs<R> a) {
+    fused_item<R, NT, GA, MAP>(a, blockIdx.x);
+}
+
+// ---- batched ensemble ----------------------------------------------------------------
+// Members are independent grids, each with its own FusedArgs (clock, dt, buffers).  Each
+// step, k_ens_plan lists the CTA-sized items of the members still running (exclusive
+// prefix over members) and k_ens_step -- a persistent grid sized to the resident CTA
+// slots -- pulls items from a queue head.  Items of one launch never wait on each other;
+// the CTA that completes a member's last item refreshes that member's dt and clock.
+struct EnsQueue {
+    unsigned head;       // next item to hand out
+    unsigned total;      // items of this step
+    unsigned n_active;   // members running this step
+    unsigned stalled;    // members stopped by a failed row copy
+};
+
+template <typename R>
+__global__ void k_ens_plan(const FusedArgs<R>* __restrict__ members, int n_members, unsigned* prefix, EnsQueue* q) {
+    // one CTA of 1024 threads; members are scanned in chunks of 1024
+    __shared__ unsigned s_run[1024];
+    __shared__ unsigned s_base, s_act, s_stall;
+    const int tid = threadIdx.x;
+    if (tid == 0) { s_base = 0; s_act = 0; s_stall = 0; }
+    __syncthreads();
+    for (int m0 = 0; m0 < n_members; m0 += 1024) {
+        const int m = m0 + tid;
+        unsigned items = 0;
+        if (m < n_members) {
+            const FusedArgs<R>& a = members[m];
+            const StepScalars* sc = a.sc;
+            const bool stalled = (sc->status & 2u) != 0u;
+            const bool running = sc->t_min <= a.t_end && !stalled;
+            items = running ? a.n_ctas : 0u;
+            if (running) atomicAdd(&s_act, 1u);
+            if (stalled) atomicAdd(&s_stall, 1u);
+        }
+        s_run[tid] = items;
+        __syncthreads();
+        // Hillis-Steele inclusive scan over the chunk
+        for (int o = 1; o < 1024; o <<= 1) {
+            const unsigned v = tid >= o ? s_run[tid - o] : 0u;
+            __syncthreads();
+            s_run[tid] += v;
+            __syncthreads();
+        }
+        if (m < n_members) prefix[m] = s_base + s_run[tid] - items;
+        __syncthreads();
+        if (tid == 0) s_base += s_run[1023];
+        __syncthreads();
+    }
+    if (tid == 0) {
+        prefix[n_members] = s_base;
+        q->head = 0;
+        q->total = s_base;
+        q->n_active = s_act;
+        q->stalled = s_stall;
+    }
+}
+
+template <typename R, int NT, bool GA, bool MAP>
+__global__ void __launch_bounds__(NT, FusedOcc<R>::minb)
+k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsigned* __restrict__ prefix,
+           EnsQueue* q) {
+    __shared__ FusedArgs<R> s_a;
+    __shared__ unsigned s_item, s_local;
+    __shared__ int s_m;
+    const int tid = threadIdx.x;
+    const unsigned total = q->total;   // written by k_ens_plan before this launch
+    for (;;) {
+        __syncthreads();   // the previous item is finished with s_a and the ring
+        if (tid == 0) {
+            const unsigned it = atomicAdd(&q->head, 1u);
+            s_item = it;
+            if (it < total) {
+                // member m with prefix[m] <= it < prefix[m+1] (members without items have
+                // prefix[m] == prefix[m+1] and are passed over)
+                int lo = 0, hi = n_members - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (prefix[mid] <= it) lo = mid; else hi = mid - 1;
+                }
+                s_m = lo;
+                s_local = it - prefix[lo];
+            }
+        }
+        __syncthreads();
+        if (s_item >= total) return;
+        {
+            const unsigned* src = reinterpret_cast<const unsigned*>(members + s_m);
+            unsigned* dst = reinterpret_cast<unsigned*>(&s_a);
+            for (int w = tid; w < int(sizeof(FusedArgs<R>) / 4); w += NT) dst[w] = src[w];
+        }
+        __syncthreads();
+        if (!fused_item<R, NT, GA, MAP>(s_a, s_local)) return;   // ring unusable after a timeout
+    }
 }
 
 // Clamp-skip flag for the first fused step of a call, over every cell (the state may

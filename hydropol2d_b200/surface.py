@@ -143,6 +143,13 @@ class SurfaceFlow:
     def set_tuning(self, rows_per_warp: int):
         self._check(self._L.hp2d_set_tuning(self._h, int(rows_per_warp)))
 
+    def autotune(self, trial_steps: int = 4) -> int:
+        """Times ``trial_steps`` steps per launch shape from the current state, undoes them
+        and keeps the fastest; returns the chosen rows per warp."""
+        rpw = C.c_int32()
+        self._check(self._L.hp2d_autotune(self._h, int(trial_steps), C.byref(rpw)))
+        return rpw.value
+
     def run(self, max_steps: int = 0) -> int:
         done = C.c_int64()
         self._check(self._L.hp2d_run(self._h, int(max_steps), C.byref(done)))

@@ -176,3 +176,66 @@ def dambreak_case(ny: int = 4096, nx: int = 8192, dx: float = 5.0, seed: int = 1
                   slope_outlet=long_slope, min_time_step=0.01, max_time_step=10.0)
     return Case(f"dambreak_{ny}x{nx}_dx{dx:g}", z, np.full((ny, nx), 0.035), dx, rows, cols, params, d0,
                 meta=dict(x_dam=x_dam, wse=wse))
+
+
+def _side(rng, lo: int = 256, hi: int = 1024, mult: int = 32) -> int:
+    s = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+    return int(min(hi, max(lo, mult * round(s / mult))))
+
+
+def ensemble_member(i: int, seed: int = 2024, lo: int = 256, hi: int = 1024, breach_share: float = 0.25,
+                    rain_tail_min: float = 30.0, breach_minutes: float = 30.0) -> Case:
+    """Member ``i`` of the batched-ensemble configuration (HydroPol2D_Main_While_Ensemble.m
+    perturbs roughness and forcing per member; Probabilistic_dam_break_analysis.m varies the
+    breach).  Seeded per member:
+
+    * grid sides log-uniform in [lo, hi], multiples of 32 (ny and nx drawn separately);
+    * rain members (share 1 - breach_share): the V-tilted catchment of the 200 x 200 case
+      (dx 10 m, planes 0.005, channel 0.002) on the member's grid plus a member-seeded
+      random field (k^-3, 0.5 m std), Manning n = 0.02 x U(0.7, 1.3), uniform rain
+      U(20, 150) mm/h for U(30, 90) min, simulated to the end of rain + ``rain_tail_min``;
+    * breach members: the dam-break valley on the member's grid (dx 5 m, valley depth and
+      random field scaled with the grid's width), a wall across the valley at 5 % of the
+      length with a breach of U(0.2, 1.0) x the valley width around the thalweg, n = 0.035
+      x U(0.7, 1.3), ``breach_minutes`` simulated.
+    """
+    rng = np.random.default_rng([seed, i])
+    ny, nx = _side(rng, lo, hi), _side(rng, lo, hi)
+    nfac = float(rng.uniform(0.7, 1.3))
+    if rng.uniform() >= breach_share:
+        dx = 10.0
+        z, ch = vtilt_domain(ny, nx, dx, 0.005, 0.002)
+        z = z + 0.5 * gaussian_random_field(ny, nx, -3.0, seed * 7919 + i)
+        rate = float(rng.uniform(20.0, 150.0))
+        dur = float(rng.uniform(30.0, 90.0))
+        rows = np.zeros(ch.size, dtype=np.int32)
+        params = dict(routing_time=dur + rain_tail_min, alfa_min=0.7, alfa_max=0.7, outlet_type=1,
+                      slope_outlet=0.002, min_time_step=0.01, max_time_step=10.0)
+        return Case(f"member{i}_rain_{ny}x{nx}", z, np.full((ny, nx), 0.02 * nfac), dx, rows,
+                    ch.astype(np.int32), params, np.zeros((ny, nx)),
+                    rain_uniform=(np.array([0.0, dur]), np.array([rate, 0.0])),
+                    meta=dict(kind="rain", rate=rate, duration=dur, n_factor=nfac))
+    dx = 5.0
+    f = float(rng.uniform(0.2, 1.0))
+    scale = ny / 4096.0
+    grf = gaussian_random_field(ny, nx, -3.0, seed * 7919 + i) * 5.0 * scale
+    y = (np.arange(ny) + 0.5) / ny * 2.0 - 1.0
+    x = np.arange(nx) * dx
+    z = 60.0 * scale * (y[:, None] ** 2) + 0.001 * (x[-1] - x)[None, :] + grf + 20.0
+    x_dam = max(2, int(round(0.05 * nx)))
+    half = max(1, int(round(0.5 * f * ny)))
+    thalweg_row = int(np.argmin(z[:, x_dam]))
+    lo_r, hi_r = max(0, thalweg_row - half), min(ny, thalweg_row + half)
+    wse = float(z[thalweg_row, x_dam]) + 30.0 * max(scale, 0.25)
+    wall = np.ones(ny, dtype=bool)
+    wall[lo_r:hi_r] = False
+    z[wall, x_dam] = wse + 5.0
+    d0 = np.zeros((ny, nx))
+    d0[:, :x_dam] = np.maximum(wse - z[:, :x_dam], 0.0) * 1000.0
+    rows = np.arange(ny, dtype=np.int32)
+    cols = np.full(ny, nx - 1, dtype=np.int32)
+    params = dict(routing_time=breach_minutes, alfa_min=0.5, alfa_max=0.7, outlet_type=1,
+                  slope_outlet=0.001, min_time_step=0.01, max_time_step=10.0)
+    return Case(f"member{i}_breach_{ny}x{nx}", z, np.full((ny, nx), 0.035 * nfac), dx, rows, cols,
+                params, d0, rain_uniform=(np.array([0.0]), np.array([0.0])),
+                meta=dict(kind="breach", breach_factor=f, n_factor=nfac, x_dam=x_dam))

@@ -181,6 +181,10 @@ hp2d_status hp2d_fused_steps_timed(hp2d_ctx* ctx, int32_t nsteps, float* elapsed
 /* Launch shape of the fused kernel: rows each warp streams through (>= 4).  Results do
  * not depend on it; hp2d_autotune picks it per grid. */
 hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp);
+/* Autotuner (no counterpart in the reference): times `trial_steps` fused steps from the
+ * current state for each launch shape, undoes them (the state, clock and maxima are copied
+ * aside first), keeps the fastest shape and returns it in *rows_per_warp (nullable). */
+hp2d_status hp2d_autotune(hp2d_ctx* ctx, int32_t trial_steps, int32_t* rows_per_warp);
 /* Runs until the clock passes routing_time (or max_steps); returns steps executed. */
 hp2d_status hp2d_run(hp2d_ctx* ctx, int64_t max_steps, int64_t* steps_done);
 
@@ -197,6 +201,32 @@ hp2d_status hp2d_download_native(hp2d_ctx* ctx, int32_t field, void* host, size_
 hp2d_status hp2d_get_diag(hp2d_ctx* ctx, hp2d_diag* out);
 /* Stored surface volume sum(d_t)*cell_area/1000 [m^3], FP64 accumulation. */
 hp2d_status hp2d_stored_volume(hp2d_ctx* ctx, double* volume);
+
+/* ---- batched ensemble ------------------------------------------------------------- */
+/* Replaces the member loop of HydroPol2D_Main_While_Ensemble.m:46-139 (and the per-member
+ * runs of Probabilistic_dam_break_analysis.m:8-60), which call the surface-flow step once
+ * per member in turn.  Members are ordinary FP32 contexts, each set up with the calls
+ * above (own grid size, DEM, roughness, rain or initial state, clock and dt); the ensemble
+ * advances every member that has not reached its routing_time by one of its own steps per
+ * launch: one persistent kernel whose CTAs take (member, block of rows) items from a
+ * queue, with each member's dt refresh and clock advance done by the CTA that completes
+ * its last item.  Members must agree on Green-Ampt on/off and on uniform vs map rain.
+ * While in an ensemble a member must not be stepped on its own concurrently; its
+ * outputs are read with hp2d_download / hp2d_get_diag as usual. */
+typedef struct hp2d_ensemble hp2d_ensemble;
+hp2d_status hp2d_ensemble_create(int32_t device, hp2d_ensemble** out);
+hp2d_status hp2d_ensemble_destroy(hp2d_ensemble* ens);
+const char* hp2d_ensemble_last_error(const hp2d_ensemble* ens);
+hp2d_status hp2d_ensemble_add(hp2d_ensemble* ens, hp2d_ctx* member);
+/* rows each warp streams (>= 4) for every member; hp2d_ensemble_autotune picks it */
+hp2d_status hp2d_ensemble_set_tuning(hp2d_ensemble* ens, int32_t rows_per_warp);
+hp2d_status hp2d_ensemble_autotune(hp2d_ensemble* ens, int32_t trial_steps, int32_t* rows_per_warp);
+/* nsteps launches; *n_active (nullable) = members still running afterwards */
+hp2d_status hp2d_ensemble_steps(hp2d_ensemble* ens, int32_t nsteps, int32_t* n_active);
+hp2d_status hp2d_ensemble_steps_timed(hp2d_ensemble* ens, int32_t nsteps, int32_t* n_active,
+                                      float* elapsed_ms);
+/* until every member has reached its routing_time (or max_steps launches, if > 0) */
+hp2d_status hp2d_ensemble_run(hp2d_ensemble* ens, int64_t max_steps, int64_t* steps_done);
 
 /* ---- allocation-free timestep (no counterpart in the reference) -------------------- */
 /* refreshing_timestep's refresh branch (as hp2d_cfl_dt) on caller-owned FP32 device

@@ -161,12 +161,13 @@ public:
 
     void upload_static(const double* z, const double* n, const int32_t* rows, const int32_t* cols,
                        int nout, const double* slopes) {
-        const double qnan = std::numeric_limits<double>::quiet_NaN();
+        // domain-edge faces +inf, faces next to a NaN elevation NaN (see face())
+        const double edge = std::numeric_limits<double>::infinity();
         for (int i = 0; i < ny; ++i)
             for (int j = 0; j < nx; ++j) {
                 size_t c = at(i, j);
-                double dx_ = (j + 1 < nx) ? z[at(i, j + 1)] - z[c] : qnan;
-                double dy_ = (i >= 1) ? z[at(i - 1, j)] - z[c] : qnan;
+                double dx_ = (j + 1 < nx) ? z[at(i, j + 1)] - z[c] : edge;
+                double dy_ = (i >= 1) ? z[at(i - 1, j)] - z[c] : edge;
                 dzx[c] = R(dx_);
                 dzy[c] = R(dy_);
                 n2[c] = R(n[c] * n[c]);
@@ -324,7 +325,14 @@ public:
     // one face: returns (Hf, q) from neighbour depths; for x faces (a, b) = (L, R);
     // for y faces (a, b) = (U, D) and dz = z_U - z_D, so the roles of max/min swap.
     inline void face(R ha, R hb, R dz, R qp, R n2c, bool is_x, const Consts<R>& K, R& Hf, R& q) const {
-        if (std::isnan(dz)) { Hf = R(0); q = R(0); return; }
+        // non-finite dz: +inf on the domain edge (Hf = 0, Local_Inertial_Model_D4.m:139-140),
+        // NaN next to an idx_nan cell: MATLAB's max skips the NaN, so Hf is the inside
+        // cell's depth (:133-134) and the NaN slope sends q to 0 (:264)
+        if (!(std::fabs(dz) <= R(3.0e38))) {
+            Hf = std::isnan(dz) ? std::fmax(std::fmax(ha, hb), R(0)) : R(0);
+            q = R(0);
+            return;
+        }
         ha = std::fmax(ha, R(0));
         hb = std::fmax(hb, R(0));
         R S;

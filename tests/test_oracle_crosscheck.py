@@ -55,10 +55,12 @@ def test_full_loop_vtilt_agrees(oracle_lib):
     assert np.allclose(dm, st.dmax, rtol=1e-9, atol=1e-9)
 
 
-@pytest.mark.parametrize("seed", [1, 2, 3])
-def test_li_step_agrees_on_random_states(oracle_lib, seed):
-    """One Local_Inertial_Model_D4 call on a random wet state with random prior fluxes."""
-    case = random_terrain(23, 37, seed=seed, walls=False)
+@pytest.mark.parametrize("seed,walls", [(1, False), (2, False), (3, False), (4, True), (5, True)])
+def test_li_step_agrees_on_random_states(oracle_lib, seed, walls):
+    """One Local_Inertial_Model_D4 call on a random wet state with random prior fluxes; with
+    walls, cells of NaN elevation (idx_nan) whose faces keep the inside cell's depth as Hf
+    (MATLAB's max skips NaN) while passing no flow."""
+    case = random_terrain(23, 37, seed=seed, walls=walls)
     rng = np.random.default_rng(seed)
     ny, nx = case.shape
     outflow = np.zeros((3, ny, nx))
@@ -67,6 +69,7 @@ def test_li_step_agrees_on_random_states(oracle_lib, seed):
     outflow[0][:, -1] = 0
     outflow[1][0, :] = 0
     d = np.where(rng.random((ny, nx)) < 0.7, rng.uniform(0, 500, (ny, nx)), 0.0)
+    d[np.isnan(case.z)] = np.nan
     ts = 0.5 / 60
     lit = L.local_inertial_model_d4(case.z, d, case.roughness, case.roughness ** 2, case.resolution ** 2, ts,
                                     case.resolution, case.outlet_rows, case.outlet_cols, 1,
@@ -75,13 +78,16 @@ def test_li_step_agrees_on_random_states(oracle_lib, seed):
     o.set_state(d, outflow)
     o.li_step(ts)
     h = o.download_native("h") * 1000
-    assert np.allclose(h, lit.d_t, rtol=1e-12, atol=1e-12)
+    assert np.allclose(h, lit.d_t, rtol=1e-12, atol=1e-12, equal_nan=True)
     qr = o.download_native("qx") * 3.6e6 / case.resolution
     qu = o.download_native("qy") * 3.6e6 / case.resolution
     assert np.allclose(qr, lit.qout_right, rtol=1e-11, atol=1e-9)
     assert np.allclose(qu, lit.qout_up, rtol=1e-11, atol=1e-9)
     assert np.allclose(o.download_native("hfx"), lit.Hf[0], rtol=1e-12, atol=1e-14)
     assert np.allclose(o.download_native("hfy"), lit.Hf[1], rtol=1e-12, atol=1e-14)
+    if walls:
+        nan_face = np.isnan(case.z[:, 1:]) ^ np.isnan(case.z[:, :-1])
+        assert (lit.Hf[0][:, :-1][nan_face] > 0).any()   # the rule is exercised
     # refreshing_timestep on that state
     cfl = L.refreshing_timestep(lit.Hf, lit.qout_right, lit.qout_up, case.resolution, 1.0, 0.5, 0.7, 10.0,
                                 0.01, 0.001)
