@@ -47,6 +47,17 @@ EXPORTS = [
 ]
 
 
+# every symbol include/hp2d_nn.h declares (the learned screening network's kernels)
+NN_EXPORTS = [
+    "hp2d_nn_gemm", "hp2d_nn_check", "hp2d_nn_error", "hp2d_nn_im2col3x3", "hp2d_nn_transpose",
+    "hp2d_nn_maxpool2", "hp2d_nn_maxpool2_bwd", "hp2d_nn_upsample2", "hp2d_nn_upsample2_bwd",
+    "hp2d_nn_copy_channels", "hp2d_nn_relu_bwd", "hp2d_nn_colsum", "hp2d_nn_mse", "hp2d_nn_adam",
+    "hp2d_nn_flip3x3", "hp2d_nn_f32_to_bf16",
+]
+
+NN_EPI = {"f32": 0, "f32_atomic": 1, "bf16_bias_relu": 2, "bf16_bias": 3, "f32_bias": 4}
+
+
 class Grid(C.Structure):
     _fields_ = [("ny", C.c_int32), ("nx", C.c_int32), ("resolution", C.c_double),
                 ("precision", C.c_int32)]
@@ -142,6 +153,25 @@ def lib() -> C.CDLL:
         "hp2d_ensemble_steps_timed": ([vp, C.c_int32, P(C.c_int32), P(C.c_float)], C.c_int),
         "hp2d_ensemble_run": ([vp, C.c_int64, P(C.c_int64)], C.c_int),
     }
+    i32, i64, f32 = C.c_int32, C.c_int64, C.c_float
+    sig.update({
+        "hp2d_nn_gemm": ([i32, i32, i32, vp, i32, vp, i32, vp, i32, vp, i32, i32, vp], C.c_int),
+        "hp2d_nn_check": ([], C.c_int),
+        "hp2d_nn_error": ([], C.c_char_p),
+        "hp2d_nn_im2col3x3": ([vp, i32, i32, i32, i32, vp, i32, i32, vp], C.c_int),
+        "hp2d_nn_transpose": ([vp, i32, i32, i32, vp, i32, vp], C.c_int),
+        "hp2d_nn_maxpool2": ([vp, i32, i32, i32, i32, vp, vp], C.c_int),
+        "hp2d_nn_maxpool2_bwd": ([vp, vp, vp, i32, i32, i32, i32, vp, i32, vp], C.c_int),
+        "hp2d_nn_upsample2": ([vp, i32, i32, i32, i32, vp, vp], C.c_int),
+        "hp2d_nn_upsample2_bwd": ([vp, i32, i32, i32, i32, vp, vp], C.c_int),
+        "hp2d_nn_copy_channels": ([vp, i32, i32, i32, i64, vp, i32, i32, vp], C.c_int),
+        "hp2d_nn_relu_bwd": ([vp, vp, i64, vp], C.c_int),
+        "hp2d_nn_colsum": ([vp, i64, i32, i32, vp, vp], C.c_int),
+        "hp2d_nn_mse": ([vp, i32, vp, vp, i64, i32, f32, vp, vp, i32, vp], C.c_int),
+        "hp2d_nn_adam": ([vp, vp, vp, vp, vp, i64, f32, f32, f32, f32, f32, i32, vp], C.c_int),
+        "hp2d_nn_flip3x3": ([vp, i32, i32, i32, vp, i32, vp], C.c_int),
+        "hp2d_nn_f32_to_bf16": ([vp, vp, i64, vp], C.c_int),
+    })
     for name, (args, res) in sig.items():
         f = getattr(L, name)
         f.argtypes = args

@@ -11,17 +11,18 @@ from hydropol2d_b200 import _abi
 ROOT = Path(__file__).resolve().parent.parent
 
 
-def declared_symbols():
-    text = (ROOT / "include" / "hp2d.h").read_text()
+def declared_symbols(header="hp2d.h"):
+    text = (ROOT / "include" / header).read_text()
     return sorted(set(re.findall(r"^\s*(?:hp2d_status|const char\*)\s+(hp2d_\w+)\s*\(", text, re.M)))
 
 
 def test_header_and_binding_agree():
     assert declared_symbols() == sorted(_abi.EXPORTS)
+    assert declared_symbols("hp2d_nn.h") == sorted(_abi.NN_EXPORTS)
 
 
 def test_library_exports_every_declared_symbol(hp2d_lib):
-    for name in declared_symbols():
+    for name in declared_symbols() + declared_symbols("hp2d_nn.h"):
         assert hasattr(hp2d_lib, name), name
 
 
