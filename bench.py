@@ -189,6 +189,57 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def ensemble_leg(device: int, n_members: int = 256) -> dict:
+    """The batched-ensemble configuration: 256 members with sides log-uniform in
+    [256, 1024] (multiples of 32), rain or breach forcing, run to their own end times in one
+    persistent launch per step; the launch shape is autotuned first (trial steps undone)."""
+    from hydropol2d_b200 import SurfaceFlow, synthetic as S
+    from hydropol2d_b200.ensemble import Ensemble
+    t0 = time.perf_counter()
+    cases = [S.ensemble_member(i) for i in range(n_members)]
+    t_gen = time.perf_counter() - t0
+    ens = Ensemble(device)
+    for c in cases:
+        g = SurfaceFlow(*c.shape, c.resolution, "fp32", device=device, **c.params)
+        c.apply(g)
+        ens.add(g)
+    rpw = ens.autotune(8)
+    total_ms, launches, active = 0.0, 0, n_members
+    while active:
+        active, ms = ens.steps_timed(512)
+        total_ms += ms
+        launches += 512
+    cu = ens.cell_updates()
+    ks = [m.diag()["k"] - 1 for m in ens.members]
+    cells = ens.cells()
+    ens.close()
+    sec = total_ms / 1e3
+    return {"members": n_members, "members_per_h": n_members / sec * 3600, "seconds": sec,
+            "gcups": cu / sec / 1e9, "cells": cells, "launches": launches, "rows_per_warp": rpw,
+            "steps_min": min(ks), "steps_max": max(ks), "steps_mean": float(np.mean(ks)),
+            "breach_members": sum(c.meta["kind"] == "breach" for c in cases),
+            "input_generation_s": t_gen,
+            "timing": "CUDA events on the ensemble's stream around every launch until the last "
+                      "member reaches its routing_time"}
+
+
+def run_surrogate(args):
+    """Learned screening at the configuration's size: 4096 solver runs on 256 x 256 tiles
+    train three U-Nets; 1024 held-out members are screened (inference + reruns of members
+    whose networks disagree by more than 5 cm) and compared with the plain batched solver
+    and, on a subset, with the FP64 solver."""
+    from hydropol2d_b200 import build, screening
+    build.build()
+    res = screening.study(n_train=4096, n_test=1024, size=256, epochs=args.surrogate_epochs,
+                          batch=16, n_fp64=64, log=lambda m: print(m, file=sys.stderr, flush=True))
+    line = {"metric": "ensemble members/h", "value": res["screened_members_per_h"], "unit": "members/h",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "bf16 network / f32 solver",
+            "data": "synthetic (seeded members, hydropol2d_b200.synthetic.ensemble_member, 256 x 256)",
+            "config": {"workload": "screening_4096train_1024test_256x256", "threshold_m": 0.05},
+            "vs_baseline": None, "impl": "ours", "study": res}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -198,12 +249,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-member ensemble leg")
+    ap.add_argument("--late-steps", type=int, default=10000,
+                    help="steps the dam-break advances before the late-window measurement (0: skip)")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="run the learned-screening study instead (4096 training / 1024 held-out members)")
+    ap.add_argument("--surrogate-epochs", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.surrogate:
+        run_surrogate(args)
         return
 
     import torch
@@ -240,6 +300,18 @@ def main():
     ms_per_step = ms / args.steps
     value = cells * args.steps * world / (ms / 1e3) / 1e9
     d = sf.diag()
+    wet_main = float(np.mean(sf.download_native("h") > 0))
+    late = None
+    if args.late_steps > 0:
+        # the same run later on, once the flood wave has spread over more of the valley
+        sf.fused_steps(args.late_steps)
+        ms_late = sf.fused_steps_timed(args.steps)
+        h = sf.download_native("h")
+        d_late = sf.diag()
+        late = {"after_steps": args.warmup + args.steps + args.late_steps, "sim_clock_min": d_late["t"],
+                "wet_fraction": float(np.mean(h > 0)), "ms_per_step": ms_late / args.steps,
+                "value": cells * args.steps / (ms_late / 1e3) / 1e9,
+                "wet_fraction_main_window": wet_main}
     sf.close()
 
     # ---- end to end through the C ABI with host buffers ------------------------------
@@ -281,6 +353,10 @@ def main():
             dist.destroy_process_group()
         return
 
+    ens = None
+    if world == 1 and not args.no_ensemble:
+        ens = ensemble_leg(local)
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         v, sample, cores = cpu_port_gcups(15.0)
@@ -294,7 +370,8 @@ def main():
         "config": {"workload": WORKLOAD, "ny": ny, "nx": nx, "dx_m": DX, "cells": cells,
                    "parallelism": f"{world} independent members (one per GPU)" if world > 1 else "single grid",
                    "l2": "state 1.5 GB per step > 126 MB L2; no flush needed",
-                   "sim_clock_min_after": d["t"], "dt_s_last": d["time_step"] * 60},
+                   "sim_clock_min_after": d["t"], "dt_s_last": d["time_step"] * 60,
+                   "wet_fraction": wet_main},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_cell": BYTES_PER_CELL,
@@ -304,6 +381,8 @@ def main():
                 "d2h_bytes_per_step": d2h_per_step, "steps": e2e_steps,
                 "includes": "input generation excluded; static+state upload, per-step hydrograph "
                             "and clock readback, final depth and dmax readback"},
+        "late_window": late,
+        "ensemble": ens,
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),
         "input_generation_s": t_gen,

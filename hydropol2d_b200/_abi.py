@@ -8,7 +8,10 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libhp2d.so"
+import os
+
+# the in-tree build; HP2D_LIBRARY names another build of the same library (A/B timing)
+LIB_PATH = Path(os.environ.get("HP2D_LIBRARY") or Path(__file__).resolve().parent / "libhp2d.so")
 
 HP2D_FP32 = 0
 HP2D_FP64 = 1

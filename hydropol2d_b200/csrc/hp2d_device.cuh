@@ -9,8 +9,9 @@
 //   green_ampt     HydroPol2D_Main_While_Ensemble.m:274-298 with Infiltration_Module.m
 //                  :179 and :444-445 (supply and depth update)
 //   cfl_cell       refreshing_timestep.m:61-89, :139-150, :181-238
-// The whole library is compiled with -fmad=false: every a*b+c below rounds twice, so the
-// results are reproducible on any IEEE machine that evaluates the same expressions.
+// The whole library is compiled with -fmad=false: every a*b+c below rounds twice unless it
+// is written as fma() (one rounding, as std::fma on the CPU), so the results are
+// reproducible on any IEEE machine that evaluates the same expressions.
 #pragma once
 
 #include <cstdint>
@@ -66,6 +67,34 @@ template <typename R> __device__ __forceinline__ R rcbrt(R x) {
 }
 template <typename R> __device__ __forceinline__ R pow73(R x) {
     if (!(x > R(0))) return R(0);
+    R r = rcbrt(x);
+    R c = x * (r * r);
+    return (x * x) * c;
+}
+// ---------------- quotient a / b for b > 0 ---------------------------------------------
+// FP32: the reciprocal from a bit-level seed (0x7EF311C3 minus the bits of b, relative
+// error below 1/8), three Newton steps r <- r + r (1 - b r) (the error squares each step),
+// then a r with one residual correction q + (a - b q) r.  Branch-free and built only from
+// IEEE multiplies and fused multiply-adds, so the CPU restatement reproduces it bit for
+// bit; within about one ulp of the IEEE quotient.  b is raised to the smallest normal
+// float first (the seed needs a normal b; a quotient by anything smaller is either zero
+// or discarded by the callers' clips).  FP64 uses the IEEE division.
+__device__ __forceinline__ float qdiv(float a, float b) {
+    b = fmaxf(b, 1.17549435e-38f);
+    float r = __uint_as_float(0x7EF311C3u - __float_as_uint(b));
+    float e = fmaf(-b, r, 1.0f);
+    r = fmaf(r, e, r);
+    e = fmaf(-b, r, 1.0f);
+    r = fmaf(r, e, r);
+    e = fmaf(-b, r, 1.0f);
+    r = fmaf(r, e, r);
+    const float q = a * r;
+    return fmaf(fmaf(-b, q, a), r, q);
+}
+__device__ __forceinline__ double qdiv(double a, double b) { return a / b; }
+
+// x^(7/3) for x > 0 (callers that have established it)
+template <typename R> __device__ __forceinline__ R pow73_pos(R x) {
     R r = rcbrt(x);
     R c = x * (r * r);
     return (x * x) * c;
@@ -299,10 +328,13 @@ __device__ __forceinline__ R green_ampt(R& hh, R& Ic, R& Tc, const SoilClass<R>&
 // domain (idx_nan, NaN elevation).  There MATLAB's max ignores the NaN, so the face depth
 // is the inside cell's depth (:133-134) while the NaN slope sends q to 0 (:264); that
 // depth still enters the wave celerity of refreshing_timestep.
+// Faces that carry no water leave early: whole warps of them skip the power and the
+// division, which matters on wet/dry fronts.
 template <typename R, bool IS_X>
 __device__ __forceinline__ void face_flux(R ha, R hb, R dz, R qp, R n2c, const StepConsts<R>& K,
                                           int flag_critical, R& Hf, R& q) {
     if (!(fabs(dz) <= R(3.0e38))) {
+        // NaN dz: MATLAB's max over the two sides skips the NaN one
         Hf = isnan(dz) ? fmax(fmax(ha, hb), R(0)) : R(0);
         q = R(0);
         return;
@@ -318,10 +350,10 @@ __device__ __forceinline__ void face_flux(R ha, R hb, R dz, R qp, R n2c, const S
         S = (dz + (ha - hb)) * K.inv_dx;
     }
     if (!(Hf > R(0))) { q = R(0); return; }
-    R num = qp - (K.gdt * Hf) * S;
-    R h73 = pow73(Hf);
-    R den = h73 + (K.gdt * n2c) * fabs(qp);
-    R qq = (num * h73) / den;
+    R num = fma(-(K.gdt * Hf), S, qp);   // one rounding for qp - (g dt Hf) S
+    R h73 = pow73_pos(Hf);
+    R den = fma(K.gdt * n2c, fabs(qp), h73);
+    R qq = qdiv(num * h73, den);
     if (!isfinite(qq)) qq = R(0);
     if (flag_critical == 1) {
         R crit = Hf * sqrt(K.g * Hf);
@@ -374,6 +406,8 @@ __device__ __forceinline__ R limit_face(R q, R s_pos, R s_neg) {
 
 template <typename R>
 __device__ __forceinline__ R continuity(R htot, R qL, R qR, R qU, R qD, const StepConsts<R>& K) {
+    // separately rounded product and sum, as the reference evaluates it: a cell drained by
+    // the limiter then ends at (or clamps to) zero alike in FP32 and FP64
     R hn = htot + K.dt_over_dx * (((qL - qR) - qU) + qD);
     if (hn < R(0)) hn = R(0);
     return hn;
@@ -399,9 +433,9 @@ __device__ __forceinline__ void cfl_cell(R qx, R qy, R qyb, R hfx, R hfy, R hfyb
     R sx = hfx < K.tol ? big : hfx;
     R sy = hfy < K.tol ? big : hfy;
     R sb = hfyb < K.tol ? big : hfyb;
-    R vr = qx / sx;
-    R vu = qy / sy;
-    R vb = qyb / sb;
+    R vr = qdiv(qx, sx);
+    R vu = qdiv(qy, sy);
+    R vb = qdiv(qyb, sb);
     R rc = first_col ? R(0.5) * vr : vr;
     R uc = R(0.5) * (vu + vb);
     speed = sqrt(rc * rc + uc * uc);

@@ -179,7 +179,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     R rain_acc_r = R(0), inf_acc_r = R(0), out_acc_r = R(0);   // per-lane partial sums (ledger only)
     unsigned dry = 0u;                        // bit i: row r-i dry across the strip
     R s2max = R(0);
-    unsigned long long cenc = 0ull;   // 0: no non-stagnant cell; else bits(value) + 1
+    R cmaxv = R(-1);   // largest celerity term of a non-stagnant cell (-1: none yet)
 
     if (wg < a.n_warps_total) {
         const int strip = wg % a.n_strips;
@@ -338,9 +338,9 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
                 if (!quiet) {
                     const R big = R(1e9);
-                    const R vr = qxl2 == R(0) ? qxl2 : qxl2 / (hfx2 < K.tol ? big : hfx2);
-                    const R vu = qyl2 == R(0) ? qyl2 : qyl2 / (hfy2 < K.tol ? big : hfy2);
-                    const R vb = qyl1 == R(0) ? qyl1 : qyl1 / (hfy1 < K.tol ? big : hfy1);
+                    const R vr = qxl2 == R(0) ? qxl2 : qdiv(qxl2, hfx2 < K.tol ? big : hfx2);
+                    const R vu = qyl2 == R(0) ? qyl2 : qdiv(qyl2, hfy2 < K.tol ? big : hfy2);
+                    const R vb = qyl1 == R(0) ? qyl1 : qdiv(qyl1, hfy1 < K.tol ? big : hfy1);
                     const R rc = j == 0 ? R(0.5) * vr : vr;
                     const R uc = R(0.5) * (vu + vb);
                     const R s2 = rc * rc + uc * uc;
@@ -354,8 +354,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                             const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
                             cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
                         }
-                        const unsigned long long e = ord_bits(cval) + 1ull;
-                        cenc = e > cenc ? e : cenc;
+                        cmaxv = fmax(cmaxv, cval);
                     }
                 }
                 V4 o4;
@@ -391,6 +390,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     out_acc += double(out_acc_r);
     const int lane_ = tid & 31, warp_ = tid >> 5;
     s2max = warp_max(s2max);
+    // 0: no non-stagnant cell; else the bits of the (non-negative, +0 for -0) maximum + 1
+    unsigned long long cenc = cmaxv >= R(0) ? ord_bits(cmaxv + R(0)) + 1ull : 0ull;
     cenc = warp_max_u(cenc);
     rain_acc = warp_sum(rain_acc);
     inf_acc = warp_sum(inf_acc);

@@ -68,9 +68,9 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_cfl_partials_noalloc(
         const float hfb = last ? 0.f : hf[n + c + nx];
         const float hfx = hf[c], hfy = hf[n + c], hf3 = hf[2 * n + c];
         const float big = 1e9f;
-        const float vr = qx[c] / (hfx < K.tol ? big : hfx);
-        const float vu = qy[c] / (hfy < K.tol ? big : hfy);
-        const float vb = qyb / (hfb < K.tol ? big : hfb);
+        const float vr = hp2d::qdiv(qx[c], hfx < K.tol ? big : hfx);
+        const float vu = hp2d::qdiv(qy[c], hfy < K.tol ? big : hfy);
+        const float vb = hp2d::qdiv(qyb, hfb < K.tol ? big : hfb);
         const float rc = j == 0 ? 0.5f * vr : vr;
         const float uc = 0.5f * (vu + vb);
         const float s2 = rc * rc + uc * uc;

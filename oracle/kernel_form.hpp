@@ -89,6 +89,27 @@ template <typename R> inline R pow53(R x) {       // x^(5/3), x >= 0
     return x * (c * c);
 }
 
+// a / b for b > 0 as the kernels compute it: FP32 reciprocal from the bit seed
+// 0x7EF311C3 - bits(b), three Newton steps, quotient with one residual correction
+// (b raised to the smallest normal first); FP64 the IEEE division.
+inline float qdiv(float a, float b) {
+    b = std::fmax(b, 1.17549435e-38f);
+    uint32_t u;
+    std::memcpy(&u, &b, 4);
+    u = 0x7EF311C3u - u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    float e = std::fma(-b, r, 1.0f);
+    r = std::fma(r, e, r);
+    e = std::fma(-b, r, 1.0f);
+    r = std::fma(r, e, r);
+    e = std::fma(-b, r, 1.0f);
+    r = std::fma(r, e, r);
+    const float q = a * r;
+    return std::fma(std::fma(-b, q, a), r, q);
+}
+inline double qdiv(double a, double b) { return a / b; }
+
 template <typename R> inline bool finite(R v) { return std::isfinite(v); }
 
 template <typename R> struct Consts {
@@ -344,10 +365,10 @@ public:
             S = (dz + (ha - hb)) * K.inv_dx;
         }
         if (!(Hf > R(0))) { q = R(0); return; }
-        R num = qp - (K.gdt * Hf) * S;
+        R num = std::fma(-(K.gdt * Hf), S, qp);
         R h73 = pow73(Hf);
-        R den = h73 + (K.gdt * n2c) * std::fabs(qp);
-        q = (num * h73) / den;
+        R den = std::fma(K.gdt * n2c, std::fabs(qp), h73);
+        q = qdiv(num * h73, den);
         if (!std::isfinite(q)) q = R(0);
         if (p.flag_critical == 1) {
             R crit = Hf * std::sqrt(K.g * Hf);
@@ -456,13 +477,13 @@ public:
                 size_t c = at(i, j);
                 R sx = hfx[c] < K.tol ? K.big_depth : hfx[c];
                 R sy = hfy[c] < K.tol ? K.big_depth : hfy[c];
-                R vr = qx[c] / sx;
-                R vu = qy[c] / sy;
+                R vr = qdiv(qx[c], sx);
+                R vu = qdiv(qy[c], sy);
                 R vb = R(0);
                 if (i + 1 < ny) {
                     size_t cb = at(i + 1, j);
                     R sb = hfy[cb] < K.tol ? K.big_depth : hfy[cb];
-                    vb = qy[cb] / sb;
+                    vb = qdiv(qy[cb], sb);
                 }
                 R rc = (j == 0) ? K.half * vr : vr;
                 R uc = K.half * (vu + vb);

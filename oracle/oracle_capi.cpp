@@ -163,6 +163,10 @@ void oracle_pow_check(int32_t precision, int32_t n, const double* x, double* p73
     }
 }
 
+void oracle_qdiv_check(int32_t n, const float* a, const float* b, float* q) {
+    for (int i = 0; i < n; ++i) q[i] = hp2d_oracle::qdiv(a[i], b[i]);
+}
+
 int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
     return dispatch(m, [&](auto& M) {
         o->t = M.t_min;

@@ -132,3 +132,29 @@ def test_rcbrt_accuracy(oracle_lib):
         ok = xr > (1e-15 if prec == 0 else 1e-130)   # results above the smallest normal
         assert np.all(np.abs(a[ok] / xr[ok] ** (7 / 3) - 1) < tol)
         assert np.all(np.abs(b[ok] / xr[ok] ** (5 / 3) - 1) < tol)
+
+
+def test_qdiv_within_one_ulp(oracle_lib):
+    """The kernels' FP32 quotient (seeded reciprocal, three Newton steps, one residual
+    correction) against the exact quotient: at most one ulp off, over quotients spanning
+    the ranges the step produces (fluxes over face depths and Bates denominators)."""
+    import ctypes as C
+    import oracle
+    L_ = oracle._load()
+    f = L_.oracle_qdiv_check
+    fp = C.POINTER(C.c_float)
+    f.argtypes = [C.c_int32, fp, fp, fp]
+    rng = np.random.default_rng(0)
+    n = 200000
+    a = (rng.uniform(-1, 1, n) * 10.0 ** rng.uniform(-20, 5, n)).astype(np.float32)
+    b = (10.0 ** rng.uniform(-30, 9, n)).astype(np.float32)
+    a[:5] = [0.0, -0.0, 1.0, 3.0, -7.0]
+    b[:5] = [3.0, 3.0, 3.0, 1e-3, 1e9]
+    q = np.empty(n, dtype=np.float32)
+    f(n, a.ctypes.data_as(fp), b.ctypes.data_as(fp), q.ctypes.data_as(fp))
+    exact = a.astype(np.float64) / b.astype(np.float64)
+    fin = np.isfinite(exact) & (np.abs(exact) < 3e38) & (np.abs(exact) > 1e-37)
+    ulp = np.spacing(np.abs(exact[fin]).astype(np.float32)).astype(np.float64)
+    err = np.abs(q[fin].astype(np.float64) - exact[fin]) / ulp
+    assert err.max() <= 1.0, err.max()
+    assert q[0] == 0.0 and q[1] == 0.0   # a zero numerator gives a zero (its sign is not kept)
