@@ -52,7 +52,7 @@ EXPORTS = [
 
 # every symbol include/hp2d_nn.h declares (the learned screening network's kernels)
 NN_EXPORTS = [
-    "hp2d_nn_gemm", "hp2d_nn_check", "hp2d_nn_error", "hp2d_nn_im2col3x3", "hp2d_nn_transpose",
+    "hp2d_nn_gemm", "hp2d_nn_conv3x3", "hp2d_nn_check", "hp2d_nn_error", "hp2d_nn_im2col3x3", "hp2d_nn_transpose",
     "hp2d_nn_maxpool2", "hp2d_nn_maxpool2_bwd", "hp2d_nn_upsample2", "hp2d_nn_upsample2_bwd",
     "hp2d_nn_copy_channels", "hp2d_nn_relu_bwd", "hp2d_nn_colsum", "hp2d_nn_mse", "hp2d_nn_adam",
     "hp2d_nn_flip3x3", "hp2d_nn_f32_to_bf16",
@@ -159,6 +159,7 @@ def lib() -> C.CDLL:
     i32, i64, f32 = C.c_int32, C.c_int64, C.c_float
     sig.update({
         "hp2d_nn_gemm": ([i32, i32, i32, vp, i32, vp, i32, vp, i32, vp, i32, i32, vp], C.c_int),
+        "hp2d_nn_conv3x3": ([vp, i32, i32, i32, i32, vp, i32, i32, vp, vp, i32, i32, vp], C.c_int),
         "hp2d_nn_check": ([], C.c_int),
         "hp2d_nn_error": ([], C.c_char_p),
         "hp2d_nn_im2col3x3": ([vp, i32, i32, i32, i32, vp, i32, i32, vp], C.c_int),

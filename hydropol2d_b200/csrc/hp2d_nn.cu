@@ -40,17 +40,34 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// K-major BF16 matrix [rows, K] with pitch ld (elements), box 64 x box_rows, 128-byte swizzle
-bool make_map(CUtensorMap* m, const void* base, int rows, int K, int ld, int box_rows) {
+// K-major BF16 matrix [rows, K] with pitch ld (elements), box kb x box_rows; 128-byte swizzle
+// for 64-element (128-byte) rows, 64-byte swizzle for 32-element rows
+bool make_map(CUtensorMap* m, const void* base, int rows, int K, int ld, int box_rows, int kb = kBK) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[2] = {cuuint64_t(K), cuuint64_t(rows)};
     cuuint64_t strides[1] = {cuuint64_t(ld) * 2};
-    cuuint32_t box[2] = {cuuint32_t(kBK), cuuint32_t(box_rows)};
+    cuuint32_t box[2] = {cuuint32_t(kb), cuuint32_t(box_rows)};
     cuuint32_t estr[2] = {1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+              CU_TENSOR_MAP_INTERLEAVE_NONE, kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// NHWC BF16 activations [B, H, W, C] as a 4-D map (C innermost); box kb channels x
+// min(W, 128) pixels x 128/min(W,128) rows x 1 image = the 128 pixels of one GEMM tile.
+// Coordinates outside the image read as zeros (the convolution's padding).
+bool make_map_nhwc(CUtensorMap* m, const void* base, int B, int H, int W, int C, int kb) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const int bw = W < kBM ? W : kBM;
+    cuuint64_t dims[4] = {cuuint64_t(C), cuuint64_t(W), cuuint64_t(H), cuuint64_t(B)};
+    cuuint64_t strides[3] = {cuuint64_t(C) * 2, cuuint64_t(W) * C * 2, cuuint64_t(H) * W * C * 2};
+    cuuint32_t box[4] = {cuuint32_t(kb), cuuint32_t(bw), cuuint32_t(kBM / bw), 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 hp2d_status fail(const std::string& msg, hp2d_status st = HP2D_INVALID_ARG) {
@@ -99,8 +116,43 @@ hp2d_status gemm_bn(int M, int N, int K, const void* A, int lda, const void* B, 
     int* err = err_ptr();
     if (!err) return fail("cannot resolve the error flag", HP2D_CUDA_ERROR);
     dim3 grid((M + kBM - 1) / kBM, (N + BN - 1) / BN, splits);
-    k_gemm_bf16<BN><<<grid, 128, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi, err);
+    k_gemm_bf16<BN><<<grid, 128, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi, err, ConvGeom{0, 0, 0});
     return launched("k_gemm_bf16");
+}
+
+template <int BN, int KB>
+hp2d_status conv_bn(const void* x, int B, int H, int W, int Cin, const void* w, int ldw, int Co, const float* bias,
+                    void* y, int ldy, int epi, cudaStream_t st) {
+    static bool attr_set[8] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smem = gemm_smem_bytes<BN, KB>();
+    if (dev < 8 && !attr_set[dev]) {
+        if (cudaFuncSetAttribute(k_gemm_bf16<BN, KB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
+            cudaSuccess)
+            return launched("cudaFuncSetAttribute");
+        attr_set[dev] = true;
+    }
+    CUtensorMap ma, mb;
+    if (!make_map_nhwc(&ma, x, B, H, W, Cin, KB) || !make_map(&mb, w, Co, 9 * Cin, ldw, BN, KB))
+        return fail("cuTensorMapEncodeTiled rejected an operand (alignment or pitch)");
+    int* err = err_ptr();
+    if (!err) return fail("cannot resolve the error flag", HP2D_CUDA_ERROR);
+    const int M = B * H * W;
+    const int kt = 9 * Cin / KB;
+    dim3 grid(M / kBM, (Co + BN - 1) / BN, 1);
+    k_gemm_bf16<BN, KB, true><<<grid, 128, smem, st>>>(ma, mb, M, Co, kt, kt, y, ldy, bias, epi, err,
+                                                       ConvGeom{H, W, Cin / KB});
+    return launched("k_gemm_bf16 (implicit convolution)");
+}
+
+template <int KB>
+hp2d_status conv_kb(const void* x, int B, int H, int W, int Cin, const void* w, int ldw, int Co, const float* bias,
+                    void* y, int ldy, int epi, cudaStream_t st) {
+    if (Co <= 32) return conv_bn<32, KB>(x, B, H, W, Cin, w, ldw, Co, bias, y, ldy, epi, st);
+    if (Co <= 64) return conv_bn<64, KB>(x, B, H, W, Cin, w, ldw, Co, bias, y, ldy, epi, st);
+    if (Co <= 128) return conv_bn<128, KB>(x, B, H, W, Cin, w, ldw, Co, bias, y, ldy, epi, st);
+    return conv_bn<256, KB>(x, B, H, W, Cin, w, ldw, Co, bias, y, ldy, epi, st);
 }
 
 inline cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
@@ -383,6 +435,24 @@ hp2d_status hp2d_nn_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t
     if (N <= 64) return gemm_bn<64>(M, N, K, A, lda, B, ldb, C, ldc, bias, epi, split_k, st);
     if (N <= 128) return gemm_bn<128>(M, N, K, A, lda, B, ldb, C, ldc, bias, epi, split_k, st);
     return gemm_bn<256>(M, N, K, A, lda, B, ldb, C, ldc, bias, epi, split_k, st);
+}
+
+hp2d_status hp2d_nn_conv3x3(const uint16_t* x, int32_t B, int32_t H, int32_t W, int32_t C, const uint16_t* w,
+                            int32_t ldw, int32_t Co, const float* bias, void* y, int32_t ldy, int32_t epi,
+                            void* stream) {
+    if (!x || !w || !y || B <= 0 || H <= 0 || W <= 0 || Co <= 0) return fail("conv3x3: bad shape");
+    if (C < 32 || C % 32) return fail("conv3x3: the input needs a multiple of 32 channels");
+    const bool rows_ok = (W % kBM == 0) || (kBM % W == 0 && H % (kBM / W) == 0);
+    if (!rows_ok || (int64_t(H) * W) % kBM) return fail("conv3x3: H*W must tile into 128-pixel rows or row groups");
+    if (ldw < 9 * C || ldw % 8 || !aligned16(x) || !aligned16(w)) return fail("conv3x3: weight pitch or alignment");
+    if (ldy < Co) return fail("conv3x3: ldy < Co");
+    if (epi != HP2D_NN_EPI_F32 && epi != HP2D_NN_EPI_BF16_BIAS_RELU && epi != HP2D_NN_EPI_BF16_BIAS &&
+        epi != HP2D_NN_EPI_F32_BIAS)
+        return fail("conv3x3: unsupported epilogue");
+    if (epi != HP2D_NN_EPI_F32 && !bias) return fail("conv3x3: bias epilogue without bias");
+    cudaStream_t st = S(stream);
+    if (C % 64 == 0) return conv_kb<64>(x, B, H, W, C, w, ldw, Co, bias, y, ldy, epi, st);
+    return conv_kb<32>(x, B, H, W, C, w, ldw, Co, bias, y, ldy, epi, st);
 }
 
 hp2d_status hp2d_nn_im2col3x3(const uint16_t* x, int32_t B, int32_t H, int32_t W, int32_t C, uint16_t* cols,

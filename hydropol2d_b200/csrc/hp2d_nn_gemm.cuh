@@ -38,15 +38,29 @@ enum Epilogue : int {
     EPI_F32_BIAS = 4,
 };
 
-template <int BN> constexpr size_t gemm_smem_bytes() {
-    return size_t(kGemmStages) * (kBM * kBK * 2 + BN * kBK * 2) + 1024;   // + alignment slack
+template <int BN, int KB = kBK> constexpr size_t gemm_smem_bytes() {
+    return size_t(kGemmStages) * (kBM * KB * 2 + BN * KB * 2) + 1024;   // + alignment slack
 }
+
+// Geometry of an implicit-GEMM 3x3 convolution (A is read straight from the NHWC input):
+// the 128 output pixels of a tile are 128 consecutive pixels of one image (W >= 128) or
+// 128/W whole rows (W < 128); k tile kt is tap kt / cblocks, channel block kt % cblocks.
+struct ConvGeom {
+    int H, W, cblocks;
+};
 
 // ---- PTX wrappers ----------------------------------------------------------------------
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
         ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
         : "memory");
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -99,6 +113,19 @@ __device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t smem_addr) {
     d |= uint64_t(2u) << 61;                 // 128-byte swizzle
     return d;
 }
+// 32-element (64-byte) rows with the 64-byte swizzle: groups of 8 rows 512 bytes apart
+__device__ __forceinline__ uint64_t sw64_kmajor_desc(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= uint64_t((smem_addr >> 4) & 0x3FFFu);
+    d |= uint64_t(1u) << 16;
+    d |= uint64_t(512u >> 4) << 32;          // stride byte offset: 8 rows x 64 B
+    d |= uint64_t(1u) << 46;
+    d |= uint64_t(4u) << 61;                 // 64-byte swizzle
+    return d;
+}
+template <int KB> __device__ __forceinline__ uint64_t kmajor_desc(uint32_t a) {
+    return KB == 64 ? sw128_kmajor_desc(a) : sw64_kmajor_desc(a);
+}
 // instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = BN
 template <int BN> __device__ __forceinline__ constexpr uint32_t bf16_idesc() {
     return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) | (uint32_t(kBM >> 4) << 24);
@@ -113,14 +140,18 @@ __device__ __forceinline__ uint16_t f2bf(float f) {
     return __bfloat16_as_ushort(__float2bfloat16_rn(f));
 }
 
-template <int BN>
+// KB: k-tile depth (64 with the 128-byte swizzle, 32 with the 64-byte swizzle); IM2COL: A is
+// the NHWC input of a 3x3 convolution read through a 4-D tensor map (see ConvGeom).
+template <int BN, int KB = kBK, bool IM2COL = false>
 __global__ void __launch_bounds__(128, 1)
 k_gemm_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M, int N,
             int kt_total, int kt_per_split, void* C, int ldc, const float* __restrict__ bias, int epi,
-            int* err) {
+            int* err, const ConvGeom g) {
     static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN");
-    constexpr uint32_t kABytes = kBM * kBK * 2;
-    constexpr uint32_t kBBytes = BN * kBK * 2;
+    static_assert(KB == 64 || KB == 32, "KB");
+    static_assert(KB == 64 || IM2COL, "32-deep tiles are for 32-channel convolutions");
+    constexpr uint32_t kABytes = kBM * KB * 2;
+    constexpr uint32_t kBBytes = BN * KB * 2;
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) unsigned long long bar_full[kGemmStages], bar_empty[kGemmStages], bar_done;
     __shared__ uint32_t s_tmem;
@@ -151,6 +182,14 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
     int issued = 0;
     if (tid == 0 && nk > 0) {
         // producer: TMA tiles of A (rows m0..) and B (rows n0..), k tile kt0 + i
+        int img = 0, y0 = 0, x0 = 0;
+        if (IM2COL) {
+            const int hw = g.H * g.W;
+            img = m0 / hw;
+            const int rem = m0 - img * hw;
+            y0 = rem / g.W;
+            x0 = rem - y0 * g.W;
+        }
         for (int i = 0; i < nk; ++i) {
             const int s = i % kGemmStages;
             const uint32_t fb = smem_addr(&bar_full[s]);
@@ -159,8 +198,15 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
                 break;
             }
             mbar_expect_tx(fb, kABytes + kBBytes);
-            const int kx = (kt0 + i) * kBK;
-            tma_load_2d(sA0 + uint32_t(s) * kABytes, &tmA, kx, m0, fb);
+            const int kt = kt0 + i;
+            const int kx = kt * KB;
+            if (IM2COL) {
+                // tap (dy, dx) shifts the pixel box; TMA fills outside the image with zeros
+                const int tap = kt / g.cblocks, cb = kt - tap * g.cblocks;
+                tma_load_4d(sA0 + uint32_t(s) * kABytes, &tmA, cb * KB, x0 + tap % 3 - 1, y0 + tap / 3 - 1, img, fb);
+            } else {
+                tma_load_2d(sA0 + uint32_t(s) * kABytes, &tmA, kx, m0, fb);
+            }
             tma_load_2d(sB0 + uint32_t(s) * kBBytes, &tmB, kx, n0, fb);
             issued = i + 1;
         }
@@ -174,10 +220,10 @@ k_gemm_bf16(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
                 break;
             }
             tc_fence_after();
-            const uint64_t da = sw128_kmajor_desc(sA0 + uint32_t(s) * kABytes);
-            const uint64_t db = sw128_kmajor_desc(sB0 + uint32_t(s) * kBBytes);
+            const uint64_t da = kmajor_desc<KB>(sA0 + uint32_t(s) * kABytes);
+            const uint64_t db = kmajor_desc<KB>(sB0 + uint32_t(s) * kBBytes);
 #pragma unroll
-            for (int kk = 0; kk < kBK / 16; ++kk)   // +32 bytes per K=16 step inside the swizzled row
+            for (int kk = 0; kk < KB / 16; ++kk)   // +32 bytes per K=16 step inside the swizzled row
                 tc_mma_bf16(tmem, da + uint64_t(2 * kk), db + uint64_t(2 * kk), idesc, (i | kk) != 0 ? 1u : 0u);
             tc_commit(smem_addr(&bar_empty[s]));
         }

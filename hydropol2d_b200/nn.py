@@ -50,6 +50,23 @@ def gemm(A: torch.Tensor, B: torch.Tensor, C_out: torch.Tensor, epilogue: str = 
                           _p(bias), EPI[epilogue], int(split_k), _stream()))
 
 
+def conv_ok(x_shape) -> bool:
+    """Whether ``conv3x3`` (implicit GEMM) takes an NHWC input of this shape."""
+    _, H, W, Cc = x_shape
+    rows_ok = W % 128 == 0 or (128 % W == 0 and H % (128 // W) == 0)
+    return Cc >= 32 and Cc % 32 == 0 and rows_ok and (H * W) % 128 == 0
+
+
+def conv3x3(x: torch.Tensor, w16: torch.Tensor, Co: int, out: torch.Tensor, epilogue: str,
+            bias: torch.Tensor | None = None):
+    """out[P, Co] (epilogue) = 3x3 convolution of x [B, H, W, C] with w16 [Co, >= 9C] (bf16,
+    K index (ky*3 + kx)*C + c), as an implicit GEMM (no im2col buffer)."""
+    Bn, H, W, Cc = x.shape
+    assert x.is_contiguous() and w16.stride(1) == 1 and out.stride(1) == 1
+    _ok(_L().hp2d_nn_conv3x3(_p(x), Bn, H, W, Cc, _p(w16), w16.stride(0), Co, _p(bias), _p(out), out.stride(0),
+                             EPI[epilogue], _stream()))
+
+
 def im2col3x3(x: torch.Tensor, Kp: int, transpose: bool = False, out: torch.Tensor | None = None):
     Bn, H, W, Cc = x.shape
     P = Bn * H * W

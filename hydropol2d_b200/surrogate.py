@@ -8,9 +8,11 @@ screens ensemble members: an ensemble of independently trained networks predicts
 member's peak-depth map, and members on which the networks disagree by more than a
 threshold go back to the solver (``screening``).
 
-Layout: activations NHWC BF16; a 3x3 convolution is im2col + GEMM
-``y[P, Co] = cols[P, Kp] . W[Co, Kp]^T`` with K index (ky*3 + kx)*Ci + ci; backward gives
-``dW = dy^T . cols`` (split-K GEMM over pixels) and ``dx = im2col(dy) . Wflip^T``.
+Layout: activations NHWC BF16; a 3x3 convolution is ``y[P, Co] = cols[P, Kp] . W[Co, Kp]^T``
+with K index (ky*3 + kx)*Ci + ci, computed as an implicit GEMM that reads tap-shifted boxes of
+the input through TMA (``nn.conv3x3``) where the shape allows, else as im2col + GEMM; backward
+gives ``dx`` as the convolution of dy with the flipped kernel (same two forms) and
+``dW = dy^T . cols`` (split-K GEMM over pixels).
 """
 from __future__ import annotations
 
@@ -86,13 +88,13 @@ class Conv3x3:
     def forward(self, x: torch.Tensor, keep: bool = True):
         B, H, W, _ = x.shape
         P = B * H * W
-        cols = nn.im2col3x3(x, self.kp)
-        if self.name == "head":
-            y = torch.empty(P, self.co, dtype=torch.float32, device=x.device)
-            nn.gemm(cols, self.W16, y, "f32_bias", bias=self.b)
+        head = self.name == "head"
+        y = torch.empty(P, self.co, dtype=torch.float32 if head else torch.bfloat16, device=x.device)
+        epi = "f32_bias" if head else ("bf16_bias_relu" if self.relu else "bf16_bias")
+        if nn.conv_ok(x.shape):
+            nn.conv3x3(x.contiguous(), self.W16, self.co, y, epi, bias=self.b)   # implicit GEMM
         else:
-            y = torch.empty(P, self.co, dtype=torch.bfloat16, device=x.device)
-            nn.gemm(cols, self.W16, y, "bf16_bias_relu" if self.relu else "bf16_bias", bias=self.b)
+            nn.gemm(nn.im2col3x3(x, self.kp), self.W16, y, epi, bias=self.b)
         if keep:
             self.x, self.y = x, y
         return y.view(B, H, W, self.co)
@@ -114,9 +116,12 @@ class Conv3x3:
         if not need_dx:
             return None
         wt = nn.flip3x3(self.W, self.co, self.ci, self.kp, self.kp2)
-        dcols = nn.im2col3x3(dy2.view(B, H, W, self.co), self.kp2)
         dx = torch.empty(P, self.ci, dtype=torch.bfloat16, device=x.device)
-        nn.gemm(dcols, wt, dx, "bf16_bias", bias=self.zero_ci)
+        dyv = dy2.view(B, H, W, self.co)
+        if nn.conv_ok(dyv.shape):
+            nn.conv3x3(dyv, wt, self.ci, dx, "bf16_bias", bias=self.zero_ci)
+        else:
+            nn.gemm(nn.im2col3x3(dyv, self.kp2), wt, dx, "bf16_bias", bias=self.zero_ci)
         return dx.view(B, H, W, self.ci)
 
 

@@ -37,6 +37,14 @@ enum {
 hp2d_status hp2d_nn_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const void* B,
                          int32_t ldb, void* C, int32_t ldc, const float* bias, int32_t epilogue,
                          int32_t split_k, void* stream);
+/* 3x3, stride-1, zero-padded convolution as an implicit GEMM on the same tensor cores:
+ * y[P, Co] (epilogue) = conv(x, w) with x [B,H,W,C] NHWC BF16 read through a 4-D tensor map
+ * (no im2col buffer), w [Co, 9C] K-major BF16 (pitch ldw, K index (ky*3+kx)*C + c), P = B*H*W.
+ * C a multiple of 32; W a multiple of 128 or a divisor of 128 with H*W a multiple of 128.
+ * Epilogues F32, F32_BIAS, BF16_BIAS, BF16_BIAS_RELU. */
+hp2d_status hp2d_nn_conv3x3(const uint16_t* x, int32_t B, int32_t H, int32_t W, int32_t C, const uint16_t* w,
+                            int32_t ldw, int32_t Co, const float* bias, void* y, int32_t ldy, int32_t epilogue,
+                            void* stream);
 /* sticky error of the kernels (1 = a wait ran out); reading clears it; synchronises */
 hp2d_status hp2d_nn_check(void);
 const char* hp2d_nn_error(void);

@@ -69,3 +69,33 @@ def test_gemm_rejects_bad_shapes():
     C = torch.zeros(128, 32, device="cuda")
     with pytest.raises(HP2DError):
         nn.gemm(A, B, C)   # K not a multiple of 64
+
+
+@pytest.mark.parametrize("B,H,W,C,Co", [(2, 16, 16, 32, 64), (1, 8, 256, 64, 32), (2, 32, 32, 96, 128),
+                                        (1, 64, 64, 128, 256), (4, 32, 32, 256, 256), (1, 16, 128, 32, 2)])
+def test_implicit_conv_matches_im2col_gemm(B, H, W, C, Co):
+    """The implicit-GEMM convolution (4-D TMA boxes shifted per tap, zero fill at the image
+    border) against im2col + the same GEMM: identical up to FP32 summation order."""
+    from hydropol2d_b200 import nn
+    g = torch.Generator().manual_seed(B * 1000 + C + Co)
+    x = torch.randn(B, H, W, C, generator=g).to(torch.bfloat16).cuda()
+    kp = -(-9 * C // 64) * 64
+    w = torch.zeros(Co, kp)
+    w[:, :9 * C] = torch.randn(Co, 9 * C, generator=g) * 0.1
+    w16 = w.to(torch.bfloat16).cuda()
+    bias = torch.randn(Co, generator=g).cuda()
+    P = B * H * W
+    y_imp = torch.empty(P, Co, device="cuda")
+    y_ref = torch.empty(P, Co, device="cuda")
+    assert nn.conv_ok(x.shape)
+    nn.conv3x3(x, w16, Co, y_imp, "f32_bias", bias=bias)
+    nn.gemm(nn.im2col3x3(x, kp), w16, y_ref, "f32_bias", bias=bias)
+    nn.check()
+    d = (y_imp - y_ref).abs().max().item()
+    scale = y_ref.abs().max().item()
+    assert d <= 1e-5 * scale + 1e-6, (d, scale)
+    yb = torch.empty(P, Co, dtype=torch.bfloat16, device="cuda")
+    nn.conv3x3(x, w16, Co, yb, "bf16_bias_relu", bias=bias)
+    nn.check()
+    ref = y_ref.clamp_min(0)
+    assert bool(((yb.float() - ref).abs() <= ref.abs() * 2 ** -8 + 1e-5).all())
