@@ -36,7 +36,7 @@ NATIVE = {
 # every symbol include/hp2d.h declares
 EXPORTS = [
     "hp2d_create", "hp2d_destroy", "hp2d_last_error", "hp2d_create_error",
-    "hp2d_upload_static", "hp2d_set_soil", "hp2d_set_state", "hp2d_set_clock",
+    "hp2d_upload_static", "hp2d_set_soil", "hp2d_set_soil_vg", "hp2d_set_state", "hp2d_set_clock",
     "hp2d_set_rain_uniform", "hp2d_set_rain_maps", "hp2d_hydrology_step", "hp2d_li_step",
     "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed",
     "hp2d_set_tuning", "hp2d_run",
@@ -127,6 +127,8 @@ def lib() -> C.CDLL:
         "hp2d_create_error": ([], C.c_char_p),
         "hp2d_upload_static": ([vp, dp, dp, i32p, i32p, C.c_int32, dp], C.c_int),
         "hp2d_set_soil": ([vp, P(C.c_uint8), C.c_int32, dp, dp, dp, dp, dp, dp, dp], C.c_int),
+        "hp2d_set_soil_vg": ([vp, P(C.c_uint8), C.c_int32, dp, dp, dp, dp, dp, dp, dp, C.c_double, C.c_double,
+                              C.c_double, C.c_double], C.c_int),
         "hp2d_set_state": ([vp, dp, dp, dp], C.c_int),
         "hp2d_set_clock": ([vp, C.c_double, C.c_double, C.c_int64], C.c_int),
         "hp2d_set_rain_uniform": ([vp, C.c_int32, dp, dp], C.c_int),

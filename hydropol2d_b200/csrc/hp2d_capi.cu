@@ -142,6 +142,12 @@ template <typename R> struct Impl : Base {
     std::vector<uint32_t> host_meta;
     std::vector<uint8_t> host_soil;
     std::vector<R> host_tr;
+    // van Genuchten infiltration: classes, globals, water-table depth per cell, DEM copy
+    Dev<SoilClassVG<R>> classes_vg;
+    int n_classes_vg = 0;
+    VGGlobals<R> vgg{};
+    std::vector<R> host_zwt;
+    std::vector<double> host_z;
     bool static_ready = false, dirty = true;
     double last_dt_s = 0;
     int rows_per_warp = 64;
@@ -210,7 +216,22 @@ template <typename R> struct Impl : Base {
         size_t b = (count + kThreads - 1) / kThreads;
         return int(std::max<size_t>(1, std::min<size_t>(b, 148 * 32)));
     }
-    bool ga() const { return ctx->p.flag_infiltration == 1 && n_classes > 0; }
+    // infiltration model in use: 0 none, 1 Green-Ampt, 2 van Genuchten
+    int inf_mode() const {
+        if (ctx->p.flag_infiltration == 1 && n_classes > 0) return 1;
+        if (ctx->p.flag_infiltration == 2 && n_classes_vg > 0) return 2;
+        return 0;
+    }
+    bool ga() const { return inf_mode() != 0; }
+    bool soil_missing() const {
+        return (ctx->p.flag_infiltration == 1 && n_classes == 0) || (ctx->p.flag_infiltration == 2 && n_classes_vg == 0);
+    }
+    // initial second component of a soil record: recovery timer (Green-Ampt) or water-table depth
+    R soil_y(size_t k) const {
+        if (host_soil.empty() || host_soil[k] == 255) return R(0);
+        return inf_mode() == 2 ? host_zwt[k] : host_tr[host_soil[k]];
+    }
+
 
     void write_meta() {
         Dev<uint32_t> m;
@@ -223,6 +244,7 @@ template <typename R> struct Impl : Base {
 
     hp2d_status upload_static(const double* z, const double* rough, const int32_t* rows, const int32_t* cols,
                               int32_t nout, const double* slopes) {
+        host_z.assign(z, z + n);
         const double edge = std::numeric_limits<double>::infinity();   // closed domain-edge face
         std::vector<std::pair<int32_t, R>> outs;
         for (int o = 0; o < nout; ++o) {
@@ -312,7 +334,62 @@ template <typename R> struct Impl : Base {
         std::vector<V2> g(n);
         if (gs2[0].p) g = fetch(gs2[hs.cur].p, n);
         else for (size_t k = 0; k < n; ++k) g[k] = V2{R(0), R(0)};
-        for (size_t k = 0; k < n; ++k) g[k].y = cls[k] != 255 ? host_tr[cls[k]] : R(0);
+        for (size_t k = 0; k < n; ++k) g[k].y = soil_y(k);
+        for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
+        upload(gs2[hs.cur].p, g);
+        invalidate_graph();
+        dirty = true;
+        return HP2D_OK;
+    }
+
+    hp2d_status set_soil_vg(const uint8_t* cls, int32_t ncls, const double* theta_r, const double* theta_s,
+                            const double* n_vg, const double* alpha, const double* ksat, const double* soil_depth,
+                            const double* gw_head, double l_vg, double ltop, double dh_max, double wk) {
+        if (!static_ready) { ctx->err = "hp2d_upload_static first (the water-table depth needs the DEM)"; return HP2D_NOT_READY; }
+        if (ncls <= 0 || ncls > 255) { ctx->err = "n_classes must be in 1..255"; return HP2D_INVALID_ARG; }
+        for (size_t k = 0; k < n; ++k)
+            if (cls[k] != 255 && cls[k] >= ncls) { ctx->err = "soil class index out of range"; return HP2D_INVALID_ARG; }
+        std::vector<SoilClassVG<R>> t(ncls);
+        for (int c = 0; c < ncls; ++c) {
+            if (!(n_vg[c] > 1.0) || !(alpha[c] > 0.0) || !(theta_s[c] >= theta_r[c])) {
+                ctx->err = "van Genuchten classes need n > 1, alpha > 0 and theta_sat >= theta_r";
+                return HP2D_INVALID_ARG;
+            }
+            const double m = 1.0 - 1.0 / n_vg[c];
+            t[c].ks = R(ksat[c] / 1000.0 / 3600.0);
+            t[c].theta_r = R(theta_r[c]);
+            t[c].theta_s = R(theta_s[c]);
+            t[c].alpha = R(alpha[c]);
+            t[c].inv_n = R(1.0 / n_vg[c]);
+            t[c].m = R(m);
+            t[c].inv_m = R(1.0 / m);
+            t[c].pad = R(0);
+        }
+        classes_vg.alloc(ncls);
+        upload(classes_vg.p, t);
+        n_classes_vg = ncls;
+        vgg.ell = R(l_vg);
+        vgg.ltop = R(std::max(ltop, 1e-6));                    // Infiltration_Module.m:232
+        vgg.dh_max = R(dh_max);
+        vgg.wk = R(std::min(std::max(wk, 0.0), 1.0));          // :321
+        // water-table depth (Infiltration_Module.m:192-199): GW_Depth = h_t - (z - Soil_Depth),
+        // zwt = max(Soil_Depth - GW_Depth, 0); no head given = water table at the soil bottom
+        host_zwt.assign(n, R(0));
+        for (size_t k = 0; k < n; ++k) {
+            const double sd = soil_depth[k];
+            const double ht = gw_head ? gw_head[k] : host_z[k] - sd;
+            const double gwd = ht - (host_z[k] - sd);
+            host_zwt[k] = R(std::max(sd - gwd, 0.0));
+        }
+        host_soil.assign(cls, cls + n);
+        for (size_t k = 0; k < n; ++k) host_meta[k] = (host_meta[k] & ~255u) | cls[k];
+        write_meta();
+        soil.alloc(n);
+        upload(soil.p, host_soil);
+        std::vector<V2> g(n);
+        if (gs2[0].p) g = fetch(gs2[hs.cur].p, n);
+        else for (size_t k = 0; k < n; ++k) g[k] = V2{R(0), R(0)};
+        for (size_t k = 0; k < n; ++k) g[k].y = soil_y(k);
         for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
         upload(gs2[hs.cur].p, g);
         invalidate_graph();
@@ -338,7 +415,7 @@ template <typename R> struct Impl : Base {
             if (!Imm) old = fetch(gs2[hs.cur].p, n);
             for (size_t k = 0; k < n; ++k) {
                 g[k].x = Imm ? R(Imm[k] / 1000.0) : old[k].x;
-                g[k].y = (!host_soil.empty() && host_soil[k] != 255) ? host_tr[host_soil[k]] : R(0);
+                g[k].y = soil_y(k);
             }
             upload(gs2[hs.cur].p, g);
         }
@@ -427,7 +504,7 @@ template <typename R> struct Impl : Base {
         unpack();
         double dts = time_step * 60.0;
         k_hydro_rain_ga<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), hs.t_min, dts, rain, h.p, I.p, T.p, soil.p,
-                                                               classes.p, ga() ? 1 : 0, sc.p);
+                                                               classes.p, classes_vg.p, vgg, inf_mode(), sc.p);
         HP_CK(cudaGetLastError());
         k_hydro_clamp<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h.p, sc.p);
         HP_CK(cudaGetLastError());
@@ -523,6 +600,8 @@ template <typename R> struct Impl : Base {
         a.st0 = st4[0].p; a.st1 = st4[1].p;
         a.gs0 = gs2[0].p; a.gs1 = gs2[1].p;
         a.classes = classes.p;
+        a.classes_vg = classes_vg.p;
+        a.vg = vgg;
         a.outlet_cells = outlet_cells.p; a.outlet_coef = outlet_coef.p; a.n_outlets = n_out;
         a.hf3 = hf3.p; a.qo = qo.p;
         a.arrival = arrival.p;
@@ -534,12 +613,18 @@ template <typename R> struct Impl : Base {
     void launch_fused(const FusedArgs<R>& a) {
         const size_t sm = fused_smem_bytes<R>(kThreads);
         const bool map = rain.n_maps > 0;
-        if (a.ga) {
-            if (map) k_fused_step<R, kThreads, true, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
-            else k_fused_step<R, kThreads, true, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
-        } else {
-            if (map) k_fused_step<R, kThreads, false, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
-            else k_fused_step<R, kThreads, false, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+        switch (inf_mode()) {
+            case 1:
+                if (map) k_fused_step<R, kThreads, 1, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                else k_fused_step<R, kThreads, 1, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                break;
+            case 2:
+                if (map) k_fused_step<R, kThreads, 2, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                else k_fused_step<R, kThreads, 2, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                break;
+            default:
+                if (map) k_fused_step<R, kThreads, 0, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                else k_fused_step<R, kThreads, 0, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
         }
     }
 
@@ -568,7 +653,7 @@ template <typename R> struct Impl : Base {
 
     hp2d_status fused_steps(int32_t nsteps, cudaEvent_t after = nullptr) {
         if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
-        if (ctx->p.flag_infiltration == 1 && n_classes == 0) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil"; return HP2D_NOT_READY; }
+        if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
         prologue();
         FusedArgs<R> a = fused_args();
         int remaining = nsteps;
@@ -657,7 +742,7 @@ template <typename R> struct Impl : Base {
     // state, undoes them, and keeps the fastest shape.  Results never depend on the shape.
     hp2d_status autotune(int32_t trial, int32_t* chosen) {
         if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
-        if (ctx->p.flag_infiltration == 1 && n_classes == 0) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil"; return HP2D_NOT_READY; }
+        if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
         prologue();
         Snapshot snap;
         take(snap);
@@ -888,23 +973,25 @@ struct hp2d_ensemble {
         graph = nullptr;
     }
 
-    template <bool GA, bool MAP> void launch_t(int nm) {
+    template <int INF, bool MAP> void launch_t(int nm) {
         const size_t smem = fused_smem_bytes<float>(kThreads);
         if (grid == 0) {
             int per_sm = 0, sms = 0;
-            HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<float, kThreads, GA, MAP>,
+            HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<float, kThreads, INF, MAP>,
                                                                 kThreads, smem));
             HP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
             grid = std::max(1, per_sm) * sms;
         }
         k_ens_plan<float><<<1, 1024, 0, stream>>>(args.p, nm, prefix.p, queue.p);
-        k_ens_step<float, kThreads, GA, MAP><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p, queue.p);
+        k_ens_step<float, kThreads, INF, MAP><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p, queue.p);
     }
     void launch(int nm) {
-        if (ga) {
-            if (map) launch_t<true, true>(nm); else launch_t<true, false>(nm);
+        if (ga == 1) {
+            if (map) launch_t<1, true>(nm); else launch_t<1, false>(nm);
+        } else if (ga == 2) {
+            if (map) launch_t<2, true>(nm); else launch_t<2, false>(nm);
         } else {
-            if (map) launch_t<false, true>(nm); else launch_t<false, false>(nm);
+            if (map) launch_t<0, true>(nm); else launch_t<0, false>(nm);
         }
     }
 
@@ -916,14 +1003,14 @@ struct hp2d_ensemble {
         for (int m = 0; m < nm; ++m) {
             Impl<float>& im = impl(m);
             if (!im.static_ready) { err = "member " + std::to_string(m) + ": hp2d_upload_static not called"; return HP2D_NOT_READY; }
-            if (members[m]->p.flag_infiltration == 1 && im.n_classes == 0) {
-                err = "member " + std::to_string(m) + ": flag_infiltration=1 needs hp2d_set_soil";
+            if (im.soil_missing()) {
+                err = "member " + std::to_string(m) + ": its infiltration model needs its soil tables";
                 return HP2D_NOT_READY;
             }
-            const int mga = im.ga() ? 1 : 0, mmap = im.rain.n_maps > 0 ? 1 : 0;
+            const int mga = im.inf_mode(), mmap = im.rain.n_maps > 0 ? 1 : 0;
             if (m == 0) { ga = mga; map = mmap; }
             if (mga != ga || mmap != map) {
-                err = "members must agree on Green-Ampt infiltration and on the kind of rain forcing";
+                err = "members must agree on the infiltration model and on the kind of rain forcing";
                 return HP2D_INVALID_ARG;
             }
             HP_CK(cudaSetDevice(device));
@@ -1080,7 +1167,7 @@ hp2d_status hp2d_create(const hp2d_grid* grid, const hp2d_params* params, int32_
     if (p.flag_D8 != 0) { g_create_error = "flag_D8=1 is not supported"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_reservoir != 0) { g_create_error = "flag_reservoir=1 is not supported"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_numerical_scheme != 1) { g_create_error = "only flag_numerical_scheme=1 (Bates) is supported"; return HP2D_UNSUPPORTED_FLAG; }
-    if (p.flag_infiltration != 0 && p.flag_infiltration != 1) { g_create_error = "flag_infiltration must be 0 or 1"; return HP2D_UNSUPPORTED_FLAG; }
+    if (p.flag_infiltration < 0 || p.flag_infiltration > 2) { g_create_error = "flag_infiltration must be 0, 1 (Green-Ampt) or 2 (van Genuchten)"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_critical != 0 && p.flag_critical != 1) { g_create_error = "flag_critical must be 0 or 1"; return HP2D_INVALID_ARG; }
     if (p.outlet_type != 1 && p.outlet_type != 2) { g_create_error = "outlet_type must be 1 or 2"; return HP2D_INVALID_ARG; }
     if (!(p.min_time_step > 0) || !(p.max_time_step >= p.min_time_step) || !(p.time_step_increments > 0) ||
@@ -1142,6 +1229,17 @@ hp2d_status hp2d_set_soil(hp2d_ctx* ctx, const uint8_t* soil_class, int32_t n_cl
     if (!soil_class || !ksat || !psi || !dtheta || !Lu || !k_out || !Tr || !min_soil_moisture) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) {
         return m.set_soil(soil_class, n_classes, ksat, psi, dtheta, Lu, k_out, Tr, min_soil_moisture);
+    });
+}
+
+hp2d_status hp2d_set_soil_vg(hp2d_ctx* ctx, const uint8_t* soil_class, int32_t n_classes, const double* theta_r,
+                             const double* theta_sat, const double* n_vg, const double* alpha_vg, const double* ksat,
+                             const double* soil_depth, const double* gw_head, double l_vg, double Ltop, double dh_max,
+                             double ksurf_weight) {
+    if (!soil_class || !theta_r || !theta_sat || !n_vg || !alpha_vg || !ksat || !soil_depth) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) {
+        return m.set_soil_vg(soil_class, n_classes, theta_r, theta_sat, n_vg, alpha_vg, ksat, soil_depth, gw_head, l_vg,
+                             Ltop, dh_max, ksurf_weight);
     });
 }
 

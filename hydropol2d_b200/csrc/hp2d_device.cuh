@@ -320,6 +320,69 @@ __device__ __forceinline__ R green_ampt(R& hh, R& Ic, R& Tc, const SoilClass<R>&
     return fd;
 }
 
+// ---------------- van Genuchten-Mualem Darcy closure (one cell) ------------------------
+// The single-layer branch of the current Infiltration_Module.m (:143-473), in SI units:
+// h [m] after rain, I = soil storage I_t [m], zwt = depth to the water table [m]
+// (:192-199, from the soil depth, groundwater head and elevation; static here).  Returns
+// the infiltrated depth [m]; updates h and I.  Powers with non-integer exponents use the
+// CUDA math library (not reproduced bit for bit by the CPU restatement).
+template <typename R> struct SoilClassVG {
+    R ks;         // saturated conductivity [m/s]
+    R theta_r, theta_s, alpha;   // residual / saturated water content [-], alpha [1/m]
+    R inv_n, m, inv_m, pad;      // 1/n, m = 1 - 1/n, 1/m
+};
+template <typename R> struct VGGlobals {
+    R ell, ltop, dh_max, wk;     // Mualem l, Ltop [m] (>= 1e-6), dh_max [m], Ksurf_weight in [0, 1]
+};
+__device__ __forceinline__ float rpow(float a, float b) { return powf(a, b); }
+__device__ __forceinline__ double rpow(double a, double b) { return pow(a, b); }
+
+template <typename R>
+__device__ __forceinline__ R vg_infiltration(R& hh, R& Ic, R zwt, const SoilClassVG<R>& s, const VGGlobals<R>& g,
+                                             const StepConsts<R>& K) {
+    const R ia = hh * K.inv_dt;                              // supply rate (:179) [m/s]
+    const R h0 = fmax(hh, R(0));                             // ponding head (:182)
+    const R dth = s.theta_s - s.theta_r;
+    const R uzmax = zwt * dth;                               // :205-206
+    const R S = fmax(Ic, R(0));                              // :209
+    const R srem = fmax(uzmax - S, R(0));                    // :214
+    const bool no_uz = !(zwt > R(0)) || !(uzmax > R(0));    // :217
+    const R zs = fmax(zwt, R(1e-6));
+    R tb = s.theta_r + S / zs;                               // :262-265
+    tb = fmin(fmax(tb, s.theta_r), s.theta_s);
+    const R dsafe = fmax(dth, R(1e-12));
+    R seb = fmin(fmax((tb - s.theta_r) / dsafe, R(1e-6)), R(1));
+    R hb = -(R(1) / s.alpha) * rpow(rpow(seb, -s.inv_m) - R(1), s.inv_n);   // :272-276
+    if (seb >= R(0.999999)) hb = R(0);
+    const R w_avail = h0;                                    // :281
+    const R w_def = g.ltop * fmax(s.theta_s - tb, R(0));     // :292 (Lmix = Ltop)
+    R w_wet = fmin(w_avail, srem);
+    w_wet = fmax(fmin(w_wet, w_def), R(0));
+    R tt = tb + w_wet / g.ltop;                              // :300-302
+    tt = fmin(fmax(tt, s.theta_r), s.theta_s);
+    const R set = fmin(fmax((tt - s.theta_r) / dsafe, R(1e-6)), R(1));
+    R term = R(1) - rpow(set, s.inv_m);                      // :307-309
+    term = fmin(fmax(term, R(0)), R(1));
+    const R om = R(1) - rpow(term, s.m);
+    R kr = rpow(set, g.ell) * (om * om);
+    kr = fmin(fmax(kr, R(0)), R(1));
+    const R ktop = s.ks * kr;
+    R ksoil = ktop;                                          // :326-333
+    if (ia > R(0) || h0 > R(0)) ksoil = g.wk * s.ks + (R(1) - g.wk) * ktop;
+    ksoil = fmin(fmax(ksoil, R(0)), s.ks);
+    const R dh = fmin(fmax(h0 - hb, R(0)), g.dh_max);        // :336-338
+    const R cap = ksoil * (dh / g.ltop + R(1));              // :340-342
+    const R flim = srem * K.inv_dt;                          // :345
+    R f = fmin(fmin(ia, cap), flim);                         // :347-352
+    if (no_uz || isnan(f)) f = R(0);
+    f = fmax(f, R(0));
+    const R fd = f * K.dt;                                   // :356-365
+    Ic = fmax(fmin(Ic + fd, uzmax), R(0));
+    hh = hh - fd;                                            // :371-372
+    if (hh < R(0)) hh = R(0);
+    return fd;
+}
+
 // ---------------- one face of the local-inertial momentum update ----------------------
 // x face: (ha, hb) = (left, right) cells, dz = z_right - z_left.
 // y face: (ha, hb) = (upper, lower) cells (row i-1, row i), dz = z_upper - z_lower.

@@ -57,13 +57,15 @@ template <typename R> struct FusedArgs {
     double tol_mm, thr_mm;
     double t_end;                // routing_time + min_time_step/60 [min]
     double min_dt, max_dt, inc, tsc, alfa_min, alfa_max;
-    int flag_timestep, adaptive, flag_critical, outlet_type, ga;
+    int flag_timestep, adaptive, flag_critical, outlet_type, ga;   // ga: infiltration on (either model)
     unsigned int n_ctas;
     R stag_s2;
     const V4* stat;
     V4* st0; V4* st1;            // state records, double buffer
     V2* gs0; V2* gs1;            // soil records, double buffer
-    const SoilClass<R>* classes;
+    const SoilClass<R>* classes;       // Green-Ampt classes
+    const SoilClassVG<R>* classes_vg;  // van Genuchten classes
+    VGGlobals<R> vg;
     const int32_t* outlet_cells; const R* outlet_coef; int n_outlets;
     R* hf3; R* qo;
     R* arrival;
@@ -124,8 +126,9 @@ template <> struct FusedOcc<double> { static constexpr int minb = 3; };
 // pulled from a queue.  Every thread of the CTA calls it; it may return early for all of
 // them together.  Returns false when a row copy timed out (the CTA must stop using its
 // shared-memory ring).
-// GA: Green-Ampt infiltration on; MAP: rain from coarse maps (else a uniform rate)
-template <typename R, int NT, bool GA, bool MAP>
+// INF: infiltration model (0 none, 1 Green-Ampt, 2 van Genuchten); MAP: rain from coarse
+// maps (else a uniform rate)
+template <typename R, int NT, int INF, bool MAP>
 __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned blk) {
     using V4 = typename Vec<R>::V4;
     using V2 = typename Vec<R>::V2;
@@ -241,7 +244,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         }
         const V2 zero2 = {R(0), R(0)};
         V2 nG = zero2;
-        if (GA && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
+        if (INF && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
 #pragma unroll kRowUnroll
         for (int k = 0; k <= last_k; ++k) {
             const int r = r0 - 2 + k;
@@ -262,7 +265,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 issue(k + kStages);
             }
             const V2 Gs = nG;
-            if (GA && col_ok && r + 1 >= 0 && r + 1 < ny) nG = gin[size_t(r + 1) * nx + j];
+            if (INF && col_ok && r + 1 >= 0 && r + 1 < ny) nG = gin[size_t(r + 1) * nx + j];
             const bool ok = col_ok && r >= 0 && r < ny;
             const size_t c = size_t(r) * nx + j;
             const unsigned meta = meta_bits(S.w);
@@ -276,12 +279,14 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 const bool own = own_lane && r >= r0 && r < r_end;
                 // uniform rain volume comes from the count of finite cells at the end
                 if (MAP && map && own && isfinite(hh)) rain_acc_r += rr;
-                if (GA) {
+                if (INF) {
                     const unsigned s = meta & 255u;
                     V2 go = Gs;
                     if (s != 255u) {
                         R Ic = Gs.x, Tc = Gs.y;
-                        const R fd = green_ampt(hh, Ic, Tc, a.classes[s], K);
+                        // Green-Ampt: {I, recovery timer}; van Genuchten: {I, water-table depth}
+                        const R fd = INF == 1 ? green_ampt(hh, Ic, Tc, a.classes[s], K)
+                                              : vg_infiltration(hh, Ic, Tc, a.classes_vg[s], a.vg, K);
                         go.x = Ic;
                         go.y = Tc;
                         if (own && isfinite(fd)) inf_acc_r += fd;
@@ -505,9 +510,9 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     return cta_ok;
 }
 
-template <typename R, int NT, bool GA, bool MAP>
+template <typename R, int NT, int INF, bool MAP>
 __global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const FusedArgs<R> a) {
-    fused_item<R, NT, GA, MAP>(a, blockIdx.x);
+    fused_item<R, NT, INF, MAP>(a, blockIdx.x);
 }
 
 // ---- batched ensemble ----------------------------------------------------------------
@@ -566,7 +571,7 @@ __global__ void k_ens_plan(const FusedArgs<R>* __restrict__ members, int n_membe
     }
 }
 
-template <typename R, int NT, bool GA, bool MAP>
+template <typename R, int NT, int INF, bool MAP>
 __global__ void __launch_bounds__(NT, FusedOcc<R>::minb)
 k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsigned* __restrict__ prefix,
            EnsQueue* q) {
@@ -600,7 +605,7 @@ k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsign
             for (int w = tid; w < int(sizeof(FusedArgs<R>) / 4); w += NT) dst[w] = src[w];
         }
         __syncthreads();
-        if (!fused_item<R, NT, GA, MAP>(s_a, s_local)) return;   // ring unusable after a timeout
+        if (!fused_item<R, NT, INF, MAP>(s_a, s_local)) return;   // ring unusable after a timeout
     }
 }
 

@@ -18,7 +18,8 @@ template <typename R> struct GridView {
 // rain + Green-Ampt (Hydrological_Model.m:14-42); records whether any depth < -1e-8 mm
 template <typename R>
 __global__ void k_hydro_rain_ga(GridView<R> g, double t_min, double dt_s, RainDesc rain, R* h, R* I, R* T,
-                                const uint8_t* soil, const SoilClass<R>* classes, int ga, StepScalars* sc) {
+                                const uint8_t* soil, const SoilClass<R>* classes, const SoilClassVG<R>* classes_vg,
+                                VGGlobals<R> vg, int inf, StepScalars* sc) {
     StepConsts<R> K;
     K.make(dt_s, g.res, g.tol_mm, g.thr_mm);
     const int m = rain.n_maps ? map_index(rain, t_min) : -1;
@@ -33,9 +34,10 @@ __global__ void k_hydro_rain_ga(GridView<R> g, double t_min, double dt_s, RainDe
         const R r = rate * K.rain_scale;
         R hh = h[c] + r;
         if (isfinite(hh)) racc += double(r);
-        if (ga && soil[c] != 255) {
-            R Ic = I[c], Tc = T[c];
-            const R fd = green_ampt(hh, Ic, Tc, classes[soil[c]], K);
+        if (inf && soil[c] != 255) {
+            R Ic = I[c], Tc = T[c];   // T: recovery timer (Green-Ampt) or water-table depth (van Genuchten)
+            const R fd = inf == 1 ? green_ampt(hh, Ic, Tc, classes[soil[c]], K)
+                                  : vg_infiltration(hh, Ic, Tc, classes_vg[soil[c]], vg, K);
             I[c] = Ic;
             T[c] = Tc;
             if (isfinite(fd)) iacc += double(fd);

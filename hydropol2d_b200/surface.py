@@ -87,6 +87,22 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_soil(self._h, cls.ctypes.data_as(C.POINTER(C.c_uint8)), ncls,
                                           *[_dp(t) for t in tabs]))
 
+    def set_soil_vg(self, soil_class, theta_r, theta_sat, n_vg, alpha_vg, ksat, soil_depth, gw_head=None,
+                    l_vg=0.5, Ltop=0.05, dh_max=1.0, Ksurf_weight=0.5):
+        """van Genuchten-Mualem soil (flag_infiltration=2): per-class tables, per-cell soil
+        depth [m] and groundwater head [m] (None: water table at the soil bottom)."""
+        shp = (self.ny, self.nx)
+        cls = np.ascontiguousarray(soil_class, dtype=np.uint8).reshape(shp)
+        tabs = [_f64(v).ravel() for v in (theta_r, theta_sat, n_vg, alpha_vg, ksat)]
+        ncls = tabs[0].size
+        if any(t.size != ncls for t in tabs):
+            raise ValueError("soil tables must have one entry per class")
+        sd = _f64(soil_depth, shp)
+        gw = None if gw_head is None else _f64(gw_head, shp)
+        self._check(self._L.hp2d_set_soil_vg(self._h, cls.ctypes.data_as(C.POINTER(C.c_uint8)), ncls,
+                                             *[_dp(t) for t in tabs], _dp(sd), None if gw is None else _dp(gw),
+                                             float(l_vg), float(Ltop), float(dh_max), float(Ksurf_weight)))
+
     def set_state(self, d, outflow=None, soil_storage=None):
         shp = (self.ny, self.nx)
         d = _f64(d, shp)

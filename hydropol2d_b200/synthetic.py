@@ -239,3 +239,20 @@ def ensemble_member(i: int, seed: int = 2024, lo: int = 256, hi: int = 1024, bre
     return Case(f"member{i}_breach_{ny}x{nx}", z, np.full((ny, nx), 0.035 * nfac), dx, rows, cols,
                 params, d0, rain_uniform=(np.array([0.0]), np.array([0.0])),
                 meta=dict(kind="breach", breach_factor=f, n_factor=nfac, x_dam=x_dam))
+
+
+# van Genuchten parameters of three textures (Carsel & Parrish, 1988, Water Resour. Res. 24):
+# sand, loam, clay; alpha [1/m], ksat [mm/h]
+VG_TEXTURES = dict(theta_r=[0.045, 0.078, 0.068], theta_sat=[0.43, 0.43, 0.38], n_vg=[2.68, 1.56, 1.09],
+                   alpha_vg=[14.5, 3.6, 0.8], ksat=[297.0, 10.4, 2.0])
+
+
+def vg_soil(ny: int, nx: int, z: np.ndarray, seed: int = 3, soil_depth: float = 1.5, wt_below_m: float = 1.0,
+            impervious_share: float = 0.1) -> dict:
+    """set_soil_vg arguments for a seeded Voronoi texture map: soil 1.5 m deep, water table
+    1 m below the surface (a groundwater head of z - 1 m), 10 % impervious cells."""
+    rng = np.random.default_rng(seed)
+    cls = voronoi_classes(ny, nx, 60, 3, seed)
+    cls = np.where(rng.random((ny, nx)) < impervious_share, 255, cls).astype(np.uint8)
+    return dict(soil_class=cls, **{k: np.asarray(v, dtype=np.float64) for k, v in VG_TEXTURES.items()},
+                soil_depth=np.full((ny, nx), soil_depth), gw_head=np.asarray(z, dtype=np.float64) - wt_below_m)

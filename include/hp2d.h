@@ -63,7 +63,7 @@ typedef struct hp2d_params {
     int32_t flag_subgrid;               /* must be 0 */
     int32_t flag_D8;                    /* must be 0 */
     int32_t flag_reservoir;             /* must be 0 */
-    int32_t flag_infiltration;          /* 0 off, 1 Green-Ampt (hp2d_set_soil) */
+    int32_t flag_infiltration;          /* 0 off, 1 Green-Ampt (hp2d_set_soil), 2 van Genuchten (hp2d_set_soil_vg) */
     int32_t flag_timestep;              /* 1: dt = min(dt_adv, dt_wave); 0: dt_wave */
     int32_t flag_adaptive_timestepping; /* 1: wave celerity only; 0: celerity + speed */
     int32_t outlet_type;                /* 1 normal-depth slope, 2 critical */
@@ -139,6 +139,19 @@ hp2d_status hp2d_set_soil(hp2d_ctx* ctx, const uint8_t* soil_class, int32_t n_cl
                           const double* Lu, const double* k_out, const double* Tr,
                           const double* min_soil_moisture);
 
+/* van Genuchten-Mualem soil (the single-layer branch of the current Infiltration_Module.m,
+ * :143-473; flag_infiltration = 2): class map (255 = no soil) and per-class theta_r,
+ * theta_sat [-], n_vg [-] (> 1), alpha_vg [1/m], ksat [mm/h]; per cell Soil_Depth [m] and
+ * the groundwater head BC_States.h_t [m] (NULL = water table at the soil bottom); the
+ * scalars Soil_Properties.l_vg, Ltop [m], dh_max [m] and Ksurf_weight (reference defaults
+ * 0.5, 0.05, 1.0, 0.5).  Call after hp2d_upload_static (the water-table depth uses the DEM).
+ * Soil storage I_t [mm] comes with hp2d_set_state. */
+hp2d_status hp2d_set_soil_vg(hp2d_ctx* ctx, const uint8_t* soil_class, int32_t n_classes,
+                             const double* theta_r, const double* theta_sat, const double* n_vg,
+                             const double* alpha_vg, const double* ksat, const double* soil_depth,
+                             const double* gw_head, double l_vg, double Ltop, double dh_max,
+                             double ksurf_weight);
+
 /* State: depths.d_t [mm]; outflow_bates pages 1-2 [mm/h] (two ny*nx blocks, right then
  * up; NULL = zeros); Soil_Properties.I_t [mm] (NULL = keep).  Resets dmax and arrival. */
 hp2d_status hp2d_set_state(hp2d_ctx* ctx, const double* d, const double* outflow,
@@ -157,7 +170,8 @@ hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_
 
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
 /* Hydrological_Model for this path: adds delta_p_agg = rate(t) * time_step/60 mm,
- * runs the Infiltration_Module (Green-Ampt when flag_infiltration=1) and the clamp; the
+ * runs the Infiltration_Module (Green-Ampt when flag_infiltration=1, van Genuchten when 2)
+ * and the clamp; the
  * resident depth becomes d_tot. */
 hp2d_status hp2d_hydrology_step(hp2d_ctx* ctx, double time_step);
 /* Local_Inertial_Model_D4 on the resident d_tot and outflow_prev with time_step [min];

@@ -275,6 +275,105 @@ def green_ampt_infiltration(d_t, I_t, T, time_step, p: GAParams, resolution):
 
 
 # --------------------------------------------------------------------------------------
+# Infiltration_Module.m, van Genuchten-Mualem single-layer branch
+# --------------------------------------------------------------------------------------
+@dataclass
+class VGParams:
+    """Per-cell van Genuchten maps (built from per-class tables) and the module's scalars."""
+    theta_r: np.ndarray
+    theta_sat: np.ndarray
+    n_vg: np.ndarray
+    alpha_vg: np.ndarray      # 1/m
+    ksat: np.ndarray          # mm/h
+    soil_depth: np.ndarray    # m
+    active: np.ndarray        # False = impervious (LULC_Properties.idx_imp): no infiltration
+    l_vg: float = 0.5
+    Ltop: float = 0.05
+    dh_max: float = 1.0
+    Ksurf_weight: float = 0.5
+
+
+def vg_water_table_depth(z, soil_depth, h_t):
+    """Infiltration_Module.m:192-199: saturated thickness and depth to the water table."""
+    GW_Depth = h_t - (z - soil_depth)
+    return np.fmax(soil_depth - GW_Depth, 0)
+
+
+def vg_infiltration(d_t, I_t, time_step, p: VGParams, zwt, resolution):
+    """Infiltration_Module.m:143-473 (flag_infiltration = 1 of the current module, no layered
+    soil, no subgrid): supply :179-182, unsaturated capacity :205-217, bucket head :262-276,
+    top-layer wetting :281-302, Mualem conductivity :307-318, surface interface :321-333,
+    Darcy capacity :336-342, limits :345-352, storage and depth updates :356-372.
+    Depths and storage in mm, time_step in minutes.  Returns (d_t, I_t, f [mm/h])."""
+    dt_h = time_step / 60
+    C_a = resolution * resolution
+    with np.errstate(all="ignore"):
+        eff_depth = d_t
+        i_a = eff_depth / max(dt_h, 1e-12)
+        h0 = np.fmax(eff_depth, 0) / 1000
+        UZ_max_storage = zwt * (p.theta_sat - p.theta_r)
+        S = np.fmax(I_t, 0) / 1000
+        S_rem = np.fmax(UZ_max_storage - S, 0)
+        idx_noUZ = (zwt <= 0) | (UZ_max_storage <= 0)
+        theta_r, theta_s, n, a = p.theta_r, p.theta_sat, p.n_vg, p.alpha_vg
+        Ks = p.ksat / 1000 / 3600
+        m = 1 - 1 / n
+        ell = p.l_vg
+        Ltop = max(p.Ltop, 1e-6)
+        dh_max = p.dh_max
+        Lmix = Ltop
+        zwt_safe = np.fmax(zwt, 1e-6)
+        theta_bucket = theta_r + (S / zwt_safe)
+        theta_bucket = np.fmax(theta_bucket, theta_r)
+        theta_bucket = np.fmin(theta_bucket, theta_s)
+        Se_bucket = (theta_bucket - theta_r) / np.fmax(theta_s - theta_r, 1e-12)
+        Se_bucket = np.fmin(np.fmax(Se_bucket, 1e-6), 1)
+        h_bucket = -(1 / a) * ((Se_bucket ** (-1 / m) - 1) ** (1 / n))
+        h_bucket = np.where(Se_bucket >= 0.999999, 0.0, h_bucket)
+        w_avail = np.fmax(eff_depth, 0) / 1000
+        w_top_deficit = Lmix * np.fmax(theta_s - theta_bucket, 0)
+        w_wet = np.fmin(w_avail, S_rem)
+        w_wet = np.fmin(w_wet, w_top_deficit)
+        w_wet = np.fmax(w_wet, 0)
+        theta_top = theta_bucket + w_wet / Lmix
+        theta_top = np.fmax(theta_top, theta_r)
+        theta_top = np.fmin(theta_top, theta_s)
+        Se_top = (theta_top - theta_r) / np.fmax(theta_s - theta_r, 1e-12)
+        Se_top = np.fmin(np.fmax(Se_top, 1e-6), 1)
+        term_top = 1 - Se_top ** (1 / m)
+        term_top = np.fmin(np.fmax(term_top, 0), 1)
+        Kr_top = Se_top ** ell * (1 - term_top ** m) ** 2
+        Kr_top = np.fmin(np.fmax(Kr_top, 0), 1)
+        Ktop = Ks * Kr_top
+        Ksurf = Ks + np.zeros_like(Ktop)
+        wK = min(max(p.Ksurf_weight, 0), 1)
+        idx_wet_boundary = (i_a > 0) | (h0 > 0)
+        Ksoil = np.where(idx_wet_boundary, wK * Ksurf + (1 - wK) * Ktop, Ktop)
+        Ksoil = np.fmin(np.fmax(Ksoil, 0), Ksurf)
+        dh = h0 - h_bucket
+        dh = np.fmax(dh, 0)
+        dh = np.fmin(dh, dh_max)
+        grad = (dh / Ltop) + 1
+        C = Ksoil * grad
+        C = C * 1000 * 3600
+        f_store_lim = (S_rem * 1000) / max(dt_h, 1e-12)
+        f = np.fmin(i_a, C)
+        f = np.fmin(f, f_store_lim)
+        f = np.where(p.active, f, 0.0)
+        f = np.where(idx_noUZ, 0.0, f)
+        f = np.where(np.isnan(f), 0.0, f)
+        f = np.fmax(f, 0)
+        inf_volume_cell = f * dt_h
+        I_new = I_t + inf_volume_cell
+        I_new = np.fmin(I_new, UZ_max_storage * 1000)
+        I_new = np.fmax(I_new, 0)
+        I_new = np.where(p.active, I_new, I_t)
+        d_new = d_t - inf_volume_cell * (resolution * resolution) / C_a
+        d_new[d_new < 0] = 0
+    return d_new, I_new, f
+
+
+# --------------------------------------------------------------------------------------
 # refreshing_timestep.m (inertial D4 branch)
 # --------------------------------------------------------------------------------------
 @dataclass
