@@ -151,10 +151,15 @@ template <typename R> struct Impl : Base {
     bool static_ready = false, dirty = true;
     double last_dt_s = 0;
     int rows_per_warp = 64;
+    int cells_per_lane = 1;   // fused-step layout: 1 (32-column strips) or 2 (64-column strips)
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
 
     explicit Impl(hp2d_ctx* c) : ctx(c) {
+        if (sizeof(R) == 4) {   // measured defaults for FP32 (hp2d_autotune refines them per grid)
+            cells_per_lane = 2;
+            rows_per_warp = 32;
+        }
         ny = c->g.ny;
         nx = c->g.nx;
         n = size_t(ny) * nx;
@@ -581,7 +586,8 @@ template <typename R> struct Impl : Base {
     }
 
     // ---------------- fused path ----------------
-    FusedArgs<R> fused_args() {
+    FusedArgs<R> fused_args(int cpl = 0) {
+        if (cpl <= 0) cpl = cells_per_lane;
         FusedArgs<R> a{};
         const hp2d_params& p = ctx->p;
         a.ny = ny; a.nx = nx; a.res = res;
@@ -591,7 +597,8 @@ template <typename R> struct Impl : Base {
         a.tsc = p.time_step_change; a.alfa_min = p.alfa_min; a.alfa_max = p.alfa_max;
         a.flag_timestep = p.flag_timestep; a.adaptive = p.flag_adaptive_timestepping;
         a.flag_critical = p.flag_critical; a.outlet_type = p.outlet_type; a.ga = ga() ? 1 : 0;
-        a.n_strips = (nx + kStripOut - 1) / kStripOut;
+        const int out_cols = 32 * cpl - 4;   // a strip's output columns (2-column apron each side)
+        a.n_strips = (nx + out_cols - 1) / out_cols;
         a.rows_per_warp = rows_per_warp;
         a.n_warps_total = a.n_strips * ((ny + rows_per_warp - 1) / rows_per_warp);
         a.n_ctas = unsigned((a.n_warps_total + kThreads / 32 - 1) / (kThreads / 32));
@@ -610,22 +617,46 @@ template <typename R> struct Impl : Base {
         return a;
     }
 
-    void launch_fused(const FusedArgs<R>& a) {
-        const size_t sm = fused_smem_bytes<R>(kThreads);
+    // kernels whose ring needs more than the default 48 KB of dynamic shared memory opt in
+    // once per instantiation (before any graph capture: fused_steps and autotune call this)
+    template <int INF, bool MAP, int CPL> static void opt_in_smem() {
+        static bool done[8] = {};
+        const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
+        int dev = 0;
+        HP_CK(cudaGetDevice(&dev));
+        if (sm > 48 * 1024 && dev < 8 && !done[dev]) {
+            HP_CK(cudaFuncSetAttribute(k_fused_step<R, kThreads, INF, MAP, CPL>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+            done[dev] = true;
+        }
+    }
+    template <int CPL> void opt_in_t() {
+        opt_in_smem<0, false, CPL>(); opt_in_smem<0, true, CPL>();
+        opt_in_smem<1, false, CPL>(); opt_in_smem<1, true, CPL>();
+        opt_in_smem<2, false, CPL>(); opt_in_smem<2, true, CPL>();
+    }
+    void opt_in() { opt_in_t<1>(); opt_in_t<2>(); }
+
+    template <int CPL> void launch_fused_t(const FusedArgs<R>& a) {
+        const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
         const bool map = rain.n_maps > 0;
         switch (inf_mode()) {
             case 1:
-                if (map) k_fused_step<R, kThreads, 1, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
-                else k_fused_step<R, kThreads, 1, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                if (map) k_fused_step<R, kThreads, 1, true, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                else k_fused_step<R, kThreads, 1, false, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
                 break;
             case 2:
-                if (map) k_fused_step<R, kThreads, 2, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
-                else k_fused_step<R, kThreads, 2, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                if (map) k_fused_step<R, kThreads, 2, true, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                else k_fused_step<R, kThreads, 2, false, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
                 break;
             default:
-                if (map) k_fused_step<R, kThreads, 0, true><<<a.n_ctas, kThreads, sm, st()>>>(a);
-                else k_fused_step<R, kThreads, 0, false><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                if (map) k_fused_step<R, kThreads, 0, true, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                else k_fused_step<R, kThreads, 0, false, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
         }
+    }
+    void launch_fused(const FusedArgs<R>& a) {
+        if (cells_per_lane == 2) launch_fused_t<2>(a);
+        else launch_fused_t<1>(a);
     }
 
     void invalidate_graph() {
@@ -654,6 +685,7 @@ template <typename R> struct Impl : Base {
     hp2d_status fused_steps(int32_t nsteps, cudaEvent_t after = nullptr) {
         if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
         if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
+        opt_in();
         prologue();
         FusedArgs<R> a = fused_args();
         int remaining = nsteps;
@@ -743,20 +775,23 @@ template <typename R> struct Impl : Base {
     hp2d_status autotune(int32_t trial, int32_t* chosen) {
         if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
         if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
+        opt_in();
         prologue();
         Snapshot snap;
         take(snap);
         const int cands[] = {16, 24, 32, 48, 64, 96, 128};
-        const int keep = rows_per_warp;
-        int best = keep;
+        const int keep = rows_per_warp, keep_cpl = cells_per_lane;
+        int best = keep, best_cpl = keep_cpl;
         float best_ms = std::numeric_limits<float>::infinity();
         bool timed_out = false;
         cudaEvent_t e0, e1;
         HP_CK(cudaEventCreate(&e0));
         HP_CK(cudaEventCreate(&e1));
+        for (int cpl = 1; cpl <= 2; ++cpl)
         for (int c : cands) {
             if (c > std::max(ny, 4) && c != 16) continue;
             rows_per_warp = c;
+            cells_per_lane = cpl;
             const FusedArgs<R> a = fused_args();
             launch_fused(a);   // warm-up
             HP_CK(cudaEventRecord(e0, st()));
@@ -766,7 +801,7 @@ template <typename R> struct Impl : Base {
             HP_CK(cudaEventSynchronize(e1));
             float ms = 0;
             HP_CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best_ms) { best_ms = ms; best = c; }
+            if (ms < best_ms) { best_ms = ms; best = c; best_cpl = cpl; }
             pull_sc();
             timed_out = timed_out || (hs.status & 2u) != 0;
             put_back(snap);
@@ -774,6 +809,7 @@ template <typename R> struct Impl : Base {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         rows_per_warp = best;
+        cells_per_lane = best_cpl;
         invalidate_graph();
         if (timed_out) { ctx->err = "a row copy did not complete within its wait limit"; return HP2D_TIMEOUT; }
         if (chosen) *chosen = best;
@@ -961,10 +997,11 @@ struct hp2d_ensemble {
     Dev<unsigned> prefix;
     Dev<EnsQueue> queue;
     int rows_per_warp = 32;
+    int cells_per_lane = 2;   // layout of the streamed strips (as hp2d_set_layout)
     int ga = -1, map = -1;
-    int grid = 0;
+    int grid_for[3] = {0, 0, 0};
     cudaGraphExec_t graph = nullptr;
-    int graph_members = -1, graph_rpw = -1;
+    int graph_members = -1, graph_rpw = -1, graph_cpl = -1;
 
     Impl<float>& impl(int m) { return *static_cast<Impl<float>*>(members[m]->impl.get()); }
 
@@ -973,26 +1010,31 @@ struct hp2d_ensemble {
         graph = nullptr;
     }
 
-    template <int INF, bool MAP> void launch_t(int nm) {
-        const size_t smem = fused_smem_bytes<float>(kThreads);
+    template <int INF, bool MAP, int CPL> void launch_t(int nm) {
+        const size_t smem = fused_smem_bytes<float, CPL>(kThreads);
+        int& grid = grid_for[CPL];
         if (grid == 0) {
             int per_sm = 0, sms = 0;
-            HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<float, kThreads, INF, MAP>,
+            HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<float, kThreads, INF, MAP, CPL>,
                                                                 kThreads, smem));
             HP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
             grid = std::max(1, per_sm) * sms;
         }
         k_ens_plan<float><<<1, 1024, 0, stream>>>(args.p, nm, prefix.p, queue.p);
-        k_ens_step<float, kThreads, INF, MAP><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p, queue.p);
+        k_ens_step<float, kThreads, INF, MAP, CPL><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p, queue.p);
+    }
+    template <int CPL> void launch_c(int nm) {
+        if (ga == 1) {
+            if (map) launch_t<1, true, CPL>(nm); else launch_t<1, false, CPL>(nm);
+        } else if (ga == 2) {
+            if (map) launch_t<2, true, CPL>(nm); else launch_t<2, false, CPL>(nm);
+        } else {
+            if (map) launch_t<0, true, CPL>(nm); else launch_t<0, false, CPL>(nm);
+        }
     }
     void launch(int nm) {
-        if (ga == 1) {
-            if (map) launch_t<1, true>(nm); else launch_t<1, false>(nm);
-        } else if (ga == 2) {
-            if (map) launch_t<2, true>(nm); else launch_t<2, false>(nm);
-        } else {
-            if (map) launch_t<0, true>(nm); else launch_t<0, false>(nm);
-        }
+        if (cells_per_lane == 2) launch_c<2>(nm);
+        else launch_c<1>(nm);
     }
 
     // members' pending work done, their first-step prologues run, argument table current
@@ -1020,7 +1062,7 @@ struct hp2d_ensemble {
             }
             im.prologue();
             HP_CK(cudaStreamSynchronize(im.st()));
-            host[m] = im.fused_args();
+            host[m] = im.fused_args(cells_per_lane);
         }
         // a captured graph holds these pointers: reallocate (and recapture) only on a size change
         if (args.n != size_t(nm)) {
@@ -1042,7 +1084,7 @@ struct hp2d_ensemble {
         const int nm = int(members.size());
         int remaining = nsteps;
         if (remaining >= kChunk) {
-            if (graph && (graph_members != nm || graph_rpw != rows_per_warp)) drop_graph();
+            if (graph && (graph_members != nm || graph_rpw != rows_per_warp || graph_cpl != cells_per_lane)) drop_graph();
             if (!graph) {
                 cudaGraph_t gr;
                 HP_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -1052,6 +1094,7 @@ struct hp2d_ensemble {
                 HP_CK(cudaGraphDestroy(gr));
                 graph_members = nm;
                 graph_rpw = rows_per_warp;
+                graph_cpl = cells_per_lane;
             }
             while (remaining >= kChunk) {
                 HP_CK(cudaGraphLaunch(graph, stream));
@@ -1099,15 +1142,17 @@ struct hp2d_ensemble {
             snaps.emplace_back(new Impl<float>::Snapshot());
             impl(m).take(*snaps.back());
         }
-        const int keep = rows_per_warp;
-        int best = keep;
+        const int keep = rows_per_warp, keep_cpl = cells_per_lane;
+        int best = keep, best_cpl = keep_cpl;
         float best_ms = std::numeric_limits<float>::infinity();
         cudaEvent_t e0, e1;
         HP_CK(cudaEventCreate(&e0));
         HP_CK(cudaEventCreate(&e1));
         bool stalled = false;
+        for (int cpl = 1; cpl <= 2; ++cpl)
         for (int c : cands) {
             rows_per_warp = c;
+            cells_per_lane = cpl;
             s = prepare();
             if (s != HP2D_OK) break;
             launch(nm);   // warm-up
@@ -1118,7 +1163,7 @@ struct hp2d_ensemble {
             HP_CK(cudaEventSynchronize(e1));
             float ms = 0;
             HP_CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best_ms) { best_ms = ms; best = c; }
+            if (ms < best_ms) { best_ms = ms; best = c; best_cpl = cpl; }
             for (int m = 0; m < nm; ++m) {
                 impl(m).pull_sc();
                 stalled = stalled || (impl(m).hs.status & 2u) != 0;
@@ -1128,6 +1173,7 @@ struct hp2d_ensemble {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         rows_per_warp = best;
+        cells_per_lane = best_cpl;
         drop_graph();
         if (s != HP2D_OK) return s;
         if (stalled) { err = "a row copy did not complete within its wait limit"; return HP2D_TIMEOUT; }
@@ -1295,6 +1341,15 @@ hp2d_status hp2d_fused_steps_timed(hp2d_ctx* ctx, int32_t nsteps, float* elapsed
     return with_impl(ctx, [&](auto& m) { return m.fused_steps_timed(nsteps, elapsed_ms); });
 }
 
+hp2d_status hp2d_set_layout(hp2d_ctx* ctx, int32_t cells_per_lane) {
+    if (cells_per_lane != 1 && cells_per_lane != 2) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) {
+        m.cells_per_lane = cells_per_lane;
+        m.invalidate_graph();
+        return HP2D_OK;
+    });
+}
+
 hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp) {
     if (rows_per_warp < 4) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) {
@@ -1391,6 +1446,15 @@ hp2d_status hp2d_ensemble_set_tuning(hp2d_ensemble* e, int32_t rows_per_warp) {
     if (rows_per_warp < 4) return HP2D_INVALID_ARG;
     return ens_guarded(e, [&]() -> hp2d_status {
         e->rows_per_warp = rows_per_warp;
+        e->drop_graph();
+        return HP2D_OK;
+    });
+}
+
+hp2d_status hp2d_ensemble_set_layout(hp2d_ensemble* e, int32_t cells_per_lane) {
+    if (cells_per_lane != 1 && cells_per_lane != 2) return HP2D_INVALID_ARG;
+    return ens_guarded(e, [&]() -> hp2d_status {
+        e->cells_per_lane = cells_per_lane;
         e->drop_graph();
         return HP2D_OK;
     });

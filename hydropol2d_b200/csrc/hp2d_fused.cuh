@@ -43,9 +43,9 @@ constexpr int kStages = HP2D_STAGES;   // shared-memory ring depth of the row pi
 #endif
 constexpr int kRowUnroll = HP2D_ROW_UNROLL;   // row-loop unroll (register renaming of the window)
 
-// dynamic shared memory of k_fused_step: per warp kStages x 64 records
-template <typename R> constexpr size_t fused_smem_bytes(int nt) {
-    return size_t(nt / 32) * kStages * 64 * sizeof(typename Vec<R>::V4);
+// dynamic shared memory of k_fused_step: per warp kStages x (2 records x 32*CPL cells)
+template <typename R, int CPL = 1> constexpr size_t fused_smem_bytes(int nt) {
+    return size_t(nt / 32) * kStages * 64 * CPL * sizeof(typename Vec<R>::V4);
 }
 
 template <typename R> struct FusedArgs {
@@ -114,12 +114,37 @@ template <typename R> __device__ __forceinline__ R bits_to(unsigned long long b)
 template <> __device__ __forceinline__ float bits_to<float>(unsigned long long b) { return __uint_as_float((unsigned)b); }
 template <> __device__ __forceinline__ double bits_to<double>(unsigned long long b) { return __longlong_as_double((long long)b); }
 
+// Neighbour exchange across a warp's strip of 32*CPL columns (cell h of lane L sits at
+// column 32h + L): value of the cell to the right / to the left.  With two cells per lane
+// one indexed shuffle carries the value across the boundary between the two halves.
+template <typename R, int CPL>
+__device__ __forceinline__ void right_of(const R (&v)[CPL], R (&out)[CPL], int lane) {
+    if (CPL == 1) {
+        out[0] = __shfl_down_sync(0xffffffffu, v[0], 1);
+    } else {
+        out[0] = __shfl_sync(0xffffffffu, lane == 0 ? v[CPL - 1] : v[0], (lane + 1) & 31);
+        out[CPL - 1] = __shfl_down_sync(0xffffffffu, v[CPL - 1], 1);
+    }
+}
+template <typename R, int CPL>
+__device__ __forceinline__ void left_of(const R (&v)[CPL], R (&out)[CPL], int lane) {
+    if (CPL == 1) {
+        out[0] = __shfl_up_sync(0xffffffffu, v[0], 1);
+    } else {
+        out[CPL - 1] = __shfl_sync(0xffffffffu, lane == 31 ? v[0] : v[CPL - 1], (lane + 31) & 31);
+        out[0] = __shfl_up_sync(0xffffffffu, v[0], 1);
+    }
+}
+
 // resident CTAs per SM the register budget is sized for (float: 8 x 128 threads)
 #ifndef HP2D_MINB_F32
 #define HP2D_MINB_F32 8
 #endif
-template <typename R> struct FusedOcc { static constexpr int minb = HP2D_MINB_F32; };
-template <> struct FusedOcc<double> { static constexpr int minb = 3; };
+#ifndef HP2D_MINB_F32_PAIR
+#define HP2D_MINB_F32_PAIR 4
+#endif
+template <typename R, int CPL = 1> struct FusedOcc { static constexpr int minb = CPL == 1 ? HP2D_MINB_F32 : HP2D_MINB_F32_PAIR; };
+template <int CPL> struct FusedOcc<double, CPL> { static constexpr int minb = CPL == 1 ? 3 : 2; };
 
 // One CTA-sized work item of the fused step: warps blk*NT/32 .. of the grid described by
 // `a`.  k_fused_step runs item blockIdx.x of one grid; k_ens_step runs items of many grids
@@ -128,7 +153,7 @@ template <> struct FusedOcc<double> { static constexpr int minb = 3; };
 // shared-memory ring).
 // INF: infiltration model (0 none, 1 Green-Ampt, 2 van Genuchten); MAP: rain from coarse
 // maps (else a uniform rate)
-template <typename R, int NT, int INF, bool MAP>
+template <typename R, int NT, int INF, bool MAP, int CPL = 1>
 __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned blk) {
     using V4 = typename Vec<R>::V4;
     using V2 = typename Vec<R>::V2;
@@ -185,33 +210,43 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     R cmaxv = R(-1);   // largest celerity term of a non-stagnant cell (-1: none yet)
 
     if (wg < a.n_warps_total) {
+        constexpr int SW = 32 * CPL;       // strip width: CPL cells per lane
         const int strip = wg % a.n_strips;
         const int rb = wg / a.n_strips;
-        const int j = strip * kStripOut - 2 + lane;
-        const bool col_ok = j >= 0 && j < nx;
-        const bool own_lane = lane >= 2 && lane < 30 && j < nx;
+        const int j_first = strip * (SW - 4) - 2;   // 2-column apron on each side
+        int j[CPL];
+        bool col_ok[CPL], own_lane[CPL];
+#pragma unroll
+        for (int h = 0; h < CPL; ++h) {
+            j[h] = j_first + 32 * h + lane;
+            col_ok[h] = j[h] >= 0 && j[h] < nx;
+            own_lane[h] = (h > 0 || lane >= 2) && (h < CPL - 1 || lane < 30) && j[h] < nx;
+        }
         const int r0 = rb * a.rows_per_warp;
         const int r_end = min(r0 + a.rows_per_warp, ny);
 
-        // rolling window (suffix = rows back)
-        R hT1 = R(0), hT2 = R(0);
-        R qxu1 = R(0), qyu1 = R(0);
-        R hfx1 = R(0), hfx2 = R(0), hfy1 = R(0), hfy2 = R(0);
-        R sc2 = R(1);
-        R qxl2 = R(0), qyl2 = R(0);
-        R dm1 = R(0), dm2 = R(0);
-        unsigned mt1 = 0u, mt2 = 0u;
+        // rolling window (suffix = rows back), one entry per cell of the lane
+        R hT1[CPL], hT2[CPL], qxu1[CPL], qyu1[CPL], hfx1[CPL], hfx2[CPL], hfy1[CPL], hfy2[CPL];
+        R sc2[CPL], qxl2[CPL], qyl2[CPL], dm1[CPL], dm2[CPL];
+        unsigned mt1[CPL], mt2[CPL];
+#pragma unroll
+        for (int h = 0; h < CPL; ++h) {
+            hT1[h] = hT2[h] = qxu1[h] = qyu1[h] = R(0);
+            hfx1[h] = hfx2[h] = hfy1[h] = hfy2[h] = R(0);
+            sc2[h] = R(1);
+            qxl2[h] = qyl2[h] = dm1[h] = dm2[h] = R(0);
+            mt1[h] = mt2[h] = 0u;
+        }
 
         // TMA pipeline: the warp's two row records (static, state) of rows k+1..k+kStages-1
         // are in flight in a ring of kStages shared-memory stages while row k is
-        // computed.  Lane 0 issues one 1-D bulk copy per record row (the strip's cells
-        // are contiguous), the stage's mbarrier counts the bytes.
-        const int j_first = strip * kStripOut - 2;
+        // computed.  One 1-D bulk copy per record row (the strip's cells are contiguous),
+        // the stage's mbarrier counts the bytes.
         const int seg_j0 = max(j_first, 0);
-        const int seg_n = min(j_first + 32, nx) - seg_j0;
+        const int seg_n = min(j_first + SW, nx) - seg_j0;
         const int seg_off = seg_j0 - j_first;
         const int last_k = (r_end + 1) - (r0 - 2);
-        V4* ring = reinterpret_cast<V4*>(smem_dyn) + size_t(warp) * kStages * 64;
+        V4* ring = reinterpret_cast<V4*>(smem_dyn) + size_t(warp) * kStages * 2 * SW;
         const uint32_t bar0 = smem_addr(&s_bar[warp][0]);
         // lane 0 arms the stage's barrier (arrive + expected bytes) and copies the static
         // row, lane 1 copies the state row; a copy that lands before the arming only makes
@@ -220,14 +255,14 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         const uint32_t ring_base = smem_addr(ring + seg_off);
         const uint32_t bytes = uint32_t(seg_n) * uint32_t(sizeof(V4));
         const V4* src_base = lane == 0 ? stat : sin;
-        const uint32_t dst_half = lane == 0 ? 0u : uint32_t(32 * sizeof(V4));
+        const uint32_t dst_half = lane == 0 ? 0u : uint32_t(SW * sizeof(V4));
         auto issue = [&](int k) {
             const int s = k % kStages;
             const uint32_t bar = bar0 + 8u * s;
             const int rr = r0 - 2 + k;
             if (rr >= 0 && rr < ny && seg_n > 0) {
                 if (lane == 0) mbar_expect_tx(bar, 2u * bytes);
-                bulk_g2s(ring_base + uint32_t(s) * uint32_t(64 * sizeof(V4)) + dst_half,
+                bulk_g2s(ring_base + uint32_t(s) * uint32_t(2 * SW * sizeof(V4)) + dst_half,
                          src_base + (size_t(rr) * nx + seg_j0), bytes, bar);
             } else if (lane == 0) {
                 mbar_arrive(bar);
@@ -242,9 +277,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             fence_proxy_async_smem();   // reads of the ring by an earlier item come first
             for (int k = 0; k < kStages && k <= last_k; ++k) issue(k);
         }
-        const V2 zero2 = {R(0), R(0)};
-        V2 nG = zero2;
-        if (INF && col_ok && r0 - 2 >= 0) nG = gin[size_t(r0 - 2) * nx + j];
+        V2 nG[CPL];
+#pragma unroll
+        for (int h = 0; h < CPL; ++h) {
+            nG[h] = V2{R(0), R(0)};
+            if (INF && col_ok[h] && r0 - 2 >= 0) nG[h] = gin[size_t(r0 - 2) * nx + j[h]];
+        }
 #pragma unroll kRowUnroll
         for (int k = 0; k <= last_k; ++k) {
             const int r = r0 - 2 + k;
@@ -257,127 +295,169 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     mbar_wait_bounded(bar0 + 8u * (kk % kStages), uint32_t((kk / kStages) & 1), 1u << 22);
                 break;
             }
-            const V4 S = ring[s * 64 + lane];
-            const V4 X = ring[s * 64 + 32 + lane];
+            V4 S[CPL], X[CPL];
+#pragma unroll
+            for (int h = 0; h < CPL; ++h) {
+                S[h] = ring[s * 2 * SW + 32 * h + lane];
+                X[h] = ring[s * 2 * SW + SW + 32 * h + lane];
+            }
             __syncwarp();
             if (lane < 2 && k + kStages <= last_k) {
                 fence_proxy_async_smem();
                 issue(k + kStages);
             }
-            const V2 Gs = nG;
-            if (INF && col_ok && r + 1 >= 0 && r + 1 < ny) nG = gin[size_t(r + 1) * nx + j];
-            const bool ok = col_ok && r >= 0 && r < ny;
-            const size_t c = size_t(r) * nx + j;
-            const unsigned meta = meta_bits(S.w);
-            // (A) hydrology of (r, j)
-            R hT0 = R(0);
-            if (ok) {
-                R hh = X.x;
-                const R rate = map ? map_rate<R>(a.rain, map, r, j, ny, nx) : rain_u;
-                const R rr = rate * K.rain_scale;
-                hh = hh + rr;
-                const bool own = own_lane && r >= r0 && r < r_end;
-                // uniform rain volume comes from the count of finite cells at the end
-                if (MAP && map && own && isfinite(hh)) rain_acc_r += rr;
-                if (INF) {
-                    const unsigned s = meta & 255u;
-                    V2 go = Gs;
-                    if (s != 255u) {
-                        R Ic = Gs.x, Tc = Gs.y;
-                        // Green-Ampt: {I, recovery timer}; van Genuchten: {I, water-table depth}
-                        const R fd = INF == 1 ? green_ampt(hh, Ic, Tc, a.classes[s], K)
-                                              : vg_infiltration(hh, Ic, Tc, a.classes_vg[s], a.vg, K);
-                        go.x = Ic;
-                        go.y = Tc;
-                        if (own && isfinite(fd)) inf_acc_r += fd;
+            const bool rok = r >= 0 && r < ny;
+            const bool own_row = r >= r0 && r < r_end;
+            R hT0[CPL];
+            unsigned meta[CPL];
+            bool all_dry = true;
+#pragma unroll
+            for (int h = 0; h < CPL; ++h) {
+                const V2 Gs = nG[h];
+                if (INF && col_ok[h] && r + 1 >= 0 && r + 1 < ny) nG[h] = gin[size_t(r + 1) * nx + j[h]];
+                meta[h] = meta_bits(S[h].w);
+                // (A) hydrology of (r, j)
+                hT0[h] = R(0);
+                if (col_ok[h] && rok) {
+                    const size_t c = size_t(r) * nx + j[h];
+                    R hh = X[h].x;
+                    const R rate = map ? map_rate<R>(a.rain, map, r, j[h], ny, nx) : rain_u;
+                    const R rr = rate * K.rain_scale;
+                    hh = hh + rr;
+                    const bool own = own_lane[h] && own_row;
+                    // uniform rain volume comes from the count of finite cells at the end
+                    if (MAP && map && own && isfinite(hh)) rain_acc_r += rr;
+                    if (INF) {
+                        const unsigned sc = meta[h] & 255u;
+                        V2 go = Gs;
+                        if (sc != 255u) {
+                            R Ic = Gs.x, Tc = Gs.y;
+                            // Green-Ampt: {I, recovery timer}; van Genuchten: {I, water-table depth}
+                            const R fd = INF == 1 ? green_ampt(hh, Ic, Tc, a.classes[sc], K)
+                                                  : vg_infiltration(hh, Ic, Tc, a.classes_vg[sc], a.vg, K);
+                            go.x = Ic;
+                            go.y = Tc;
+                            if (own && isfinite(fd)) inf_acc_r += fd;
+                        }
+                        if (own) gout[c] = go;
                     }
-                    if (own) gout[c] = go;
+                    if (!skip && hh < R(1e-9)) hh = R(0);
+                    if (hh < R(0)) hh = R(0);
+                    hT0[h] = hh;
                 }
-                if (!skip && hh < R(1e-9)) hh = R(0);
-                if (hh < R(0)) hh = R(0);
-                hT0 = hh;
+                all_dry = all_dry && hT0[h] == R(0);
             }
             // rows r-2..r dry across the whole strip: every face flux of row r and r-1 is
             // zero (Hf = 0), the donor scale of row r-1 is one and its limited faces are
             // zero, so (B)-(E) are skipped; the values below are what they would compute
-            dry = (dry << 1) | (__all_sync(FULL, hT0 == R(0)) ? 1u : 0u);
-            R qxu0 = R(0), hfx0 = R(0), qyu0 = R(0), hfy0 = R(0), sc1 = R(1), qxl1 = R(0), qyl1 = R(0);
+            dry = (dry << 1) | (__all_sync(FULL, all_dry) ? 1u : 0u);
+            R qxu0[CPL], hfx0[CPL], qyu0[CPL], hfy0[CPL], sc1[CPL], qxl1[CPL], qyl1[CPL];
+#pragma unroll
+            for (int h = 0; h < CPL; ++h) {
+                qxu0[h] = hfx0[h] = qyu0[h] = hfy0[h] = qxl1[h] = qyl1[h] = R(0);
+                sc1[h] = R(1);
+            }
             if ((dry & 7u) != 7u) {
                 // (B) x face (r, j) between (r, j) and (r, j+1)
-                const R hR = __shfl_down_sync(FULL, hT0, 1);
-                if (ok) face_flux<R, true>(hT0, hR, S.x, X.y, S.z, K, a.flag_critical, hfx0, qxu0);
+                R hR[CPL];
+                right_of<R, CPL>(hT0, hR, lane);
+#pragma unroll
+                for (int h = 0; h < CPL; ++h)
+                    if (col_ok[h] && rok) face_flux<R, true>(hT0[h], hR[h], S[h].x, X[h].y, S[h].z, K, a.flag_critical, hfx0[h], qxu0[h]);
                 // (C) y face (r, j) between (r-1, j) and (r, j)
-                if (ok && r >= r0 - 1)
-                    face_flux<R, false>(hT1, hT0, S.y, X.z, S.z, K, a.flag_critical, hfy0, qyu0);
+#pragma unroll
+                for (int h = 0; h < CPL; ++h)
+                    if (col_ok[h] && rok && r >= r0 - 1)
+                        face_flux<R, false>(hT1[h], hT0[h], S[h].y, X[h].z, S[h].z, K, a.flag_critical, hfy0[h], qyu0[h]);
                 // (D) donor scale of (r-1, j)
-                const R qxu1_left = __shfl_up_sync(FULL, qxu1, 1);
-                if (col_ok && r >= r0 && r - 1 >= 0 && r - 1 < ny)
-                    sc1 = donor_scale_finite(qxu1, qxu1_left, qyu1, qyu0, hT1, K);
+                R qxu1_left[CPL];
+                left_of<R, CPL>(qxu1, qxu1_left, lane);
+                const bool drow = r >= r0 && r - 1 >= 0 && r - 1 < ny;
+#pragma unroll
+                for (int h = 0; h < CPL; ++h)
+                    if (col_ok[h] && drow) sc1[h] = donor_scale_finite(qxu1[h], qxu1_left[h], qyu1[h], qyu0[h], hT1[h], K);
                 // (E) limited faces of row r-1
-                const R sc1_right = __shfl_down_sync(FULL, sc1, 1);
-                qxl1 = limit_face_finite(qxu1, sc1, sc1_right);
-                qyl1 = limit_face_finite(qyu1, sc1, sc2);
+                R sc1_right[CPL];
+                right_of<R, CPL>(sc1, sc1_right, lane);
+#pragma unroll
+                for (int h = 0; h < CPL; ++h) {
+                    qxl1[h] = limit_face_finite(qxu1[h], sc1[h], sc1_right[h]);
+                    qyl1[h] = limit_face_finite(qyu1[h], sc1[h], sc2[h]);
+                }
             }
             // (F) continuity, outlet, maxima and CFL of row r-2.  When rows r-3..r-1 are dry
             // across the strip every flux into row r-2 is +0 (and so are its face depths):
             // continuity gives hT2 + 0 and the cell adds nothing to the CFL reductions.
             const bool quiet = (dry & 14u) == 14u;
-            const R qxl2_left = quiet ? R(0) : __shfl_up_sync(FULL, qxl2, 1);
+            R qxl2_left[CPL];
+            if (quiet) {
+#pragma unroll
+                for (int h = 0; h < CPL; ++h) qxl2_left[h] = R(0);
+            } else {
+                left_of<R, CPL>(qxl2, qxl2_left, lane);
+            }
             const int rm2 = r - 2;
-            if (own_lane && rm2 >= r0 && rm2 < r_end) {
-                const size_t c2 = size_t(rm2) * nx + j;
-                R hn = quiet ? hT2 + R(0) : continuity(hT2, qxl2_left, qxl2, qyl2, qyl1, K);
-                R hf3 = R(0);
-                const unsigned ord = mt2 >> 8;
-                if (ord) {
-                    const int o = int(ord) - 1;
-                    R ho;
-                    const R qq = outlet_sink(hn, a.outlet_coef[o], a.outlet_type, K, ho);
-                    hf3 = ho;
-                    a.hf3[o] = ho;
-                    a.qo[o] = qq;
-                    out_acc_r += qq * K.dt;
-                }
-                const R dm = dm2;
-                if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
-                // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
-                if (!quiet) {
-                    const R big = R(1e9);
-                    const R vr = qxl2 == R(0) ? qxl2 : qdiv(qxl2, hfx2 < K.tol ? big : hfx2);
-                    const R vu = qyl2 == R(0) ? qyl2 : qdiv(qyl2, hfy2 < K.tol ? big : hfy2);
-                    const R vb = qyl1 == R(0) ? qyl1 : qdiv(qyl1, hfy1 < K.tol ? big : hfy1);
-                    const R rc = j == 0 ? R(0.5) * vr : vr;
-                    const R uc = R(0.5) * (vu + vb);
-                    const R s2 = rc * rc + uc * uc;
-                    s2max = fmax(s2max, s2);
-                    if (s2 >= a.stag_s2) {
-                        const R dts = fmax(fmax(hfx2, hfy2), hf3);
-                        R cval;
-                        if (a.adaptive == 1) {
-                            cval = K.g * fmax(dts, R(0));
-                        } else {
-                            const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
-                            cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
-                        }
-                        cmaxv = fmax(cmaxv, cval);
+            const bool frow = rm2 >= r0 && rm2 < r_end;
+#pragma unroll
+            for (int h = 0; h < CPL; ++h) {
+                if (own_lane[h] && frow) {
+                    const size_t c2 = size_t(rm2) * nx + j[h];
+                    R hn = quiet ? hT2[h] + R(0) : continuity(hT2[h], qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
+                    R hf3 = R(0);
+                    const unsigned ord = mt2[h] >> 8;
+                    if (ord) {
+                        const int o = int(ord) - 1;
+                        R ho;
+                        const R qq = outlet_sink(hn, a.outlet_coef[o], a.outlet_type, K, ho);
+                        hf3 = ho;
+                        a.hf3[o] = ho;
+                        a.qo[o] = qq;
+                        out_acc_r += qq * K.dt;
                     }
+                    const R dm = dm2[h];
+                    if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
+                    // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
+                    if (!quiet) {
+                        const R big = R(1e9);
+                        const R vr = qxl2[h] == R(0) ? qxl2[h] : qdiv(qxl2[h], hfx2[h] < K.tol ? big : hfx2[h]);
+                        const R vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
+                        const R vb = qyl1[h] == R(0) ? qyl1[h] : qdiv(qyl1[h], hfy1[h] < K.tol ? big : hfy1[h]);
+                        const R rc = j[h] == 0 ? R(0.5) * vr : vr;
+                        const R uc = R(0.5) * (vu + vb);
+                        const R s2 = rc * rc + uc * uc;
+                        s2max = fmax(s2max, s2);
+                        if (s2 >= a.stag_s2) {
+                            const R dts = fmax(fmax(hfx2[h], hfy2[h]), hf3);
+                            R cval;
+                            if (a.adaptive == 1) {
+                                cval = K.g * fmax(dts, R(0));
+                            } else {
+                                const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
+                                cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
+                            }
+                            cmaxv = fmax(cmaxv, cval);
+                        }
+                    }
+                    V4 o4;
+                    o4.x = hn;
+                    o4.y = qxl2[h];
+                    o4.z = qyl2[h];
+                    o4.w = hn > dm ? hn : dm;   // save_output_maps.m:598, max(d_t, dmax)
+                    sout[c2] = o4;
                 }
-                V4 o4;
-                o4.x = hn;
-                o4.y = qxl2;
-                o4.z = qyl2;
-                o4.w = hn > dm ? hn : dm;   // save_output_maps.m:598, max(d_t, dmax)
-                sout[c2] = o4;
             }
             // (G) shift the window down one row
-            hT2 = hT1; hT1 = hT0;
-            qxu1 = qxu0; qyu1 = qyu0;
-            hfx2 = hfx1; hfx1 = hfx0;
-            hfy2 = hfy1; hfy1 = hfy0;
-            sc2 = sc1;
-            qxl2 = qxl1; qyl2 = qyl1;
-            dm2 = dm1; dm1 = X.w;
-            mt2 = mt1; mt1 = meta;
+#pragma unroll
+            for (int h = 0; h < CPL; ++h) {
+                hT2[h] = hT1[h]; hT1[h] = hT0[h];
+                qxu1[h] = qxu0[h]; qyu1[h] = qyu0[h];
+                hfx2[h] = hfx1[h]; hfx1[h] = hfx0[h];
+                hfy2[h] = hfy1[h]; hfy1[h] = hfy0[h];
+                sc2[h] = sc1[h];
+                qxl2[h] = qxl1[h]; qyl2[h] = qyl1[h];
+                dm2[h] = dm1[h]; dm1[h] = X[h].w;
+                mt2[h] = mt1[h]; mt1[h] = meta[h];
+            }
         }
         // every phase of the ring's barriers has completed: retire them so that the next
         // item of a persistent CTA can initialise them again
@@ -510,9 +590,9 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     return cta_ok;
 }
 
-template <typename R, int NT, int INF, bool MAP>
-__global__ void __launch_bounds__(NT, FusedOcc<R>::minb) k_fused_step(const FusedArgs<R> a) {
-    fused_item<R, NT, INF, MAP>(a, blockIdx.x);
+template <typename R, int NT, int INF, bool MAP, int CPL = 1>
+__global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb) k_fused_step(const FusedArgs<R> a) {
+    fused_item<R, NT, INF, MAP, CPL>(a, blockIdx.x);
 }
 
 // ---- batched ensemble ----------------------------------------------------------------
@@ -571,8 +651,8 @@ __global__ void k_ens_plan(const FusedArgs<R>* __restrict__ members, int n_membe
     }
 }
 
-template <typename R, int NT, int INF, bool MAP>
-__global__ void __launch_bounds__(NT, FusedOcc<R>::minb)
+template <typename R, int NT, int INF, bool MAP, int CPL = 1>
+__global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb)
 k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsigned* __restrict__ prefix,
            EnsQueue* q) {
     __shared__ FusedArgs<R> s_a;
@@ -605,7 +685,7 @@ k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsign
             for (int w = tid; w < int(sizeof(FusedArgs<R>) / 4); w += NT) dst[w] = src[w];
         }
         __syncthreads();
-        if (!fused_item<R, NT, INF, MAP>(s_a, s_local)) return;   // ring unusable after a timeout
+        if (!fused_item<R, NT, INF, MAP, CPL>(s_a, s_local)) return;   // ring unusable after a timeout
     }
 }
 

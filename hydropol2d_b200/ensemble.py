@@ -38,6 +38,9 @@ class Ensemble:
     def set_tuning(self, rows_per_warp: int) -> None:
         self._check(self._L.hp2d_ensemble_set_tuning(self._h, int(rows_per_warp)))
 
+    def set_layout(self, cells_per_lane: int) -> None:
+        self._check(self._L.hp2d_ensemble_set_layout(self._h, int(cells_per_lane)))
+
     def autotune(self, trial_steps: int = 4) -> int:
         rpw = C.c_int32()
         self._check(self._L.hp2d_ensemble_autotune(self._h, int(trial_steps), C.byref(rpw)))

@@ -156,6 +156,10 @@ class SurfaceFlow:
         self._check(self._L.hp2d_fused_steps_timed(self._h, int(n), C.byref(ms)))
         return ms.value
 
+    def set_layout(self, cells_per_lane: int):
+        """1 or 2 cells per lane in the fused kernel (32- or 64-column strips)."""
+        self._check(self._L.hp2d_set_layout(self._h, int(cells_per_lane)))
+
     def set_tuning(self, rows_per_warp: int):
         self._check(self._L.hp2d_set_tuning(self._h, int(rows_per_warp)))
 

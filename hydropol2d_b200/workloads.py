@@ -1,6 +1,7 @@
 """Named synthetic workloads for profiling and timing (each prints one line).
 
     python -m hydropol2d_b200.workloads wet [--steps N]        fully wet 2048 x 2048 grid
+    python -m hydropol2d_b200.workloads dambreak [--ny R]      the bench's dam-break on R x 8192 cells
     python -m hydropol2d_b200.workloads unet [--batch B]        U-Net forward + training step
     python -m hydropol2d_b200.workloads ensemble [--members M]  batched ensemble, a few launches
 
@@ -31,6 +32,18 @@ def wet(steps: int) -> str:
     ms = g.fused_steps_timed(200)
     g.close()
     return "wet 2048^2: %.4f ms/step, %.1f GCUPS" % (ms / 200, 2048 * 2048 * 200 / ms / 1e6)
+
+
+def dambreak(ny: int, steps: int) -> str:
+    """The dam-break of the benchmark on ny x 8192 cells (the bench's rows when ny = 4096)."""
+    from . import SurfaceFlow, synthetic as S
+    case = S.dambreak_case(ny, 8192, 5.0, seed=11)
+    g = SurfaceFlow(ny, 8192, 5.0, "fp32", **case.params)
+    case.apply(g)
+    g.fused_steps(steps)
+    ms = g.fused_steps_timed(200)
+    g.close()
+    return "dambreak %dx8192: %.4f ms/step, %.1f GCUPS" % (ny, ms / 200, ny * 8192 * 200 / ms / 1e6)
 
 
 def unet(batch: int) -> str:
@@ -85,7 +98,8 @@ def ensemble(members: int, launches: int) -> str:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["wet", "unet", "ensemble"])
+    ap.add_argument("workload", choices=["wet", "dambreak", "unet", "ensemble"])
+    ap.add_argument("--ny", type=int, default=2048)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--members", type=int, default=256)
@@ -93,6 +107,8 @@ def main():
     a = ap.parse_args()
     if a.workload == "wet":
         print(wet(a.steps), flush=True)
+    elif a.workload == "dambreak":
+        print(dambreak(a.ny, a.steps), flush=True)
     elif a.workload == "unet":
         print(unet(a.batch), flush=True)
     else:

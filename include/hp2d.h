@@ -195,9 +195,14 @@ hp2d_status hp2d_fused_steps_timed(hp2d_ctx* ctx, int32_t nsteps, float* elapsed
 /* Launch shape of the fused kernel: rows each warp streams through (>= 4).  Results do
  * not depend on it; hp2d_autotune picks it per grid. */
 hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp);
+/* Layout of the fused kernel: cells each lane streams side by side (1: 32-column strips
+ * with 28 output columns; 2: 64-column strips with 60).  Results do not depend on it;
+ * hp2d_autotune picks it with the rows per warp. */
+hp2d_status hp2d_set_layout(hp2d_ctx* ctx, int32_t cells_per_lane);
 /* Autotuner (no counterpart in the reference): times `trial_steps` fused steps from the
- * current state for each launch shape, undoes them (the state, clock and maxima are copied
- * aside first), keeps the fastest shape and returns it in *rows_per_warp (nullable). */
+ * current state for each launch shape (rows per warp x cells per lane), undoes them (the
+ * state, clock and maxima are copied aside first), keeps the fastest shape and returns its
+ * rows per warp in *rows_per_warp (nullable). */
 hp2d_status hp2d_autotune(hp2d_ctx* ctx, int32_t trial_steps, int32_t* rows_per_warp);
 /* Runs until the clock passes routing_time (or max_steps); returns steps executed. */
 hp2d_status hp2d_run(hp2d_ctx* ctx, int64_t max_steps, int64_t* steps_done);
@@ -232,8 +237,10 @@ hp2d_status hp2d_ensemble_create(int32_t device, hp2d_ensemble** out);
 hp2d_status hp2d_ensemble_destroy(hp2d_ensemble* ens);
 const char* hp2d_ensemble_last_error(const hp2d_ensemble* ens);
 hp2d_status hp2d_ensemble_add(hp2d_ensemble* ens, hp2d_ctx* member);
-/* rows each warp streams (>= 4) for every member; hp2d_ensemble_autotune picks it */
+/* rows each warp streams (>= 4) and cells per lane (1 or 2) for every member;
+ * hp2d_ensemble_autotune picks both */
 hp2d_status hp2d_ensemble_set_tuning(hp2d_ensemble* ens, int32_t rows_per_warp);
+hp2d_status hp2d_ensemble_set_layout(hp2d_ensemble* ens, int32_t cells_per_lane);
 hp2d_status hp2d_ensemble_autotune(hp2d_ensemble* ens, int32_t trial_steps, int32_t* rows_per_warp);
 /* nsteps launches; *n_active (nullable) = members still running afterwards */
 hp2d_status hp2d_ensemble_steps(hp2d_ensemble* ens, int32_t nsteps, int32_t* n_active);

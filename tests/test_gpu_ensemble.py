@@ -52,8 +52,8 @@ def check_member(g, ref, diag_ref, name):
         assert np.isclose(d[k], diag_ref[k], rtol=1e-5, atol=1e-9), (name, k, d[k], diag_ref[k])
 
 
-@pytest.mark.parametrize("rpw", [8, 24])
-def test_ensemble_members_match_oracle(rpw):
+@pytest.mark.parametrize("rpw,layout", [(8, 1), (24, 1), (16, 2), (32, 2)])
+def test_ensemble_members_match_oracle(rpw, layout):
     from hydropol2d_b200.ensemble import Ensemble
     cases = small_members()
     refs = [oracle_final(c) for c in cases]
@@ -62,6 +62,7 @@ def test_ensemble_members_match_oracle(rpw):
         for c in cases:
             ens.add(member(c))
         ens.set_tuning(rpw)
+        ens.set_layout(layout)
         launches = ens.run()
         assert launches >= max(r[1]["k"] for r in refs) - 1
         assert ens.steps(3) == 0   # launches after the end leave every member alone
