@@ -158,7 +158,7 @@ template <typename R> struct Impl : Base {
     explicit Impl(hp2d_ctx* c) : ctx(c) {
         if (sizeof(R) == 4) {   // measured defaults for FP32 (hp2d_autotune refines them per grid)
             cells_per_lane = 2;
-            rows_per_warp = 32;
+            rows_per_warp = 40;   // 4096 x 8192 dam-break: 94.7 GCUPS vs 93.5 at 32
         }
         ny = c->g.ny;
         nx = c->g.nx;
@@ -599,8 +599,9 @@ template <typename R> struct Impl : Base {
         a.flag_critical = p.flag_critical; a.outlet_type = p.outlet_type; a.ga = ga() ? 1 : 0;
         const int out_cols = 32 * cpl - 4;   // a strip's output columns (2-column apron each side)
         a.n_strips = (nx + out_cols - 1) / out_cols;
-        a.rows_per_warp = rows_per_warp;
-        a.n_warps_total = a.n_strips * ((ny + rows_per_warp - 1) / rows_per_warp);
+        const int rpw = rows_per_warp;
+        a.rows_per_warp = rpw;
+        a.n_warps_total = a.n_strips * ((ny + rpw - 1) / rpw);
         a.n_ctas = unsigned((a.n_warps_total + kThreads / 32 - 1) / (kThreads / 32));
         a.stag_s2 = stagnant_threshold<R>();
         a.stat = stat.p;

@@ -192,8 +192,8 @@ hp2d_status hp2d_fused_steps(hp2d_ctx* ctx, int32_t nsteps);
 /* hp2d_fused_steps bracketed by CUDA events on the context's stream; *elapsed_ms is the
  * device time of the nsteps launches (for benchmarking). */
 hp2d_status hp2d_fused_steps_timed(hp2d_ctx* ctx, int32_t nsteps, float* elapsed_ms);
-/* Launch shape of the fused kernel: rows each warp streams through (>= 4).  Results do
- * not depend on it; hp2d_autotune picks it per grid. */
+/* Launch shape of the fused kernel: rows each warp streams through (>= 4; FP32 default 40,
+ * FP64 64).  Results do not depend on it; hp2d_autotune times the candidates per grid. */
 hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp);
 /* Layout of the fused kernel: cells each lane streams side by side (1: 32-column strips
  * with 28 output columns; 2: 64-column strips with 60).  Results do not depend on it;
