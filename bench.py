@@ -10,7 +10,8 @@ sink, maxima, CFL reduction and timestep refresh) -- one fused kernel launch.
 
 N > 1 runs under torchrun, one rank per GPU, each rank an independent dam-break member
 (different DEM seed): ensemble members share nothing, so there is no collective on the
-data path (weak scaling).  Timing: CUDA events on the library's stream, barrier +
+data path (weak scaling).  The 256-member ensemble leg is split the same way: each rank
+runs its cost-balanced share (hydropol2d_b200.sharding), members/h is the whole job's.  Timing: CUDA events on the library's stream, barrier +
 synchronize on both sides, max over ranks.  The state (~1.5 GB) is far larger than L2,
 so no flush is needed between steps.
 """
@@ -189,38 +190,28 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def ensemble_leg(device: int, n_members: int = 256) -> dict:
+def ensemble_leg(device: int, n_members: int = 256) -> dict | None:
     """The batched-ensemble configuration: 256 members with sides log-uniform in
     [256, 1024] (multiples of 32), rain or breach forcing, run to their own end times in one
-    persistent launch per step; the launch shape is autotuned first (trial steps undone)."""
-    from hydropol2d_b200 import SurfaceFlow, synthetic as S
-    from hydropol2d_b200.ensemble import Ensemble
-    t0 = time.perf_counter()
-    cases = [S.ensemble_member(i) for i in range(n_members)]
-    t_gen = time.perf_counter() - t0
-    ens = Ensemble(device)
-    for c in cases:
-        g = SurfaceFlow(*c.shape, c.resolution, "fp32", device=device, **c.params)
-        c.apply(g)
-        ens.add(g)
-    rpw = ens.autotune(8)
-    total_ms, launches, active = 0.0, 0, n_members
-    while active:
-        active, ms = ens.steps_timed(512)
-        total_ms += ms
-        launches += 512
-    cu = ens.cell_updates()
-    ks = [m.diag()["k"] - 1 for m in ens.members]
-    cells = ens.cells()
-    ens.close()
-    sec = total_ms / 1e3
-    return {"members": n_members, "members_per_h": n_members / sec * 3600, "seconds": sec,
-            "gcups": cu / sec / 1e9, "cells": cells, "launches": launches, "rows_per_warp": rpw,
+    persistent launch per step; the launch shape is autotuned first (trial steps undone).
+    With N ranks every rank runs its share of the members on its own GPU (balanced by an a
+    priori cost, no collective on the data path) and the job's time is the slowest rank's.
+    Returns the summary on rank 0, None elsewhere."""
+    from hydropol2d_b200 import synthetic as S
+    from hydropol2d_b200.sharding import run_sharded
+    costs = [S.ensemble_member_cost(i) for i in range(n_members)]
+    res = run_sharded(S.ensemble_member, n_members, costs=costs, device=device)
+    if res is None:
+        return None
+    ks = [r["steps"] for r in res["results"]]
+    return {"members": n_members, "ranks": res["ranks"], "members_per_rank": res["members_per_rank"],
+            "members_per_h": res["members_per_h"], "seconds": res["seconds"], "gcups": res["gcups"],
+            "cells": sum(r["cells"] for r in res["results"]), "launches_rank0": res["launches_rank0"],
+            "rows_per_warp_rank0": res["rows_per_warp_rank0"],
             "steps_min": min(ks), "steps_max": max(ks), "steps_mean": float(np.mean(ks)),
-            "breach_members": sum(c.meta["kind"] == "breach" for c in cases),
-            "input_generation_s": t_gen,
-            "timing": "CUDA events on the ensemble's stream around every launch until the last "
-                      "member reaches its routing_time"}
+            "breach_members": sum(S.ensemble_member_spec(i)["kind"] == "breach" for i in range(n_members)),
+            "timing": "CUDA events on each rank's ensemble stream around every launch until its last "
+                      "member reaches its routing_time; max over ranks"}
 
 
 def run_surrogate(args):
@@ -347,15 +338,15 @@ def main():
     achieved = BYTES_PER_CELL * cells / (ms_per_step / 1e3) / 1e9
     traffic_pc = load_traffic()
 
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble_leg(local)   # every rank takes part (its share of the members)
+
     if rank != 0:
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()
         return
-
-    ens = None
-    if world == 1 and not args.no_ensemble:
-        ens = ensemble_leg(local)
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:

@@ -183,6 +183,37 @@ def _side(rng, lo: int = 256, hi: int = 1024, mult: int = 32) -> int:
     return int(min(hi, max(lo, mult * round(s / mult))))
 
 
+def ensemble_member_spec(i: int, seed: int = 2024, lo: int = 256, hi: int = 1024,
+                         breach_share: float = 0.25) -> dict:
+    """The seeded draws of ensemble member ``i`` (grid sides, roughness factor, forcing kind
+    and its parameters) without building its arrays; ``ensemble_member`` builds from these."""
+    rng = np.random.default_rng([seed, i])
+    ny, nx = _side(rng, lo, hi), _side(rng, lo, hi)
+    nfac = float(rng.uniform(0.7, 1.3))
+    if rng.uniform() >= breach_share:
+        rate = float(rng.uniform(20.0, 150.0))
+        dur = float(rng.uniform(30.0, 90.0))
+        return dict(kind="rain", ny=ny, nx=nx, n_factor=nfac, rate=rate, duration=dur)
+    return dict(kind="breach", ny=ny, nx=nx, n_factor=nfac, breach_factor=float(rng.uniform(0.2, 1.0)))
+
+
+def ensemble_member_cost(i: int, seed: int = 2024, lo: int = 256, hi: int = 1024, breach_share: float = 0.25,
+                         rain_tail_min: float = 30.0, breach_minutes: float = 30.0) -> float:
+    """A priori cell-updates of member ``i``: cells x (simulated seconds / a CFL timestep
+    alpha dx / sqrt(g h)), with h the event's rain depth (rain members, at least 1 cm) or the
+    reservoir depth (breach members).  Used to balance members across GPUs; the members'
+    real step counts come from their own CFL sequence."""
+    sp = ensemble_member_spec(i, seed, lo, hi, breach_share)
+    cells = sp["ny"] * sp["nx"]
+    if sp["kind"] == "rain":
+        h = max(sp["rate"] * sp["duration"] / 60.0 / 1000.0, 0.01)
+        dt = min(0.7 * 10.0 / np.sqrt(9.81 * h), 10.0)
+        return float(cells * (sp["duration"] + rain_tail_min) * 60.0 / dt)
+    h = 30.0 * max(sp["ny"] / 4096.0, 0.25)
+    dt = min(0.5 * 5.0 / np.sqrt(9.81 * h), 10.0)
+    return float(cells * breach_minutes * 60.0 / dt)
+
+
 def ensemble_member(i: int, seed: int = 2024, lo: int = 256, hi: int = 1024, breach_share: float = 0.25,
                     rain_tail_min: float = 30.0, breach_minutes: float = 30.0) -> Case:
     """Member ``i`` of the batched-ensemble configuration (HydroPol2D_Main_While_Ensemble.m
@@ -199,15 +230,13 @@ def ensemble_member(i: int, seed: int = 2024, lo: int = 256, hi: int = 1024, bre
       length with a breach of U(0.2, 1.0) x the valley width around the thalweg, n = 0.035
       x U(0.7, 1.3), ``breach_minutes`` simulated.
     """
-    rng = np.random.default_rng([seed, i])
-    ny, nx = _side(rng, lo, hi), _side(rng, lo, hi)
-    nfac = float(rng.uniform(0.7, 1.3))
-    if rng.uniform() >= breach_share:
+    sp = ensemble_member_spec(i, seed, lo, hi, breach_share)
+    ny, nx, nfac = sp["ny"], sp["nx"], sp["n_factor"]
+    if sp["kind"] == "rain":
         dx = 10.0
         z, ch = vtilt_domain(ny, nx, dx, 0.005, 0.002)
         z = z + 0.5 * gaussian_random_field(ny, nx, -3.0, seed * 7919 + i)
-        rate = float(rng.uniform(20.0, 150.0))
-        dur = float(rng.uniform(30.0, 90.0))
+        rate, dur = sp["rate"], sp["duration"]
         rows = np.zeros(ch.size, dtype=np.int32)
         params = dict(routing_time=dur + rain_tail_min, alfa_min=0.7, alfa_max=0.7, outlet_type=1,
                       slope_outlet=0.002, min_time_step=0.01, max_time_step=10.0)
@@ -216,7 +245,7 @@ def ensemble_member(i: int, seed: int = 2024, lo: int = 256, hi: int = 1024, bre
                     rain_uniform=(np.array([0.0, dur]), np.array([rate, 0.0])),
                     meta=dict(kind="rain", rate=rate, duration=dur, n_factor=nfac))
     dx = 5.0
-    f = float(rng.uniform(0.2, 1.0))
+    f = sp["breach_factor"]
     scale = ny / 4096.0
     grf = gaussian_random_field(ny, nx, -3.0, seed * 7919 + i) * 5.0 * scale
     y = (np.arange(ny) + 0.5) / ny * 2.0 - 1.0
