@@ -175,6 +175,11 @@ template <typename R> struct Impl : Base {
         hs.t_min = c->p.min_time_step / 60.0;
         hs.time_step = c->p.min_time_step / 60.0;   // HydroPol2D_preprocessing.m:2469
         hs.k = 1;
+        // the first step's rain: update_spatial_BC before the loop (HydroPol2D_Main_While.m:115)
+        // over [t_previous, t] with t_previous = 0 (:120)
+        hs.rain_a = 0.0;
+        hs.rain_b = hs.t_min;
+        hs.t_prev = 0.0;
         push_sc();
         // closed faces everywhere until hp2d_upload_static, dry state
         std::vector<V4> s(n), x(n);
@@ -429,11 +434,39 @@ template <typename R> struct Impl : Base {
         return HP2D_OK;
     }
 
+    // The rain interval follows the clock: k = 1 starts as a fresh run; k one above the
+    // current counter is the loop's advance (the interval becomes [t_previous, old clock]
+    // and t_previous the increment time_step on the first step, the old clock after it);
+    // any other k re-seeds it as if the last two steps had taken time_step
+    // (hp2d_set_rain_clock sets it exactly).
     hp2d_status set_clock(double t, double time_step, int64_t k) {
         pull_sc();
+        if (k == 1) {
+            hs.rain_a = 0.0;
+            hs.rain_b = t;
+            hs.t_prev = 0.0;
+        } else if (k == hs.k + 1) {
+            hs.rain_a = hs.t_prev;
+            hs.rain_b = hs.t_min;
+            hs.t_prev = hs.k == 1 ? time_step : hs.t_min;
+        } else {
+            hs.rain_a = t - 2.0 * time_step;
+            hs.rain_b = t - time_step;
+            hs.t_prev = t - time_step;
+        }
         hs.t_min = t;
         hs.time_step = time_step;
         hs.k = k;
+        push_sc();
+        dirty = true;
+        return HP2D_OK;
+    }
+
+    hp2d_status set_rain_clock(double rain_a, double rain_b, double t_previous) {
+        pull_sc();
+        hs.rain_a = rain_a;
+        hs.rain_b = rain_b;
+        hs.t_prev = t_previous;
         push_sc();
         dirty = true;
         return HP2D_OK;
@@ -457,6 +490,10 @@ template <typename R> struct Impl : Base {
 
     hp2d_status set_rain_maps(int32_t nm, int32_t my, int32_t mx, const float* rate, double map_dt) {
         if (nm <= 0 || my <= 0 || mx <= 0 || !(map_dt > 0)) { ctx->err = "bad rain map shape"; return HP2D_INVALID_ARG; }
+        if (map_dt * 60.0 < ctx->p.max_time_step) {   // a step's rain interval spans at most two maps
+            ctx->err = "rain map interval shorter than max_time_step";
+            return HP2D_INVALID_ARG;
+        }
         size_t cnt = size_t(nm) * my * mx;
         maps.alloc(cnt);
         upload(maps.p, std::vector<float>(rate, rate + cnt));
@@ -508,7 +545,7 @@ template <typename R> struct Impl : Base {
         push_sc();
         unpack();
         double dts = time_step * 60.0;
-        k_hydro_rain_ga<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), hs.t_min, dts, rain, h.p, I.p, T.p, soil.p,
+        k_hydro_rain_ga<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), hs.rain_a, hs.rain_b, dts, rain, h.p, I.p, T.p, soil.p,
                                                                classes.p, classes_vg.p, vgg, inf_mode(), sc.p);
         HP_CK(cudaGetLastError());
         k_hydro_clamp<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h.p, sc.p);
@@ -638,21 +675,21 @@ template <typename R> struct Impl : Base {
     }
     void opt_in() { opt_in_t<1>(); opt_in_t<2>(); }
 
-    template <int CPL> void launch_fused_t(const FusedArgs<R>& a) {
+    template <int INF, bool MAP, int CPL> void launch_one(const FusedArgs<R>& a) {
         const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
+        k_fused_step<R, kThreads, INF, MAP, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+    }
+    template <int CPL> void launch_fused_t(const FusedArgs<R>& a) {
         const bool map = rain.n_maps > 0;
         switch (inf_mode()) {
             case 1:
-                if (map) k_fused_step<R, kThreads, 1, true, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
-                else k_fused_step<R, kThreads, 1, false, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                if (map) launch_one<1, true, CPL>(a); else launch_one<1, false, CPL>(a);
                 break;
             case 2:
-                if (map) k_fused_step<R, kThreads, 2, true, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
-                else k_fused_step<R, kThreads, 2, false, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                if (map) launch_one<2, true, CPL>(a); else launch_one<2, false, CPL>(a);
                 break;
             default:
-                if (map) k_fused_step<R, kThreads, 0, true, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
-                else k_fused_step<R, kThreads, 0, false, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+                if (map) launch_one<0, true, CPL>(a); else launch_one<0, false, CPL>(a);
         }
     }
     void launch_fused(const FusedArgs<R>& a) {
@@ -949,6 +986,9 @@ template <typename R> struct Impl : Base {
         o->t = hs.t_min;
         o->time_step = hs.time_step;
         o->k = hs.k;
+        o->rain_t0 = hs.rain_a;
+        o->rain_t1 = hs.rain_b;
+        o->t_previous = hs.t_prev;
         o->max_velocity = hs.vmax_last;
         o->rain_volume = hs.rain_vol;
         o->infiltration_volume = hs.inf_vol;
@@ -1319,6 +1359,10 @@ hp2d_status hp2d_set_clock(hp2d_ctx* ctx, double t, double time_step, int64_t k)
 hp2d_status hp2d_set_rain_uniform(hp2d_ctx* ctx, int32_t n, const double* t_start, const double* rate) {
     if (n < 0 || (n > 0 && (!t_start || !rate))) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.set_rain_uniform(n, t_start, rate); });
+}
+
+hp2d_status hp2d_set_rain_clock(hp2d_ctx* ctx, double rain_t0, double rain_t1, double t_previous) {
+    return with_impl(ctx, [&](auto& m) { return m.set_rain_clock(rain_t0, rain_t1, t_previous); });
 }
 
 hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx, const float* rate, double map_dt) {

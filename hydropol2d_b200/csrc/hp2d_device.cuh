@@ -108,7 +108,7 @@ template <typename R> __device__ __forceinline__ R pow53(R x) {
 
 // ---------------- per-step constants (computed in FP64, rounded once) ------------------
 template <typename R> struct StepConsts {
-    R dt, gdt, dt_over_dx, dx_over_dt, inv_dt, inv_dx, rain_scale, g, tol, thr;
+    R dt, gdt, dt_over_dx, dx_over_dt, inv_dt, inv_dx, g, tol, thr;
     __device__ __host__ void make(double dt_s, double res, double tol_mm, double thr_mm) {
         dt = R(dt_s);
         gdt = R(kG * dt_s);
@@ -116,7 +116,6 @@ template <typename R> struct StepConsts {
         dx_over_dt = R(res / dt_s);
         inv_dt = R(1.0 / dt_s);
         inv_dx = R(1.0 / res);
-        rain_scale = R(dt_s / 3.6e6);
         g = R(kG);
         tol = R(tol_mm / 1000.0);
         thr = R(thr_mm / 1000.0);
@@ -143,6 +142,9 @@ struct StepScalars {
     int acc_neg;           // unfused path: some depth < -1e-8 mm after hydrology
     int pad;
     unsigned long long n_finite;   // cells with a finite depth (walls excluded)
+    // rain of the current step: the depth update_spatial_BC computed over the clock interval
+    // [rain_a, rain_b] at the end of the previous step, and the loop's t_previous [min]
+    double rain_a, rain_b, t_prev;
 };
 
 // non-negative floats/doubles order like their bit patterns
@@ -268,16 +270,61 @@ struct RainDesc {
     const float* maps;       // n_maps * my * mx
 };
 
-__device__ __forceinline__ double uniform_rate(const RainDesc& rd, double t) {
-    int idx = -1;
-    for (int q = 0; q < rd.n_uniform; ++q)
-        if (rd.t_start[q] <= t) idx = q;
-    return idx < 0 ? 0.0 : rd.rate[idx];
+// Integral [mm/h x min] over [a, b] of the uniform series: rate q holds from t_start[q] up to
+// t_start[q+1] (the last one for ever); non-finite rates add nothing
+// (update_spatial_BC.m:1131-1184 on the equivalent end-stamped series)
+__device__ __host__ inline double uniform_integral(const RainDesc& rd, double a, double b) {
+    double acc = 0.0;
+    if (!(b > a)) return acc;
+    for (int q = 0; q < rd.n_uniform; ++q) {
+        const double lo = rd.t_start[q];
+        const double hi = q + 1 < rd.n_uniform ? rd.t_start[q + 1] : b;
+        const double ov = fmax(0.0, fmin(b, hi) - fmax(a, lo));
+        if (ov > 0.0 && isfinite(rd.rate[q])) acc += rd.rate[q] * ov;
+    }
+    return acc;
 }
-__device__ __forceinline__ int map_index(const RainDesc& rd, double t) {
-    int m = (int)floor(t / rd.map_dt);
-    return max(0, min(m, rd.n_maps - 1));
-}
+
+template <typename R>
+__device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i, int j, int ny, int nx);
+
+// Rain of one step over the clock interval [a, b] [min]: a uniform depth, or the (at most
+// two) rate maps overlapping the interval with their overlaps (map m holds over
+// [m, m+1) x map_dt, nothing after the last map; update_spatial_BC.m:1287-1359).  Depths
+// are rate [mm/h] x overlap [min] / 60 [mm], in metres.
+template <typename R> struct RainStep {
+    R depth;       // uniform series [m]
+    int nm;        // maps overlapping the interval (0..2)
+    int m[2];
+    R w[2];        // overlap / 60000: mm/h -> m
+    __device__ __host__ void make(const RainDesc& rd, double a, double b) {
+        depth = rd.n_uniform ? R(uniform_integral(rd, a, b) / 60000.0) : R(0);
+        nm = 0;
+        m[0] = m[1] = 0;
+        w[0] = w[1] = R(0);
+        if (!rd.n_maps || !(b > a)) return;
+        const int m0 = max(0, int(floor(a / rd.map_dt)) - 1);
+        for (int q = m0; q < rd.n_maps && nm < 2; ++q) {
+            const double lo = q * rd.map_dt, hi = (q + 1) * rd.map_dt;
+            if (lo >= b) break;
+            const double ov = fmin(b, hi) - fmax(a, lo);
+            if (ov > 0.0) {
+                m[nm] = q;
+                w[nm] = R(ov / 60000.0);
+                ++nm;
+            }
+        }
+    }
+    // depth [m] the step adds at cell (i, j)
+    __device__ R at(const RainDesc& rd, int i, int j, int ny, int nx) const {
+        if (!rd.n_maps) return depth;
+        if (nm == 0) return R(0);
+        R r = w[0] * map_rate<R>(rd, rd.maps + size_t(m[0]) * rd.my * rd.mx, i, j, ny, nx);
+        if (nm > 1) r = r + w[1] * map_rate<R>(rd, rd.maps + size_t(m[1]) * rd.my * rd.mx, i, j, ny, nx);
+        return r;
+    }
+};
+
 template <typename R>
 __device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i, int j, int ny, int nx) {
     const R half = R(0.5);

@@ -168,8 +168,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     constexpr unsigned FULL = 0xffffffffu;
     __shared__ StepConsts<R> s_K;
     __shared__ double s_tmin, s_dts;
-    __shared__ int s_cur, s_skip, s_done, s_map, s_last;
-    __shared__ R s_rain;
+    __shared__ int s_cur, s_skip, s_done, s_last;
+    __shared__ RainStep<R> s_rs;
     __shared__ R red_s2[NT / 32];
     __shared__ unsigned long long red_c[NT / 32];
     __shared__ double red_d[3][NT / 32];
@@ -187,8 +187,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         s_skip = sc->skip_clamp;
         s_done = !(s_tmin <= a.t_end);
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
-        s_rain = a.rain.n_uniform ? R(uniform_rate(a.rain, s_tmin)) : R(0);
-        s_map = a.rain.n_maps ? map_index(a.rain, s_tmin) : -1;
+        s_rs.make(a.rain, sc->rain_a, sc->rain_b);
         if (!s_done && s_skip && blk == 0) sc->neg_warn += 1;
     }
     __syncthreads();
@@ -198,13 +197,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     const int ny = a.ny, nx = a.nx;
     const int cur = s_cur;
     const bool skip = s_skip != 0;
-    const R rain_u = s_rain;
+    const RainStep<R> RS = s_rs;
     const V4* __restrict__ sin = cur ? a.st1 : a.st0;
     V4* __restrict__ sout = cur ? a.st0 : a.st1;
     const V2* __restrict__ gin = cur ? a.gs1 : a.gs0;
     V2* __restrict__ gout = cur ? a.gs0 : a.gs1;
     const V4* __restrict__ stat = a.stat;
-    const float* map = (MAP && s_map >= 0) ? a.rain.maps + size_t(s_map) * a.rain.my * a.rain.mx : nullptr;
     const R t_arr = R(s_tmin * 60.0 + s_dts);
     const R NaNR = R(__int_as_float(0x7fc00000));
 
@@ -329,12 +327,11 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 if (col_ok[h] && rok) {
                     const size_t c = size_t(r) * nx + j[h];
                     R hh = X[h].x;
-                    const R rate = map ? map_rate<R>(a.rain, map, r, j[h], ny, nx) : rain_u;
-                    const R rr = rate * K.rain_scale;
+                    const R rr = MAP ? RS.at(a.rain, r, j[h], ny, nx) : RS.depth;
                     hh = hh + rr;
                     const bool own = own_lane[h] && own_row;
                     // uniform rain volume comes from the count of finite cells at the end
-                    if (MAP && map && own && isfinite(hh)) rain_acc_r += rr;
+                    if (MAP && own && isfinite(hh)) rain_acc_r += rr;
                     if (INF) {
                         const unsigned sc = meta[h] & 255u;
                         V2 go = Gs;
@@ -564,7 +561,6 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
 
     // ---- last CTA: refreshing_timestep + clock (HydroPol2D_Main_While.m:691-705, :779)
     __threadfence();
-    __shared__ double s_tnew, s_dtnew;
     if (tid == 0) {
         StepScalars* sc = a.sc;
         const unsigned long long vbits = atomicAdd(&sc->acc_vmax, 0ull);
@@ -578,7 +574,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         }
         double rain_s = atomicAdd(&sc->acc_rain, 0.0);
         // uniform rain: the same depth on every cell with a finite depth
-        if (a.rain.n_uniform) rain_s += double(s_rain * s_K.rain_scale) * double(sc->n_finite);
+        if (a.rain.n_uniform) rain_s += double(s_rs.depth) * double(sc->n_finite);
         const double inf_s = atomicAdd(&sc->acc_inf, 0.0);
         const double out_s = atomicAdd(&sc->acc_out, 0.0);
         const double t = s_tmin;
@@ -597,6 +593,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->rain_vol += rain_s * area;
         sc->inf_vol += inf_s * area;
         sc->out_vol += out_s * area;
+        // the next step's rain: update_spatial_BC over [t_previous, t]
+        // (HydroPol2D_Main_While.m:721), then t_previous <- the clock increment on the first
+        // step and t after it (:734-738), and the clock advances by the new step (:779)
+        sc->rain_a = sc->t_prev;
+        sc->rain_b = t;
+        sc->t_prev = sc->k == 1 ? tcr / 60.0 : t;
         sc->time_step = tcr / 60.0;
         sc->t_min = tcr / 60.0 + t;
         sc->k += 1;
@@ -607,25 +609,19 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->acc_inf = 0.0;
         sc->acc_out = 0.0;
         sc->counter = 0u;
-        s_tnew = sc->t_min;
-        s_dtnew = sc->time_step * 60.0;
+        s_rs.make(a.rain, sc->rain_a, sc->rain_b);   // the next step's rain
     }
     __syncthreads();
     // skip flag of the next step's clamp: only outlet cells can hold a negative depth
     // after a step (continuity clamps every other cell at zero).
     int neg = 0;
     if (a.n_outlets) {
-        StepConsts<R> K2;
-        K2.make(s_dtnew, a.res, a.tol_mm, a.thr_mm);
-        const int m2 = a.rain.n_maps ? map_index(a.rain, s_tnew) : -1;
-        const float* map2 = m2 >= 0 ? a.rain.maps + size_t(m2) * a.rain.my * a.rain.mx : nullptr;
-        const R ru = a.rain.n_uniform ? R(uniform_rate(a.rain, s_tnew)) : R(0);
+        const RainStep<R> RS2 = s_rs;
         for (int o = tid; o < a.n_outlets; o += NT) {
             const int c = a.outlet_cells[o];
             if (a.ga && (meta_bits(a.stat[c].w) & 255u) != 255u) continue;
             const int i = c / nx, j = c - (c / nx) * nx;
-            const R rate = map2 ? map_rate<R>(a.rain, map2, i, j, ny, nx) : ru;
-            const R hv = __ldcg(&sout[c].x) + rate * K2.rain_scale;
+            const R hv = __ldcg(&sout[c].x) + RS2.at(a.rain, i, j, ny, nx);
             if (hv < R(-1e-11)) neg = 1;
         }
     }
@@ -739,12 +735,8 @@ template <typename R>
 __global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>::V4* stat, int ny, int nx,
                             RainDesc rain, int ga, double res, double tol_mm, double thr_mm, StepScalars* sc) {
     const size_t n = size_t(ny) * nx;
-    const double t = sc->t_min, dts = sc->time_step * 60.0;
-    StepConsts<R> K;
-    K.make(dts, res, tol_mm, thr_mm);
-    const int m = rain.n_maps ? map_index(rain, t) : -1;
-    const float* map = m >= 0 ? rain.maps + size_t(m) * rain.my * rain.mx : nullptr;
-    const R ru = rain.n_uniform ? R(uniform_rate(rain, t)) : R(0);
+    RainStep<R> RS;
+    RS.make(rain, sc->rain_a, sc->rain_b);
     int neg = 0;
     unsigned long long fin = 0;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
@@ -752,8 +744,7 @@ __global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>
         if (isfinite(hc)) ++fin;
         if (ga && (meta_bits(stat[c].w) & 255u) != 255u) continue;
         const int i = int(c / nx), j = int(c % nx);
-        const R rate = map ? map_rate<R>(rain, map, i, j, ny, nx) : ru;
-        if (hc + rate * K.rain_scale < R(-1e-11)) neg = 1;
+        if (hc + RS.at(rain, i, j, ny, nx) < R(-1e-11)) neg = 1;
     }
     for (int o = 16; o > 0; o >>= 1) fin += __shfl_xor_sync(0xffffffffu, fin, o);
     if ((threadIdx.x & 31) == 0 && fin) atomicAdd(&sc->n_finite, fin);

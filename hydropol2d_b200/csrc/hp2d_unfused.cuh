@@ -17,21 +17,19 @@ template <typename R> struct GridView {
 
 // rain + Green-Ampt (Hydrological_Model.m:14-42); records whether any depth < -1e-8 mm
 template <typename R>
-__global__ void k_hydro_rain_ga(GridView<R> g, double t_min, double dt_s, RainDesc rain, R* h, R* I, R* T,
+__global__ void k_hydro_rain_ga(GridView<R> g, double rain_a, double rain_b, double dt_s, RainDesc rain, R* h, R* I, R* T,
                                 const uint8_t* soil, const SoilClass<R>* classes, const SoilClassVG<R>* classes_vg,
                                 VGGlobals<R> vg, int inf, StepScalars* sc) {
     StepConsts<R> K;
     K.make(dt_s, g.res, g.tol_mm, g.thr_mm);
-    const int m = rain.n_maps ? map_index(rain, t_min) : -1;
-    const float* map = m >= 0 ? rain.maps + size_t(m) * rain.my * rain.mx : nullptr;
-    const R ru = rain.n_uniform ? R(uniform_rate(rain, t_min)) : R(0);
+    RainStep<R> RS;
+    RS.make(rain, rain_a, rain_b);
     const size_t n = size_t(g.ny) * g.nx;
     double racc = 0, iacc = 0;
     int neg = 0;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
         const int i = int(c / g.nx), j = int(c % g.nx);
-        const R rate = map ? map_rate<R>(rain, map, i, j, g.ny, g.nx) : ru;
-        const R r = rate * K.rain_scale;
+        const R r = RS.at(rain, i, j, g.ny, g.nx);
         R hh = h[c] + r;
         if (isfinite(hh)) racc += double(r);
         if (inf && soil[c] != 255) {

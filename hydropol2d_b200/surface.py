@@ -119,6 +119,11 @@ class SurfaceFlow:
     def set_clock(self, t: float, time_step: float, k: int = 1):
         self._check(self._L.hp2d_set_clock(self._h, float(t), float(time_step), int(k)))
 
+    def set_rain_clock(self, rain_t0: float, rain_t1: float, t_previous: float):
+        """The clock interval whose rain the next step applies and the loop's t_previous
+        [min] (``diag`` reports them), for an exact restart."""
+        self._check(self._L.hp2d_set_rain_clock(self._h, float(rain_t0), float(rain_t1), float(t_previous)))
+
     def set_rain_uniform(self, t_start, rate):
         t = _f64(t_start).ravel()
         r = _f64(rate).ravel()

@@ -107,6 +107,8 @@ typedef struct hp2d_diag {
     int64_t neg_depth_warnings;   /* Hydrological_Model.m:45-47 events */
     int64_t unstable_steps;       /* refreshing_timestep.m:357-359 events */
     int64_t status_bits;          /* bit 0: non-finite state seen */
+    double rain_t0, rain_t1;      /* clock interval whose rain the next step applies [min] */
+    double t_previous;            /* the loop's t_previous [min] */
 } hp2d_diag;
 
 typedef struct hp2d_ctx hp2d_ctx;
@@ -157,19 +159,36 @@ hp2d_status hp2d_set_soil_vg(hp2d_ctx* ctx, const uint8_t* soil_class, int32_t n
 hp2d_status hp2d_set_state(hp2d_ctx* ctx, const double* d, const double* outflow,
                            const double* soil_storage);
 
-/* Clock [min], the step the next call applies [min] and the step counter k (1-based). */
+/* Clock [min], the step the next call applies [min] and the step counter k (1-based).
+ * The rain interval follows it: k = 1 starts a run (interval [0, t], t_previous 0); k one
+ * above the current counter is the loop's advance (HydroPol2D_Main_While.m:721-779: the
+ * interval becomes [t_previous, previous clock], t_previous becomes time_step after the
+ * first step and the previous clock after that); any other k re-seeds the interval as if
+ * the last two steps had taken time_step. */
 hp2d_status hp2d_set_clock(hp2d_ctx* ctx, double t, double time_step, int64_t k);
 
-/* Rain forcing.  Uniform: piecewise-constant rates [mm/h] starting at t_start [min].
- * Maps: n_maps coarse fields (my x mx, row-major) [mm/h], map m active for
- * t in [m*map_dt, (m+1)*map_dt) [min], bilinearly interpolated to the grid. */
+/* The rain interval [rain_t0, rain_t1] [min] whose rain the next step applies and the loop's
+ * t_previous [min] (the update_spatial_BC state; hp2d_get_diag reports them), for an exact
+ * restart. */
+hp2d_status hp2d_set_rain_clock(hp2d_ctx* ctx, double rain_t0, double rain_t1, double t_previous);
+
+/* Rain forcing.  A step applies the rain of a clock interval, as update_spatial_BC.m does
+ * at the end of the step before it: the exact integral of the piecewise-constant rate
+ * over the interval (:435-470, :1131-1184; maps :536-558, :1287-1359), / 60 -> mm.
+ * Uniform: rates [mm/h] holding from t_start[q] [min] up to t_start[q+1], the last one for
+ * ever (an end-stamped series converts by prepending its first start and appending a
+ * zero rate).  Maps: n_maps coarse fields (my x mx, row-major) [mm/h], map m holding over
+ * [m*map_dt, (m+1)*map_dt) [min] and nothing after the last one, bilinearly interpolated
+ * to the grid; map_dt*60 must be at least params.max_time_step [s] (a step's interval then
+ * overlaps at most two maps). */
 hp2d_status hp2d_set_rain_uniform(hp2d_ctx* ctx, int32_t n, const double* t_start,
                                   const double* rate);
 hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx,
                                const float* rate, double map_dt);
 
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
-/* Hydrological_Model for this path: adds delta_p_agg = rate(t) * time_step/60 mm,
+/* Hydrological_Model for this path: adds delta_p_agg (the rain of the current rain
+ * interval, see hp2d_set_rain_uniform),
  * runs the Infiltration_Module (Green-Ampt when flag_infiltration=1, van Genuchten when 2)
  * and the clamp; the
  * resident depth becomes d_tot. */

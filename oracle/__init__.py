@@ -62,6 +62,7 @@ def _load():
             "oracle_set_state": ([vp, dp, dp, dp], C.c_int),
             "oracle_set_depth": ([vp, dp], C.c_int),
             "oracle_set_clock": ([vp, C.c_double, C.c_double, C.c_int64], C.c_int),
+            "oracle_set_rain_clock": ([vp, C.c_double, C.c_double, C.c_double], C.c_int),
             "oracle_set_rain_uniform": ([vp, C.c_int32, dp, dp], C.c_int),
             "oracle_set_rain_maps": ([vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_float), C.c_double], C.c_int),
             "oracle_hydrology_step": ([vp, C.c_double], C.c_int),
@@ -138,6 +139,9 @@ class KernelFormOracle:
 
     def set_clock(self, t, time_step, k=1):
         self._L.oracle_set_clock(self._h, float(t), float(time_step), int(k))
+
+    def set_rain_clock(self, rain_t0, rain_t1, t_previous):
+        self._L.oracle_set_rain_clock(self._h, float(rain_t0), float(rain_t1), float(t_previous))
 
     def set_rain_uniform(self, t_start, rate):
         t = np.ascontiguousarray(t_start, dtype=np.float64).ravel()

@@ -113,7 +113,7 @@ inline double qdiv(double a, double b) { return a / b; }
 template <typename R> inline bool finite(R v) { return std::isfinite(v); }
 
 template <typename R> struct Consts {
-    R dt, gdt, dt_over_dx, dx_over_dt, inv_dt, inv_dx, rain_scale, g, tol, thr,
+    R dt, gdt, dt_over_dx, dx_over_dt, inv_dt, inv_dx, g, tol, thr,
       clamp_eps, neg_eps, ten, half, stagnant, celer_floor, big_depth;
     Consts(double dt_s, double res, double tol_mm, double thr_mm) {
         dt = R(dt_s);
@@ -122,7 +122,6 @@ template <typename R> struct Consts {
         dx_over_dt = R(res / dt_s);
         inv_dt = R(1.0 / dt_s);
         inv_dx = R(1.0 / res);
-        rain_scale = R(dt_s / 3.6e6);
         g = R(kG);
         tol = R(tol_mm / 1000.0);
         thr = R(thr_mm / 1000.0);
@@ -160,6 +159,10 @@ public:
     // clock
     double t_min = 0, time_step = 0, tsp = 0;   // clock [min], step [min], time_save_previous
     int64_t k = 1;
+    // rain interval of the current step and the loop's t_previous [min]; the first step's
+    // comes from the update_spatial_BC call before the loop (HydroPol2D_Main_While.m:115)
+    // with t_previous = 0 (:120)
+    double rain_a = 0, rain_b = 0, t_prev = 0;
     // diagnostics
     double vmax_last = 0, rain_vol = 0, inf_vol = 0, out_vol = 0;
     int64_t neg_warn = 0, unstable = 0;
@@ -176,6 +179,21 @@ public:
         qx_unl.assign(n, R(0)); qy_unl.assign(n, R(0)); scale.assign(n, R(1));
         time_step = p.min_time_step / 60.0;   // HydroPol2D_preprocessing.m:2469
         t_min = p.min_time_step / 60.0;
+        rain_b = t_min;
+    }
+
+    // the clock setter of the unfused drivers: k = 1 starts a run, k + 1 is the loop's
+    // advance (HydroPol2D_Main_While.m:721, :734-738), any other k re-seeds the rain
+    // interval as if the last two steps had taken time_step
+    void set_clock(double t, double ts, int64_t kk) {
+        if (kk == 1) {
+            rain_a = 0.0; rain_b = t; t_prev = 0.0;
+        } else if (kk == k + 1) {
+            rain_a = t_prev; rain_b = t_min; t_prev = k == 1 ? ts : t_min;
+        } else {
+            rain_a = t - 2.0 * ts; rain_b = t - ts; t_prev = t - ts;
+        }
+        t_min = t; time_step = ts; k = kk;
     }
 
     size_t at(int i, int j) const { return size_t(i) * nx + j; }
@@ -263,37 +281,79 @@ public:
         for (size_t c = 0; c < h.size(); ++c) h[c] = R(d_mm[c] / 1000.0);
     }
 
-    // rain rate [mm/h] in R for cell (i, j) at clock t [min]
-    R rain_rate(int i, int j, double t) const {
-        if (n_maps > 0) {
-            int m = int(std::floor(t / map_dt));
-            m = std::max(0, std::min(m, n_maps - 1));
-            const float* f = maps.data() + size_t(m) * my * mx;
-            const R half = R(0.5);
-            R fy = (R(i) + half) * R(double(my) / ny) - half;
-            R fx = (R(j) + half) * R(double(mx) / nx) - half;
-            fy = std::fmin(std::fmax(fy, R(0)), R(my - 1));
-            fx = std::fmin(std::fmax(fx, R(0)), R(mx - 1));
-            int iy0 = int(std::floor(fy)), ix0 = int(std::floor(fx));
-            int iy1 = std::min(iy0 + 1, my - 1), ix1 = std::min(ix0 + 1, mx - 1);
-            R wy = fy - R(iy0), wx = fx - R(ix0);
-            R f00 = R(f[iy0 * mx + ix0]), f01 = R(f[iy0 * mx + ix1]);
-            R f10 = R(f[iy1 * mx + ix0]), f11 = R(f[iy1 * mx + ix1]);
-            R top = (R(1) - wx) * f00 + wx * f01;
-            R bot = (R(1) - wx) * f10 + wx * f11;
-            return (R(1) - wy) * top + wy * bot;
+    // ---------------- rain of a step (update_spatial_BC.m:435-470, :536-558) ----------------
+    // A step applies the rain of the clock interval [rain_a, rain_b]: the exact integral of
+    // the piecewise-constant rate over it (localAverageRateOverStep x interval,
+    // update_spatial_BC.m:1131-1184; maps :1287-1359) / 60 -> mm, here in metres.  Uniform
+    // rates hold from rain_t[q] up to rain_t[q+1] (the last for ever); map m holds over
+    // [m, m+1) x map_dt and nothing after the last map; an interval overlaps at most two maps
+    // (map_dt >= max_time_step, checked by the library).
+    struct StepRain {
+        R depth = R(0);        // uniform [m]
+        int nm = 0;
+        int m[2] = {0, 0};
+        R w[2] = {R(0), R(0)}; // overlap [min] / 60000
+    };
+    StepRain step_rain(double a, double b) const {
+        StepRain s;
+        if (!rain_r.empty()) {
+            double acc = 0.0;
+            if (b > a) {
+                const size_t nq = rain_r.size();
+                for (size_t q = 0; q < nq; ++q) {
+                    const double lo = rain_t[q];
+                    const double hi = q + 1 < nq ? rain_t[q + 1] : b;
+                    const double ov = std::fmax(0.0, std::fmin(b, hi) - std::fmax(a, lo));
+                    if (ov > 0.0 && std::isfinite(rain_r[q])) acc += rain_r[q] * ov;
+                }
+            }
+            s.depth = R(acc / 60000.0);
         }
-        if (rain_r.empty()) return R(0);
-        int idx = -1;
-        for (size_t q = 0; q < rain_t.size(); ++q)
-            if (rain_t[q] <= t) idx = int(q);
-        if (idx < 0) return R(0);
-        return R(rain_r[idx]);
+        if (n_maps > 0 && b > a) {
+            const int m0 = std::max(0, int(std::floor(a / map_dt)) - 1);
+            for (int q = m0; q < n_maps && s.nm < 2; ++q) {
+                const double lo = q * map_dt, hi = (q + 1) * map_dt;
+                if (lo >= b) break;
+                const double ov = std::fmin(b, hi) - std::fmax(a, lo);
+                if (ov > 0.0) {
+                    s.m[s.nm] = q;
+                    s.w[s.nm] = R(ov / 60000.0);
+                    ++s.nm;
+                }
+            }
+        }
+        return s;
+    }
+    // cell-centred bilinear sample of map m at cell (i, j) [mm/h]
+    R map_sample(int m, int i, int j) const {
+        const float* f = maps.data() + size_t(m) * my * mx;
+        const R half = R(0.5);
+        R fy = (R(i) + half) * R(double(my) / ny) - half;
+        R fx = (R(j) + half) * R(double(mx) / nx) - half;
+        fy = std::fmin(std::fmax(fy, R(0)), R(my - 1));
+        fx = std::fmin(std::fmax(fx, R(0)), R(mx - 1));
+        int iy0 = int(std::floor(fy)), ix0 = int(std::floor(fx));
+        int iy1 = std::min(iy0 + 1, my - 1), ix1 = std::min(ix0 + 1, mx - 1);
+        R wy = fy - R(iy0), wx = fx - R(ix0);
+        R f00 = R(f[iy0 * mx + ix0]), f01 = R(f[iy0 * mx + ix1]);
+        R f10 = R(f[iy1 * mx + ix0]), f11 = R(f[iy1 * mx + ix1]);
+        R top = (R(1) - wx) * f00 + wx * f01;
+        R bot = (R(1) - wx) * f10 + wx * f11;
+        return (R(1) - wy) * top + wy * bot;
+    }
+    // rain depth [m] the step adds at cell (i, j)
+    R rain_depth(const StepRain& s, int i, int j) const {
+        if (n_maps <= 0) return s.depth;
+        if (s.nm == 0) return R(0);
+        R r = s.w[0] * map_sample(s.m[0], i, j);
+        if (s.nm > 1) r = r + s.w[1] * map_sample(s.m[1], i, j);
+        return r;
     }
 
     // ---------------- hydrology: rain + Green-Ampt + clamp ----------------
     void hydrology(double dts) {
         Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
+        const StepRain SR = step_rain(rain_a, rain_b);
         size_t n = size_t(ny) * nx;
         double rv = 0, iv = 0;
         const bool ga = p.flag_infiltration == 1 && !soil.empty();
@@ -301,7 +361,7 @@ public:
         for (int i = 0; i < ny; ++i)
             for (int j = 0; j < nx; ++j) {
                 size_t c = at(i, j);
-                R r = rain_rate(i, j, t_min) * K.rain_scale;
+                R r = rain_depth(SR, i, j);
                 R hh = h[c] + r;
                 if (std::isfinite(double(hh))) rv += double(r);
                 if (ga && soil[c] != 255) {
@@ -555,6 +615,11 @@ public:
             if (tcr == p.min_time_step) ++unstable;
         }
         track(t_min * 60.0 + dts);
+        // the next step's rain interval: [t_previous, t] (HydroPol2D_Main_While.m:721), then
+        // t_previous <- the increment on the first step, t after it (:734-738)
+        rain_a = t_prev;
+        rain_b = t_min;
+        t_prev = k == 1 ? tcr / 60.0 : t_min;
         time_step = tcr / 60.0;
         t_min = tcr / 60.0 + t_min;
         ++k;

@@ -501,20 +501,69 @@ def bilinear_rain(field: np.ndarray, ny: int, nx: int, dtype=np.float64) -> np.n
     return ((one - wy) * top + wy * bot).astype(dtype)
 
 
-def rain_rate_at(cfg: RunConfig, t_min: float, ny: int, nx: int):
-    """Rain rate (mm/h) for the step starting at clock ``t_min``: scalar or (ny, nx)."""
+def average_rate_over_step(times_end, values, t0: float, t1: float) -> float:
+    """``localAverageRateOverStep`` (update_spatial_BC.m:1131-1184): the exact time average
+    over [t0, t1] of an END-stamped piecewise-constant series -- value i holds from
+    times_end[i-1] (times_end[0] minus the series' spacing for i = 0) up to times_end[i] and
+    nothing after the last end; non-finite values contribute nothing.  0 when t1 <= t0."""
+    times = np.asarray(times_end, dtype=np.float64)
+    vals = np.asarray(values, dtype=np.float64)
+    n = min(len(times), len(vals))
+    if n == 0 or not (np.isfinite(t0) and np.isfinite(t1)) or t1 <= t0:
+        return 0.0
+    dt_force = times[1] - times[0] if n >= 2 else 0.0   # localEstimateConstantDt, :1240-1253
+    if not np.isfinite(dt_force) or dt_force <= 0:
+        dt_force = 0.0
+    acc = 0.0
+    for i in range(n):
+        ts = times[0] - dt_force if i == 0 else times[i - 1]
+        ov = max(0.0, min(t1, times[i]) - max(t0, ts))
+        if ov > 0 and np.isfinite(vals[i]):
+            acc += vals[i] * ov
+        if times[i] >= t1:
+            break
+    return acc / (t1 - t0)
+
+
+def rain_depth_mm(cfg: RunConfig, t0: float, t1: float, ny: int, nx: int):
+    """Rain depth [mm] a step receives from the clock interval [t0, t1] [min]: the exact
+    integral of the piecewise-constant rate over the interval / 60, which is what
+    update_spatial_BC.m:435-470 (uniform series: average rate x interval / 60) and :536-558
+    with :1287-1359 (rate maps: time-weighted map average x interval / 60) give.  The uniform
+    series here is START-stamped -- rate q holds from times[q] up to times[q+1], the last one
+    for ever -- and map m holds over [m, m+1) x map_dt and nothing after the last map
+    (an end-stamped series converts by prepending its first start and appending a zero).
+    Scalar for a uniform series, (ny, nx) for maps."""
+    if t1 <= t0:
+        return 0.0 if cfg.rain_maps_mmh is None else np.zeros((ny, nx))
     if cfg.rain_maps_mmh is not None:
-        k = int(math.floor(t_min / cfg.rain_map_dt_min))
-        k = max(0, min(k, cfg.rain_maps_mmh.shape[0] - 1))
-        return bilinear_rain(cfg.rain_maps_mmh[k], ny, nx)
+        acc = np.zeros((ny, nx))
+        dtm = cfg.rain_map_dt_min
+        for m in range(cfg.rain_maps_mmh.shape[0]):
+            ov = max(0.0, min(t1, (m + 1) * dtm) - max(t0, m * dtm))
+            if ov > 0:
+                acc = acc + ov * bilinear_rain(cfg.rain_maps_mmh[m], ny, nx)
+        return acc / 60.0
     if cfg.rain_rates_mmh is None:
         return 0.0
     times = np.asarray(cfg.rain_times_min, dtype=np.float64)
     rates = np.asarray(cfg.rain_rates_mmh, dtype=np.float64)
-    idx = int(np.searchsorted(times, t_min, side="right")) - 1
-    if idx < 0 or idx >= len(rates):
-        return 0.0
-    return float(rates[idx])
+    acc = 0.0
+    for q in range(len(rates)):
+        hi = times[q + 1] if q + 1 < len(times) else np.inf
+        ov = max(0.0, min(t1, hi) - max(t0, times[q]))
+        if ov > 0 and np.isfinite(rates[q]):
+            acc += rates[q] * ov
+    return acc / 60.0
+
+
+def next_rain_interval(a: float, b: float, t_previous: float, t: float, k: int, tcr_s: float):
+    """The loop's bookkeeping of the rain interval.  At the end of iteration k (clock t, the
+    end of step k) update_spatial_BC computes the depth the NEXT step applies over
+    [t_previous, t] (HydroPol2D_Main_While.m:721); then t_previous becomes the clock
+    increment on the first iteration and t after that (:734-738) and the clock advances by
+    the new step (:779).  Returns the next step's (a, b) and the new t_previous."""
+    return t_previous, t, (tcr_s / 60.0 if k == 1 else t)
 
 
 @dataclass
@@ -534,6 +583,12 @@ class RunState:
     rain_volume: float = 0.0
     infiltration_volume: float = 0.0
     outlet_volume: float = 0.0
+    # rain interval [rain_a, rain_b] of the current step and the loop's t_previous [min]; the
+    # first step's comes from the call before the loop (HydroPol2D_Main_While.m:115) with
+    # t_previous = 0 (:120)
+    rain_a: float = 0.0
+    rain_b: float = 0.0
+    t_previous: float = 0.0
     history: list = field(default_factory=list)
 
 
@@ -546,7 +601,8 @@ def init_state(cfg: RunConfig) -> RunState:
     ts = (cfg.fixed_time_step_s if cfg.fixed_time_step_s else cfg.min_time_step) / 60
     return RunState(d=d, outflow=np.zeros((3, ny, nx)), I=I, T=T,
                     dmax=np.full((ny, nx), -np.inf), arrival=np.full((ny, nx), np.inf),
-                    t=cfg.min_time_step / 60, k=1, time_step=ts)
+                    t=cfg.min_time_step / 60, k=1, time_step=ts,
+                    rain_a=0.0, rain_b=cfg.min_time_step / 60, t_previous=0.0)
 
 
 def step(cfg: RunConfig, st: RunState) -> None:
@@ -556,8 +612,8 @@ def step(cfg: RunConfig, st: RunState) -> None:
     A = res * res
     time_step = st.time_step
     # Hydrological_Model.m:14-55; rain via interception_module.m:68 + Snow_Module.m:99
-    rate = rain_rate_at(cfg, st.t, ny, nx)
-    delta_p = rate * (time_step / 60)
+    # the depth update_spatial_BC computed for this step at the end of the previous one
+    delta_p = rain_depth_mm(cfg, st.rain_a, st.rain_b, ny, nx)
     d_t = st.d + delta_p
     st.rain_volume += float(np.nansum(np.broadcast_to(delta_p, (ny, nx)))) * A / 1000
     if cfg.ga is not None:
@@ -603,6 +659,8 @@ def step(cfg: RunConfig, st: RunState) -> None:
     # HydroPol2D_Main_While.m:766-782 (state carry, clock by the new dt)
     st.d = out.d_t
     st.outflow = out.outflow
+    st.rain_a, st.rain_b, st.t_previous = next_rain_interval(st.rain_a, st.rain_b, st.t_previous, st.t,
+                                                             st.k, tcr)
     st.time_step = tcr / 60
     st.t = tcr / 60 + st.t
     st.k += 1

@@ -59,9 +59,16 @@ int oracle_set_depth(oracle_model* m, const double* d) {
 
 int oracle_set_clock(oracle_model* m, double t, double time_step, int64_t k) {
     return dispatch(m, [&](auto& M) {
-        M.t_min = t;
-        M.time_step = time_step;
-        M.k = k;
+        M.set_clock(t, time_step, k);
+        return 0;
+    });
+}
+
+int oracle_set_rain_clock(oracle_model* m, double a, double b, double t_previous) {
+    return dispatch(m, [&](auto& M) {
+        M.rain_a = a;
+        M.rain_b = b;
+        M.t_prev = t_previous;
         return 0;
     });
 }
@@ -179,6 +186,9 @@ int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
         o->neg_depth_warnings = M.neg_warn;
         o->unstable_steps = M.unstable;
         o->status_bits = 0;
+        o->rain_t0 = M.rain_a;
+        o->rain_t1 = M.rain_b;
+        o->t_previous = M.t_prev;
         return 0;
     });
 }

@@ -40,6 +40,7 @@ def test_vg_hydrology_step_matches_literal(precision, rtol, atol):
     case, soil, I0 = vg_case()
     g = make(case, soil, I0, precision)
     ts = 0.5   # minutes
+    g.set_rain_clock(0.0, ts, 0.0)   # the step applies the rain of [0, ts]
     d = g.diag()
     g.hydrology_step(ts)
     h = g.download("depth")

@@ -105,7 +105,7 @@ def test_green_ampt_step_agrees(oracle_lib):
     d = np.random.default_rng(0).uniform(0, 30, case.shape)
     o.set_state(d, None, case.I0)
     o.hydrology_step(ts)
-    dl, Il, Tl, f = L.green_ampt_infiltration(d + L.rain_rate_at(cfg, st.t, *case.shape) * (ts / 60), st.I, st.T,
+    dl, Il, Tl, f = L.green_ampt_infiltration(d + L.rain_depth_mm(cfg, st.rain_a, st.rain_b, *case.shape), st.I, st.T,
                                               ts, cfg.ga, case.resolution)
     dl[dl < 1e-6] = 0
     assert np.allclose(o.download_native("h") * 1000, dl, rtol=1e-10, atol=1e-9)
