@@ -145,6 +145,8 @@ struct StepScalars {
     // rain of the current step: the depth update_spatial_BC computed over the clock interval
     // [rain_a, rain_b] at the end of the previous step, and the loop's t_previous [min]
     double rain_a, rain_b, t_prev;
+    int skip_next;         // fused step: some outlet cell ends below -1e-11 m after the next rain
+    int pad2;
 };
 
 // non-negative floats/doubles order like their bit patterns

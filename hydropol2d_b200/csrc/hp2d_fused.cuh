@@ -169,7 +169,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     __shared__ StepConsts<R> s_K;
     __shared__ double s_tmin, s_dts;
     __shared__ int s_cur, s_skip, s_done, s_last;
-    __shared__ RainStep<R> s_rs;
+    __shared__ RainStep<R> s_rs, s_rsn;   // this step's rain and the next one's
     __shared__ R red_s2[NT / 32];
     __shared__ unsigned long long red_c[NT / 32];
     __shared__ double red_d[3][NT / 32];
@@ -188,6 +188,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         s_done = !(s_tmin <= a.t_end);
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
         s_rs.make(a.rain, sc->rain_a, sc->rain_b);
+        // the next step applies the rain of [t_previous, t] (HydroPol2D_Main_While.m:721)
+        s_rsn.make(a.rain, sc->t_prev, s_tmin);
         if (!s_done && s_skip && blk == 0) sc->neg_warn += 1;
     }
     __syncthreads();
@@ -212,6 +214,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     double rain_acc = 0.0, inf_acc = 0.0, out_acc = 0.0;
     R rain_acc_r = R(0), inf_acc_r = R(0), out_acc_r = R(0);   // per-lane partial sums (ledger only)
     unsigned dry = 0u;                        // bit i: row r-i dry across the strip
+    int neg_next = 0;                         // an outlet cell would go below -1e-11 m after the next rain
     R s2max = R(0);
     R cmaxv = R(-1);   // largest celerity term of a non-stagnant cell (-1: none yet)
 
@@ -454,6 +457,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         a.hf3[o] = ho;
                         a.qo[o] = qq;
                         out_acc_r += qq * K.dt;
+                        // the next step's clamp is skipped when an outlet cell (outside the
+                        // infiltrating soils) stays negative after the next rain
+                        // (Hydrological_Model.m:45-50); only outlet cells can end negative
+                        if (!(a.ga && (mt2[h] & 255u) != 255u) &&
+                            hn + s_rsn.at(a.rain, rm2, j[h], ny, nx) < R(-1e-11))
+                            neg_next = 1;
                     }
                     const R dm = dm2[h];
                     if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
@@ -508,9 +517,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     }
 
     // ---- CTA reductions ---------------------------------------------------------------
-    // every thread publishes its stores before the CTA takes its ticket, so the last
-    // CTA can read the new outlet depths
-    __threadfence();
+    // (the last CTA reads only the step accumulators, which thread 0 publishes before its
+    // ticket; the state records reach the next launch through the kernel boundary)
     rain_acc += double(rain_acc_r);
     inf_acc += double(inf_acc_r);
     out_acc += double(out_acc_r);
@@ -531,7 +539,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         red_d[2][warp_] = out_acc;
         red_to[warp_] = to_any;
     }
-    __syncthreads();
+    const int negn = __syncthreads_or(neg_next);
     if (tid == 0) {
         int to = 0;
         for (int w = 0; w < NT / 32; ++w) to |= red_to[w];
@@ -549,6 +557,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         if (rain_acc != 0.0) atomicAdd(&sc->acc_rain, rain_acc);
         if (inf_acc != 0.0) atomicAdd(&sc->acc_inf, inf_acc);
         if (out_acc != 0.0) atomicAdd(&sc->acc_out, out_acc);
+        if (negn) atomicOr(&sc->skip_next, 1);
         __threadfence();
         const unsigned int ticket = atomicAdd(&sc->counter, 1u);
         s_last = (ticket == a.n_ctas - 1);
@@ -609,24 +618,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->acc_inf = 0.0;
         sc->acc_out = 0.0;
         sc->counter = 0u;
-        s_rs.make(a.rain, sc->rain_a, sc->rain_b);   // the next step's rain
+        sc->skip_clamp = atomicExch(&sc->skip_next, 0);   // gathered by every CTA's outlets
     }
-    __syncthreads();
-    // skip flag of the next step's clamp: only outlet cells can hold a negative depth
-    // after a step (continuity clamps every other cell at zero).
-    int neg = 0;
-    if (a.n_outlets) {
-        const RainStep<R> RS2 = s_rs;
-        for (int o = tid; o < a.n_outlets; o += NT) {
-            const int c = a.outlet_cells[o];
-            if (a.ga && (meta_bits(a.stat[c].w) & 255u) != 255u) continue;
-            const int i = c / nx, j = c - (c / nx) * nx;
-            const R hv = __ldcg(&sout[c].x) + RS2.at(a.rain, i, j, ny, nx);
-            if (hv < R(-1e-11)) neg = 1;
-        }
-    }
-    neg = __syncthreads_or(neg);
-    if (tid == 0) a.sc->skip_clamp = neg;
     return cta_ok;
 }
 
