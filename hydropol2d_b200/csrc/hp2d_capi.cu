@@ -133,6 +133,12 @@ template <typename R> struct Impl : Base {
     Dev<R> hfx, hfy, qxu, qyu, scale;
     // forcing, clock
     Dev<double> rain_t, rain_r;
+    // inflow hydrographs
+    Dev<double> inf_t, inf_r, inf_cells;
+    Dev<R> inf_depth;
+    Dev<int32_t> inf_off, inf_gauge;
+    InflowDesc<R> inflow{};
+    std::vector<double> host_gcells;
     Dev<float> maps;
     RainDesc rain{};
     Dev<StepScalars> sc;
@@ -268,11 +274,12 @@ template <typename R> struct Impl : Base {
                               : std::sqrt(kG) / res;
             outs.emplace_back(int32_t(k), R(coef));
         }
-        if (size_t(outs.size()) >= (1u << 24)) { ctx->err = "too many outlet cells"; return HP2D_INVALID_ARG; }
+        if (size_t(outs.size()) >= (1u << 23)) { ctx->err = "too many outlet cells"; return HP2D_INVALID_ARG; }
         std::sort(outs.begin(), outs.end(), [](auto& x, auto& y) { return x.first < y.first; });
         outs.erase(std::unique(outs.begin(), outs.end(), [](auto& x, auto& y) { return x.first == y.first; }), outs.end());
         n_out = int(outs.size());
-        for (size_t k = 0; k < n; ++k) host_meta[k] &= 255u;
+        for (size_t k = 0; k < n; ++k) host_meta[k] &= 255u;   // outlets and inflow cells are set anew
+        inflow.n_gauges = 0;
         std::vector<int32_t> cells(n_out);
         std::vector<R> coefs(n_out);
         std::vector<uint32_t> bits(size_t(ny) * bit_words, 0u);
@@ -504,6 +511,71 @@ template <typename R> struct Impl : Base {
         return HP2D_OK;
     }
 
+    // Inflow hydrographs: gauge rates [n_times][n_gauges] on the start-stamped table t_start,
+    // (row, col, gauge) cells; replaces any earlier inflow (n_gauges = 0 removes it).
+    hp2d_status set_inflow(int32_t ng, int32_t nt, const double* t0, const double* rate, int32_t nc,
+                           const int32_t* rows, const int32_t* cols, const int32_t* gauge) {
+        if (!static_ready) { ctx->err = "hp2d_upload_static must come before hp2d_set_inflow"; return HP2D_NOT_READY; }
+        if (ng < 0 || (ng > 0 && (nt < 1 || nc < 1))) { ctx->err = "bad inflow table shape"; return HP2D_INVALID_ARG; }
+        std::vector<std::vector<int32_t>> per(n);
+        std::vector<size_t> used;
+        for (int q = 0; q < (ng ? nc : 0); ++q) {
+            if (rows[q] < 0 || rows[q] >= ny || cols[q] < 0 || cols[q] >= nx || gauge[q] < 0 || gauge[q] >= ng) {
+                ctx->err = "inflow cell or gauge out of range";
+                return HP2D_INVALID_ARG;
+            }
+            const size_t k = size_t(rows[q]) * nx + cols[q];
+            if (!(host_meta[k] & kInflowBit) && (host_meta[k] >> 8) != 0u) {
+                ctx->err = "an outlet cell cannot also be an inflow cell";
+                return HP2D_INVALID_ARG;
+            }
+            if (per[k].empty()) used.push_back(k);
+            per[k].push_back(gauge[q]);
+        }
+        if (used.size() >= (1u << 23)) { ctx->err = "too many inflow cells"; return HP2D_INVALID_ARG; }
+        for (size_t k = 0; k < n; ++k)
+            if (host_meta[k] & kInflowBit) host_meta[k] &= 255u;
+        std::sort(used.begin(), used.end());
+        std::vector<int32_t> off(1, 0), gl;
+        host_gcells.assign(size_t(ng), 0.0);
+        for (size_t e = 0; e < used.size(); ++e) {
+            const size_t k = used[e];
+            auto& v = per[k];
+            std::sort(v.begin(), v.end());   // a cell listed twice for a gauge gets it twice
+            for (int32_t g : v) {
+                gl.push_back(g);
+                if (std::isfinite(host_z[k])) host_gcells[size_t(g)] += 1.0;
+            }
+            off.push_back(int32_t(gl.size()));
+            host_meta[k] = (host_meta[k] & 255u) | kInflowBit | (uint32_t(e) << 8);
+        }
+        write_meta();
+        if (ng) {
+            inf_t.alloc(size_t(nt));
+            inf_r.alloc(size_t(nt) * ng);
+            inf_cells.alloc(size_t(ng));
+            inf_depth.alloc(size_t(ng));
+            inf_off.alloc(off.size());
+            inf_gauge.alloc(std::max<size_t>(gl.size(), 1));
+            upload(inf_t.p, std::vector<double>(t0, t0 + nt));
+            upload(inf_r.p, std::vector<double>(rate, rate + size_t(nt) * ng));
+            upload(inf_cells.p, host_gcells);
+            upload(inf_off.p, off);
+            if (!gl.empty()) upload(inf_gauge.p, gl);
+        }
+        inflow.n_gauges = ng;
+        inflow.n_times = nt;
+        inflow.t_start = inf_t.p;
+        inflow.rate = inf_r.p;
+        inflow.depth = inf_depth.p;
+        inflow.cell_off = inf_off.p;
+        inflow.cell_gauge = inf_gauge.p;
+        inflow.gauge_cells = inf_cells.p;
+        invalidate_graph();
+        dirty = true;
+        return HP2D_OK;
+    }
+
     void fold_accumulators() {
         pull_sc();
         double area = res * res;
@@ -545,14 +617,22 @@ template <typename R> struct Impl : Base {
         push_sc();
         unpack();
         double dts = time_step * 60.0;
+        if (inflow.n_gauges) {   // gauge depths of the current rain interval
+            k_inflow_depth<R><<<1, kThreads, 0, st()>>>(inflow, sc.p);
+            HP_CK(cudaGetLastError());
+        }
         k_hydro_rain_ga<R><<<blocks_for(n), kThreads, 0, st()>>>(view(), hs.rain_a, hs.rain_b, dts, rain, h.p, I.p, T.p, soil.p,
-                                                               classes.p, classes_vg.p, vgg, inf_mode(), sc.p);
+                                                               classes.p, classes_vg.p, vgg, inf_mode(), inflow,
+                                                               stat.p, sc.p);
         HP_CK(cudaGetLastError());
         k_hydro_clamp<R><<<blocks_for(n), kThreads, 0, st()>>>(n, h.p, sc.p);
         HP_CK(cudaGetLastError());
         pack();
+        std::vector<R> gd;
+        if (inflow.n_gauges) gd = fetch(inf_depth.p, size_t(inflow.n_gauges));
         pull_sc();
         if (hs.acc_neg) hs.neg_warn += 1;
+        for (size_t g = 0; g < gd.size(); ++g) hs.inflow_vol += double(gd[g]) * host_gcells[g] * res * res;
         push_sc();
         fold_accumulators();
         dirty = true;
@@ -651,45 +731,48 @@ template <typename R> struct Impl : Base {
         a.hf3 = hf3.p; a.qo = qo.p;
         a.arrival = arrival.p;
         a.rain = rain;
+        a.inflow = inflow;
         a.sc = sc.p;
         return a;
     }
 
     // kernels whose ring needs more than the default 48 KB of dynamic shared memory opt in
     // once per instantiation (before any graph capture: fused_steps and autotune call this)
-    template <int INF, bool MAP, int CPL> static void opt_in_smem() {
+    template <int INF, bool MAP, int CPL, bool INFL> static void opt_in_smem() {
         static bool done[8] = {};
         const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
         int dev = 0;
         HP_CK(cudaGetDevice(&dev));
         if (sm > 48 * 1024 && dev < 8 && !done[dev]) {
-            HP_CK(cudaFuncSetAttribute(k_fused_step<R, kThreads, INF, MAP, CPL>,
+            HP_CK(cudaFuncSetAttribute(k_fused_step<R, kThreads, INF, MAP, CPL, INFL>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
             done[dev] = true;
         }
     }
-    template <int CPL> void opt_in_t() {
-        opt_in_smem<0, false, CPL>(); opt_in_smem<0, true, CPL>();
-        opt_in_smem<1, false, CPL>(); opt_in_smem<1, true, CPL>();
-        opt_in_smem<2, false, CPL>(); opt_in_smem<2, true, CPL>();
+    template <int INF, int CPL> void opt_in_i() {
+        opt_in_smem<INF, false, CPL, false>(); opt_in_smem<INF, true, CPL, false>();
+        opt_in_smem<INF, false, CPL, true>(); opt_in_smem<INF, true, CPL, true>();
     }
+    template <int CPL> void opt_in_t() { opt_in_i<0, CPL>(); opt_in_i<1, CPL>(); opt_in_i<2, CPL>(); }
     void opt_in() { opt_in_t<1>(); opt_in_t<2>(); }
 
-    template <int INF, bool MAP, int CPL> void launch_one(const FusedArgs<R>& a) {
+    template <int INF, bool MAP, int CPL, bool INFL> void launch_one(const FusedArgs<R>& a) {
         const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
-        k_fused_step<R, kThreads, INF, MAP, CPL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+        k_fused_step<R, kThreads, INF, MAP, CPL, INFL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+    }
+    template <int INF, int CPL> void launch_i(const FusedArgs<R>& a) {
+        const bool map = rain.n_maps > 0, infl = inflow.n_gauges > 0;
+        if (map) {
+            if (infl) launch_one<INF, true, CPL, true>(a); else launch_one<INF, true, CPL, false>(a);
+        } else {
+            if (infl) launch_one<INF, false, CPL, true>(a); else launch_one<INF, false, CPL, false>(a);
+        }
     }
     template <int CPL> void launch_fused_t(const FusedArgs<R>& a) {
-        const bool map = rain.n_maps > 0;
         switch (inf_mode()) {
-            case 1:
-                if (map) launch_one<1, true, CPL>(a); else launch_one<1, false, CPL>(a);
-                break;
-            case 2:
-                if (map) launch_one<2, true, CPL>(a); else launch_one<2, false, CPL>(a);
-                break;
-            default:
-                if (map) launch_one<0, true, CPL>(a); else launch_one<0, false, CPL>(a);
+            case 1: launch_i<1, CPL>(a); break;
+            case 2: launch_i<2, CPL>(a); break;
+            default: launch_i<0, CPL>(a);
         }
     }
     void launch_fused(const FusedArgs<R>& a) {
@@ -715,6 +798,10 @@ template <typename R> struct Impl : Base {
         k_skip_flag<R><<<blocks_for(n), kThreads, 0, st()>>>(st4[hs.cur].p, stat.p, ny, nx, rain, ga() ? 1 : 0, res,
                                                            ctx->p.depth_tolerance, ctx->p.arrival_threshold, sc.p);
         HP_CK(cudaGetLastError());
+        if (inflow.n_gauges) {
+            k_inflow_depth<R><<<1, kThreads, 0, st()>>>(inflow, sc.p);
+            HP_CK(cudaGetLastError());
+        }
         dirty = false;
     }
 
@@ -989,6 +1076,7 @@ template <typename R> struct Impl : Base {
         o->rain_t0 = hs.rain_a;
         o->rain_t1 = hs.rain_b;
         o->t_previous = hs.t_prev;
+        o->inflow_volume = hs.inflow_vol;
         o->max_velocity = hs.vmax_last;
         o->rain_volume = hs.rain_vol;
         o->infiltration_volume = hs.inf_vol;
@@ -1049,9 +1137,12 @@ struct hp2d_ensemble {
     int rows_per_warp = 32;
     int cells_per_lane = 2;   // layout of the streamed strips (as hp2d_set_layout)
     int ga = -1, map = -1;
-    int grid_for[3] = {0, 0, 0};
+    bool infl = false;   // some member has inflow hydrographs
+    int grid_for[3][2] = {};
     cudaGraphExec_t graph = nullptr;
-    int graph_members = -1, graph_rpw = -1, graph_cpl = -1;
+    int graph_members = -1, graph_rpw = -1, graph_cpl = -1, graph_kind = -1;
+    // the kernel variant a captured graph launches
+    int kind() const { return ga * 4 + map * 2 + (infl ? 1 : 0); }
 
     Impl<float>& impl(int m) { return *static_cast<Impl<float>*>(members[m]->impl.get()); }
 
@@ -1060,27 +1151,31 @@ struct hp2d_ensemble {
         graph = nullptr;
     }
 
-    template <int INF, bool MAP, int CPL> void launch_t(int nm) {
+    template <int INF, bool MAP, int CPL, bool INFL> void launch_t(int nm) {
         const size_t smem = fused_smem_bytes<float, CPL>(kThreads);
-        int& grid = grid_for[CPL];
+        int& grid = grid_for[CPL][INFL ? 1 : 0];
         if (grid == 0) {
             int per_sm = 0, sms = 0;
-            HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_step<float, kThreads, INF, MAP, CPL>,
-                                                                kThreads, smem));
+            HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, k_ens_step<float, kThreads, INF, MAP, CPL, INFL>, kThreads, smem));
             HP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
             grid = std::max(1, per_sm) * sms;
         }
         k_ens_plan<float><<<1, 1024, 0, stream>>>(args.p, nm, prefix.p, queue.p);
-        k_ens_step<float, kThreads, INF, MAP, CPL><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p, queue.p);
+        k_ens_step<float, kThreads, INF, MAP, CPL, INFL><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p,
+                                                                                        queue.p);
+    }
+    template <int INF, int CPL> void launch_m(int nm) {
+        if (map) {
+            if (infl) launch_t<INF, true, CPL, true>(nm); else launch_t<INF, true, CPL, false>(nm);
+        } else {
+            if (infl) launch_t<INF, false, CPL, true>(nm); else launch_t<INF, false, CPL, false>(nm);
+        }
     }
     template <int CPL> void launch_c(int nm) {
-        if (ga == 1) {
-            if (map) launch_t<1, true, CPL>(nm); else launch_t<1, false, CPL>(nm);
-        } else if (ga == 2) {
-            if (map) launch_t<2, true, CPL>(nm); else launch_t<2, false, CPL>(nm);
-        } else {
-            if (map) launch_t<0, true, CPL>(nm); else launch_t<0, false, CPL>(nm);
-        }
+        if (ga == 1) launch_m<1, CPL>(nm);
+        else if (ga == 2) launch_m<2, CPL>(nm);
+        else launch_m<0, CPL>(nm);
     }
     void launch(int nm) {
         if (cells_per_lane == 2) launch_c<2>(nm);
@@ -1100,7 +1195,8 @@ struct hp2d_ensemble {
                 return HP2D_NOT_READY;
             }
             const int mga = im.inf_mode(), mmap = im.rain.n_maps > 0 ? 1 : 0;
-            if (m == 0) { ga = mga; map = mmap; }
+            if (m == 0) { ga = mga; map = mmap; infl = false; }
+            if (im.inflow.n_gauges > 0) infl = true;
             if (mga != ga || mmap != map) {
                 err = "members must agree on the infiltration model and on the kind of rain forcing";
                 return HP2D_INVALID_ARG;
@@ -1130,7 +1226,8 @@ struct hp2d_ensemble {
 
     // the CUDA graph of kChunk launches for the current members and launch shape
     void ensure_graph(int nm) {
-        if (graph && (graph_members != nm || graph_rpw != rows_per_warp || graph_cpl != cells_per_lane)) drop_graph();
+        if (graph && (graph_members != nm || graph_rpw != rows_per_warp || graph_cpl != cells_per_lane ||
+                      graph_kind != kind())) drop_graph();
         if (graph) return;
         cudaGraph_t gr;
         HP_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -1141,6 +1238,7 @@ struct hp2d_ensemble {
         graph_members = nm;
         graph_rpw = rows_per_warp;
         graph_cpl = cells_per_lane;
+        graph_kind = kind();
     }
 
     // `after` (optional) is recorded once the launches and the plan pass are queued, before
@@ -1359,6 +1457,13 @@ hp2d_status hp2d_set_clock(hp2d_ctx* ctx, double t, double time_step, int64_t k)
 hp2d_status hp2d_set_rain_uniform(hp2d_ctx* ctx, int32_t n, const double* t_start, const double* rate) {
     if (n < 0 || (n > 0 && (!t_start || !rate))) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.set_rain_uniform(n, t_start, rate); });
+}
+
+hp2d_status hp2d_set_inflow(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, const double* t_start,
+                            const double* rates, int32_t n_cells, const int32_t* rows, const int32_t* cols,
+                            const int32_t* gauge) {
+    if (n_gauges > 0 && (!t_start || !rates || !rows || !cols || !gauge)) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) { return m.set_inflow(n_gauges, n_times, t_start, rates, n_cells, rows, cols, gauge); });
 }
 
 hp2d_status hp2d_set_rain_clock(hp2d_ctx* ctx, double rain_t0, double rain_t1, double t_previous) {

@@ -147,6 +147,7 @@ struct StepScalars {
     double rain_a, rain_b, t_prev;
     int skip_next;         // fused step: some outlet cell ends below -1e-11 m after the next rain
     int pad2;
+    double inflow_vol;     // cumulative inflow-hydrograph volume [m^3]
 };
 
 // non-negative floats/doubles order like their bit patterns
@@ -289,6 +290,47 @@ __device__ __host__ inline double uniform_integral(const RainDesc& rd, double a,
 
 template <typename R>
 __device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i, int j, int ny, int nx);
+
+// ---------------- inflow hydrographs (flag_inflow, update_spatial_BC.m:359-395) ----------
+// Gauge g's rate [mm/h] holds from t_start[q] up to t_start[q+1] (the last for ever); a
+// step adds to every cell of the gauge the integral over the step's rain interval / 60
+// [mm] (delta_inflow_agg x inflow_cells), after the infiltration (Hydrological_Model.m:27-28).
+// Inflow cells carry kInflowBit in their meta word and, in bits 8..30, their entry e: the
+// cell's gauges are cell_gauge[cell_off[e] .. cell_off[e+1]) in increasing order.
+constexpr unsigned kInflowBit = 0x80000000u;
+template <typename R> struct InflowDesc {
+    int n_gauges, n_times;
+    const double* t_start;      // [n_times] [min]
+    const double* rate;         // [n_times][n_gauges] [mm/h]
+    R* depth;                   // [n_gauges] this step's depth [m]
+    const int32_t* cell_off;    // [entries + 1]
+    const int32_t* cell_gauge;
+    const double* gauge_cells;  // [n_gauges] cells of the gauge with a finite elevation
+};
+template <typename R>
+__device__ __host__ inline double inflow_integral(const InflowDesc<R>& d, int g, double a, double b) {
+    double acc = 0.0;
+    if (!(b > a)) return acc;
+    for (int q = 0; q < d.n_times; ++q) {
+        const double lo = d.t_start[q];
+        const double hi = q + 1 < d.n_times ? d.t_start[q + 1] : b;
+        const double ov = fmax(0.0, fmin(b, hi) - fmax(a, lo));
+        const double r = d.rate[size_t(q) * d.n_gauges + g];
+        if (ov > 0.0 && isfinite(r)) acc += r * ov;
+    }
+    return acc;
+}
+// inflow depth [m] of the cell with meta word `meta` (0 when it is no inflow cell)
+template <typename R> __device__ __forceinline__ R inflow_at(const InflowDesc<R>& d, unsigned meta) {
+    R v = R(0);
+    if (meta & kInflowBit) {
+        const unsigned e = (meta >> 8) & 0x7FFFFFu;
+        for (int q = d.cell_off[e]; q < d.cell_off[e + 1]; ++q) v = v + d.depth[d.cell_gauge[q]];
+    }
+    return v;
+}
+// outlet entry + 1 of a meta word (0: not an outlet)
+__device__ __host__ inline unsigned outlet_ord(unsigned meta) { return (meta & kInflowBit) ? 0u : meta >> 8; }
 
 // Rain of one step over the clock interval [a, b] [min]: a uniform depth, or the (at most
 // two) rate maps overlapping the interval with their overlaps (map m holds over

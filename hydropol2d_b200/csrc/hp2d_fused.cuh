@@ -78,6 +78,7 @@ template <typename R> struct FusedArgs {
     R* hf3; R* qo;
     R* arrival;
     RainDesc rain;
+    InflowDesc<R> inflow;
     StepScalars* sc;
 };
 
@@ -160,8 +161,9 @@ template <int CPL> struct FusedOcc<double, CPL> { static constexpr int minb = CP
 // them together.  Returns false when a row copy timed out (the CTA must stop using its
 // shared-memory ring).
 // INF: infiltration model (0 none, 1 Green-Ampt, 2 van Genuchten); MAP: rain from coarse
-// maps (else a uniform rate)
-template <typename R, int NT, int INF, bool MAP, int CPL = 1>
+// maps (else a uniform rate); INFL: inflow hydrographs present (the grids without them do not
+// carry the lookup)
+template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>
 __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned blk) {
     using V4 = typename Vec<R>::V4;
     using V2 = typename Vec<R>::V2;
@@ -169,6 +171,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     __shared__ StepConsts<R> s_K;
     __shared__ double s_tmin, s_dts;
     __shared__ int s_cur, s_skip, s_done, s_last;
+    __shared__ int s_negn;   // an outlet cell would go below -1e-11 m after the next rain
     __shared__ RainStep<R> s_rs, s_rsn;   // this step's rain and the next one's
     __shared__ R red_s2[NT / 32];
     __shared__ unsigned long long red_c[NT / 32];
@@ -185,6 +188,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         s_dts = sc->time_step * 60.0;
         s_cur = sc->cur;
         s_skip = sc->skip_clamp;
+        s_negn = 0;
         s_done = !(s_tmin <= a.t_end);
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
         s_rs.make(a.rain, sc->rain_a, sc->rain_b);
@@ -214,7 +218,6 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     double rain_acc = 0.0, inf_acc = 0.0, out_acc = 0.0;
     R rain_acc_r = R(0), inf_acc_r = R(0), out_acc_r = R(0);   // per-lane partial sums (ledger only)
     unsigned dry = 0u;                        // bit i: row r-i dry across the strip
-    int neg_next = 0;                         // an outlet cell would go below -1e-11 m after the next rain
     R s2max = R(0);
     R cmaxv = R(-1);   // largest celerity term of a non-stagnant cell (-1: none yet)
 
@@ -349,6 +352,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         }
                         if (own) gout[c] = go;
                     }
+                    // inflow hydrographs after the infiltration (Hydrological_Model.m:27-28)
+                    if (INFL && (meta[h] & kInflowBit)) hh = hh + inflow_at(a.inflow, meta[h]);
                     if (!skip && hh < R(1e-9)) hh = R(0);
                     if (hh < R(0)) hh = R(0);
                     hT0[h] = hh;
@@ -448,7 +453,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     const size_t c2 = size_t(rm2) * nx + j[h];
                     R hn = quiet ? hT2[h] + R(0) : continuity(hT2[h], qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
                     R hf3 = R(0);
-                    const unsigned ord = mt2[h] >> 8;
+                    const unsigned ord = outlet_ord(mt2[h]);
                     if (ord) {
                         const int o = int(ord) - 1;
                         R ho;
@@ -462,7 +467,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         // (Hydrological_Model.m:45-50); only outlet cells can end negative
                         if (!(a.ga && (mt2[h] & 255u) != 255u) &&
                             hn + s_rsn.at(a.rain, rm2, j[h], ny, nx) < R(-1e-11))
-                            neg_next = 1;
+                            s_negn = 1;   // rare: kept in shared memory, not a register
                     }
                     const R dm = dm2[h];
                     if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
@@ -539,7 +544,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         red_d[2][warp_] = out_acc;
         red_to[warp_] = to_any;
     }
-    const int negn = __syncthreads_or(neg_next);
+    __syncthreads();
+    const int negn = s_negn;
     if (tid == 0) {
         int to = 0;
         for (int w = 0; w < NT / 32; ++w) to |= red_to[w];
@@ -602,6 +608,11 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->rain_vol += rain_s * area;
         sc->inf_vol += inf_s * area;
         sc->out_vol += out_s * area;
+        if (a.inflow.n_gauges) {   // every cell of a gauge with a finite elevation got its depth
+            double v = 0.0;
+            for (int g = 0; g < a.inflow.n_gauges; ++g) v += double(a.inflow.depth[g]) * a.inflow.gauge_cells[g];
+            sc->inflow_vol += v * area;
+        }
         // the next step's rain: update_spatial_BC over [t_previous, t]
         // (HydroPol2D_Main_While.m:721), then t_previous <- the clock increment on the first
         // step and t after it (:734-738), and the clock advances by the new step (:779)
@@ -620,12 +631,25 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->counter = 0u;
         sc->skip_clamp = atomicExch(&sc->skip_next, 0);   // gathered by every CTA's outlets
     }
+    if (a.inflow.n_gauges) {   // the next step's gauge depths over its rain interval
+        __syncthreads();
+        const double ra = a.sc->rain_a, rb = a.sc->rain_b;
+        for (int g = tid; g < a.inflow.n_gauges; g += NT)
+            a.inflow.depth[g] = R(inflow_integral(a.inflow, g, ra, rb) / 60000.0);
+    }
     return cta_ok;
 }
 
-template <typename R, int NT, int INF, bool MAP, int CPL = 1>
+// gauge depths of the current rain interval (after a host change of the inflow or clock)
+template <typename R> __global__ void k_inflow_depth(InflowDesc<R> d, const StepScalars* sc) {
+    const double ra = sc->rain_a, rb = sc->rain_b;
+    for (int g = threadIdx.x; g < d.n_gauges; g += blockDim.x)
+        d.depth[g] = R(inflow_integral(d, g, ra, rb) / 60000.0);
+}
+
+template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>
 __global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb) k_fused_step(const FusedArgs<R> a) {
-    fused_item<R, NT, INF, MAP, CPL>(a, blockIdx.x);
+    fused_item<R, NT, INF, MAP, CPL, INFL>(a, blockIdx.x);
 }
 
 // ---- batched ensemble ----------------------------------------------------------------
@@ -684,7 +708,7 @@ __global__ void k_ens_plan(const FusedArgs<R>* __restrict__ members, int n_membe
     }
 }
 
-template <typename R, int NT, int INF, bool MAP, int CPL = 1>
+template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>
 __global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb)
 k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsigned* __restrict__ prefix,
            EnsQueue* q) {
@@ -718,7 +742,7 @@ k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsign
             for (int w = tid; w < int(sizeof(FusedArgs<R>) / 4); w += NT) dst[w] = src[w];
         }
         __syncthreads();
-        if (!fused_item<R, NT, INF, MAP, CPL>(s_a, s_local)) return;   // ring unusable after a timeout
+        if (!fused_item<R, NT, INF, MAP, CPL, INFL>(s_a, s_local)) return;   // ring unusable after a timeout
     }
 }
 

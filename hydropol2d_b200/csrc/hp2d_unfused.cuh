@@ -19,7 +19,8 @@ template <typename R> struct GridView {
 template <typename R>
 __global__ void k_hydro_rain_ga(GridView<R> g, double rain_a, double rain_b, double dt_s, RainDesc rain, R* h, R* I, R* T,
                                 const uint8_t* soil, const SoilClass<R>* classes, const SoilClassVG<R>* classes_vg,
-                                VGGlobals<R> vg, int inf, StepScalars* sc) {
+                                VGGlobals<R> vg, int inf, InflowDesc<R> inflow, const typename Vec<R>::V4* stat,
+                                StepScalars* sc) {
     StepConsts<R> K;
     K.make(dt_s, g.res, g.tol_mm, g.thr_mm);
     RainStep<R> RS;
@@ -40,6 +41,7 @@ __global__ void k_hydro_rain_ga(GridView<R> g, double rain_a, double rain_b, dou
             T[c] = Tc;
             if (isfinite(fd)) iacc += double(fd);
         }
+        if (inflow.n_gauges) hh = hh + inflow_at(inflow, meta_bits(stat[c].w));   // Hydrological_Model.m:27-28
         if (hh < R(-1e-11)) neg = 1;
         h[c] = hh;
     }

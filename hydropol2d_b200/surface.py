@@ -124,6 +124,20 @@ class SurfaceFlow:
         [min] (``diag`` reports them), for an exact restart."""
         self._check(self._L.hp2d_set_rain_clock(self._h, float(rain_t0), float(rain_t1), float(t_previous)))
 
+    def set_inflow(self, t_start, rates, rows, cols, gauge):
+        """Inflow hydrographs: ``rates`` (n_times, n_gauges) [mm/h] on the start-stamped
+        ``t_start`` [min]; cells ``rows``/``cols`` of gauge ``gauge`` (Wshed_Properties.inflow_cells).
+        After ``upload_static``; ``rates`` with no gauges removes the inflow."""
+        t = _f64(t_start).ravel()
+        r = np.ascontiguousarray(np.asarray(rates, dtype=np.float64).reshape(t.size, -1))
+        ng = r.shape[1]
+        rr = np.ascontiguousarray(rows, dtype=np.int32).ravel()
+        cc = np.ascontiguousarray(cols, dtype=np.int32).ravel()
+        gg = np.ascontiguousarray(gauge, dtype=np.int32).ravel()
+        ip = C.POINTER(C.c_int32)
+        self._check(self._L.hp2d_set_inflow(self._h, int(ng), int(t.size), _dp(t), _dp(r), int(rr.size),
+                                            rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
+
     def set_rain_uniform(self, t_start, rate):
         t = _f64(t_start).ravel()
         r = _f64(rate).ravel()

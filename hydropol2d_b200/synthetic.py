@@ -38,6 +38,7 @@ class Case:
     soil: dict | None = None                # set_soil kwargs
     I0: np.ndarray | None = None            # mm
     meta: dict = field(default_factory=dict)
+    inflow: dict | None = None              # set_inflow kwargs (t_start, rates, rows, cols, gauge)
 
     @property
     def shape(self):
@@ -53,6 +54,8 @@ class Case:
             sf.set_rain_uniform(*self.rain_uniform)
         if self.rain_maps is not None:
             sf.set_rain_maps(self.rain_maps, self.rain_map_dt)
+        if self.inflow is not None:
+            sf.set_inflow(**self.inflow)
         return sf
 
 
@@ -128,6 +131,36 @@ def vtilt_case(ny: int = 200, nx: int = 200, dx: float = 10.0) -> Case:
                   min_time_step=0.01, max_time_step=10.0)
     return Case("vtilt_200x200_dx10", z, np.full((ny, nx), 0.02), dx, rows, ch.astype(np.int32), params,
                 np.zeros((ny, nx)), rain_uniform=(np.array([0.0, 30.0]), np.array([100.0, 0.0])))
+
+
+def inflow_hydrograph_rates(q_m3s: np.ndarray, n_cells: int, dx: float) -> np.ndarray:
+    """Discharge [m^3/s] spread over a gauge's cells as a depth rate [mm/h], the reference's
+    conversion (Analytical_Catchments.m:118)."""
+    return np.asarray(q_m3s, dtype=np.float64) / (n_cells * dx * dx) * 1000.0 * 3600.0
+
+
+def inflow_case(ny: int = 96, nx: int = 96, dx: float = 10.0, minutes: float = 40.0, peak_m3s: float = 4.0) -> Case:
+    """The V-tilted catchment, dry and without rain, fed by two inflow hydrographs: gauge 0
+    on the channel's upstream cells (a triangular flood, 0 -> peak at 10 min -> 0 at 30 min,
+    1-min steps) and gauge 1 on a block of cells of the left plane (a constant 0.2 m^3/s from
+    minute 5).  Outlets on the channel's downstream end (row 0)."""
+    z, ch = vtilt_domain(ny, nx, dx, 0.005, 0.002)
+    rows = np.zeros(ch.size, dtype=np.int32)
+    params = dict(routing_time=minutes, alfa_min=0.7, alfa_max=0.7, outlet_type=1, slope_outlet=0.002,
+                  min_time_step=0.01, max_time_step=10.0)
+    t = np.arange(0.0, 31.0)                      # start of each 1-min interval [min]
+    q0 = np.interp(t + 0.5, [0.0, 10.0, 30.0], [0.0, peak_m3s, 0.0])
+    q0[-1] = 0.0
+    g0_r = np.full(ch.size, ny - 1, dtype=np.int32)
+    g0_c = ch.astype(np.int32)
+    br, bc = np.meshgrid(np.arange(ny // 2, ny // 2 + 3), np.arange(nx // 6, nx // 6 + 3), indexing="ij")
+    g1_r, g1_c = br.ravel().astype(np.int32), bc.ravel().astype(np.int32)
+    q1 = np.where(t >= 5.0, 0.2, 0.0)
+    rates = np.stack([inflow_hydrograph_rates(q0, g0_r.size, dx), inflow_hydrograph_rates(q1, g1_r.size, dx)], axis=1)
+    inflow = dict(t_start=t, rates=rates, rows=np.concatenate([g0_r, g1_r]), cols=np.concatenate([g0_c, g1_c]),
+                  gauge=np.concatenate([np.zeros(g0_r.size, np.int32), np.ones(g1_r.size, np.int32)]))
+    return Case(f"inflow_vtilt_{ny}x{nx}", z, np.full((ny, nx), 0.03), dx, rows, ch.astype(np.int32), params,
+                np.zeros((ny, nx)), inflow=inflow)
 
 
 def urban_case(n: int = 2048, dx: float = 2.0, seed: int = 7, hours: float = 2.0) -> Case:

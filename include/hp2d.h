@@ -109,6 +109,7 @@ typedef struct hp2d_diag {
     int64_t status_bits;          /* bit 0: non-finite state seen */
     double rain_t0, rain_t1;      /* clock interval whose rain the next step applies [min] */
     double t_previous;            /* the loop's t_previous [min] */
+    double inflow_volume;         /* cumulative inflow-hydrograph volume [m^3] */
 } hp2d_diag;
 
 typedef struct hp2d_ctx hp2d_ctx;
@@ -185,6 +186,18 @@ hp2d_status hp2d_set_rain_uniform(hp2d_ctx* ctx, int32_t n, const double* t_star
                                   const double* rate);
 hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx,
                                const float* rate, double map_dt);
+
+/* Inflow hydrographs (flags.flag_inflow = 1; update_spatial_BC.m:359-395): n_gauges rate
+ * series [mm/h] (rates row-major [n_times][n_gauges]) on the start-stamped table t_start
+ * [min] (rate q holds from t_start[q] up to t_start[q+1], the last for ever), and the
+ * n_cells (rows, cols, gauge) entries of Wshed_Properties.inflow_cells(:,:,gauge) (a cell may
+ * belong to several gauges).  Each step adds to a cell, after the infiltration
+ * (Hydrological_Model.m:27-28), the integral of its gauges' rates over the step's rain
+ * interval / 60 mm (BC_States.inflow).  Call after hp2d_upload_static (which removes the
+ * inflow); an outlet cell cannot be an inflow cell; n_gauges = 0 removes the inflow. */
+hp2d_status hp2d_set_inflow(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, const double* t_start,
+                            const double* rates, int32_t n_cells, const int32_t* rows, const int32_t* cols,
+                            const int32_t* gauge);
 
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
 /* Hydrological_Model for this path: adds delta_p_agg (the rain of the current rain

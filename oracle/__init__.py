@@ -63,6 +63,8 @@ def _load():
             "oracle_set_depth": ([vp, dp], C.c_int),
             "oracle_set_clock": ([vp, C.c_double, C.c_double, C.c_int64], C.c_int),
             "oracle_set_rain_clock": ([vp, C.c_double, C.c_double, C.c_double], C.c_int),
+            "oracle_set_inflow": ([vp, C.c_int32, C.c_int32, dp, dp, C.c_int32, P(C.c_int32), P(C.c_int32),
+                                   P(C.c_int32), dp], C.c_int),
             "oracle_set_rain_uniform": ([vp, C.c_int32, dp, dp], C.c_int),
             "oracle_set_rain_maps": ([vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_float), C.c_double], C.c_int),
             "oracle_hydrology_step": ([vp, C.c_double], C.c_int),
@@ -118,6 +120,7 @@ class KernelFormOracle:
                                      cols.ctypes.data_as(C.POINTER(C.c_int32)), int(rows.size),
                                      None if sl is None else _dp(sl))
         self.n_outlets = len(set(zip(rows.tolist(), cols.tolist())))
+        self._z = z   # the inflow volume ledger counts gauge cells with a finite elevation
 
     def set_soil(self, soil_class, ksat, psi, dtheta, Lu, k_out, Tr, min_soil_moisture):
         cls = np.ascontiguousarray(soil_class, dtype=np.uint8).reshape(self.ny, self.nx)
@@ -139,6 +142,17 @@ class KernelFormOracle:
 
     def set_clock(self, t, time_step, k=1):
         self._L.oracle_set_clock(self._h, float(t), float(time_step), int(k))
+
+    def set_inflow(self, t_start, rates, rows, cols, gauge):
+        t = np.ascontiguousarray(t_start, dtype=np.float64).ravel()
+        r = np.ascontiguousarray(np.asarray(rates, dtype=np.float64).reshape(t.size, -1))
+        rr = np.ascontiguousarray(rows, dtype=np.int32).ravel()
+        cc = np.ascontiguousarray(cols, dtype=np.int32).ravel()
+        gg = np.ascontiguousarray(gauge, dtype=np.int32).ravel()
+        ip = C.POINTER(C.c_int32)
+        self._L.oracle_set_inflow(self._h, int(r.shape[1]), int(t.size), _dp(t), _dp(r), int(rr.size),
+                                  rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip),
+                                  _dp(self._z))
 
     def set_rain_clock(self, rain_t0, rain_t1, t_previous):
         self._L.oracle_set_rain_clock(self._h, float(rain_t0), float(rain_t1), float(t_previous))

@@ -350,10 +350,67 @@ public:
         return r;
     }
 
+    // ---------------- inflow hydrographs (update_spatial_BC.m:359-395) ----------------
+    // gauge g's rate holds from inf_t[q] up to inf_t[q+1] (the last for ever); a cell of the
+    // gauge receives the integral over the step's rain interval / 60 mm after the
+    // infiltration (Hydrological_Model.m:27-28); cells of several gauges sum them in
+    // increasing gauge order
+    int inf_ng = 0, inf_nt = 0;
+    std::vector<double> inf_t, inf_r, inf_gcells;
+    std::vector<int32_t> inf_entry, inf_off, inf_gauge;
+    std::vector<R> inf_depth;
+    double inflow_vol = 0;
+
+    void set_inflow(int ng, int nt, const double* t0, const double* rate, int nc, const int32_t* rows,
+                    const int32_t* cols, const int32_t* gauge, const double* z) {
+        const size_t n = size_t(ny) * nx;
+        inf_ng = ng; inf_nt = nt;
+        inf_t.assign(t0, t0 + (ng ? nt : 0));
+        inf_r.assign(rate, rate + (ng ? size_t(nt) * ng : 0));
+        inf_entry.assign(n, -1);
+        inf_off.assign(1, 0);
+        inf_gauge.clear();
+        inf_gcells.assign(size_t(ng), 0.0);
+        inf_depth.assign(size_t(ng), R(0));
+        std::vector<std::vector<int32_t>> per(n);
+        for (int q = 0; q < (ng ? nc : 0); ++q) per[at(rows[q], cols[q])].push_back(gauge[q]);
+        for (size_t c = 0; c < n; ++c) {
+            if (per[c].empty()) continue;
+            std::sort(per[c].begin(), per[c].end());
+            inf_entry[c] = int32_t(inf_off.size() - 1);
+            for (int32_t g : per[c]) {
+                inf_gauge.push_back(g);
+                if (std::isfinite(z[c])) inf_gcells[size_t(g)] += 1.0;
+            }
+            inf_off.push_back(int32_t(inf_gauge.size()));
+        }
+    }
+    void inflow_depths(double a, double b) {
+        for (int g = 0; g < inf_ng; ++g) {
+            double acc = 0.0;
+            if (b > a) {
+                for (int q = 0; q < inf_nt; ++q) {
+                    const double lo = inf_t[q];
+                    const double hi = q + 1 < inf_nt ? inf_t[q + 1] : b;
+                    const double ov = std::fmax(0.0, std::fmin(b, hi) - std::fmax(a, lo));
+                    const double r = inf_r[size_t(q) * inf_ng + g];
+                    if (ov > 0.0 && std::isfinite(r)) acc += r * ov;
+                }
+            }
+            inf_depth[g] = R(acc / 60000.0);
+        }
+    }
+
     // ---------------- hydrology: rain + Green-Ampt + clamp ----------------
     void hydrology(double dts) {
         Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
         const StepRain SR = step_rain(rain_a, rain_b);
+        if (inf_ng) {
+            inflow_depths(rain_a, rain_b);
+            double v = 0.0;
+            for (int g = 0; g < inf_ng; ++g) v += double(inf_depth[g]) * inf_gcells[g];
+            inflow_vol += v * res * res;
+        }
         size_t n = size_t(ny) * nx;
         double rv = 0, iv = 0;
         const bool ga = p.flag_infiltration == 1 && !soil.empty();
@@ -385,6 +442,12 @@ public:
                     hh = hh - fd;
                     if (hh < R(0)) hh = R(0);
                     if (std::isfinite(double(fd))) iv += double(fd);
+                }
+                if (inf_ng && inf_entry[c] >= 0) {   // BC_States.inflow is summed over gauges first
+                    const int e = inf_entry[c];
+                    R v = R(0);
+                    for (int q = inf_off[e]; q < inf_off[e + 1]; ++q) v = v + inf_depth[inf_gauge[q]];
+                    hh = hh + v;
                 }
                 h[c] = hh;
             }

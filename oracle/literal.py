@@ -469,6 +469,11 @@ class RunConfig:
     rain_map_dt_min: float = 5.0
     ga: GAParams | None = None
     I0: np.ndarray | None = None                # mm
+    # inflow hydrographs: start-stamped times [min], rates (n_times, n_gauges) [mm/h] and
+    # Wshed_Properties.inflow_cells as (n_gauges, ny, nx) 0/1 masks
+    inflow_times_min: np.ndarray | None = None
+    inflow_rates_mmh: np.ndarray | None = None
+    inflow_cells: np.ndarray | None = None
     fixed_time_step_s: float | None = None      # bypass refreshing_timestep
 
 
@@ -557,6 +562,27 @@ def rain_depth_mm(cfg: RunConfig, t0: float, t1: float, ny: int, nx: int):
     return acc / 60.0
 
 
+def inflow_depth_mm(cfg: RunConfig, t0: float, t1: float) -> np.ndarray:
+    """BC_States.inflow [mm] of update_spatial_BC.m:359-395: per gauge z the exact integral of
+    its rate over [t0, t1] / 60 (delta_inflow_agg), spread over inflow_cells(:,:,z) and summed
+    over gauges; NaN on idx_nan cells."""
+    masks = np.asarray(cfg.inflow_cells, dtype=np.float64)
+    times = np.asarray(cfg.inflow_times_min, dtype=np.float64)
+    rates = np.asarray(cfg.inflow_rates_mmh, dtype=np.float64).reshape(times.size, -1)
+    out = np.zeros(masks.shape[1:])
+    if t1 > t0:
+        for z in range(masks.shape[0]):
+            acc = 0.0
+            for q in range(times.size):
+                hi = times[q + 1] if q + 1 < times.size else np.inf
+                ov = max(0.0, min(t1, hi) - max(t0, times[q]))
+                if ov > 0 and np.isfinite(rates[q, z]):
+                    acc += rates[q, z] * ov
+            out = out + acc / 60.0 * masks[z]
+    out[np.isnan(cfg.z)] = np.nan
+    return out
+
+
 def next_rain_interval(a: float, b: float, t_previous: float, t: float, k: int, tcr_s: float):
     """The loop's bookkeeping of the rain interval.  At the end of iteration k (clock t, the
     end of step k) update_spatial_BC computes the depth the NEXT step applies over
@@ -583,6 +609,7 @@ class RunState:
     rain_volume: float = 0.0
     infiltration_volume: float = 0.0
     outlet_volume: float = 0.0
+    inflow_volume: float = 0.0
     # rain interval [rain_a, rain_b] of the current step and the loop's t_previous [min]; the
     # first step's comes from the call before the loop (HydroPol2D_Main_While.m:115) with
     # t_previous = 0 (:120)
@@ -619,6 +646,10 @@ def step(cfg: RunConfig, st: RunState) -> None:
     if cfg.ga is not None:
         d_t, st.I, st.T, f = green_ampt_infiltration(d_t, st.I, st.T, time_step, cfg.ga, res)
         st.infiltration_volume += float(np.nansum(f * (time_step / 60))) * A / 1000
+    if cfg.inflow_cells is not None:   # Hydrological_Model.m:27-28, after the infiltration
+        inflow = inflow_depth_mm(cfg, st.rain_a, st.rain_b)
+        d_t = d_t + inflow
+        st.inflow_volume += float(np.nansum(inflow)) * A / 1000
     if np.nanmin(d_t) < -1e-8:
         st.neg_warnings += 1
     else:

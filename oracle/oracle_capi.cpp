@@ -64,6 +64,14 @@ int oracle_set_clock(oracle_model* m, double t, double time_step, int64_t k) {
     });
 }
 
+int oracle_set_inflow(oracle_model* m, int32_t ng, int32_t nt, const double* t0, const double* rate, int32_t nc,
+                      const int32_t* rows, const int32_t* cols, const int32_t* gauge, const double* z) {
+    return dispatch(m, [&](auto& M) {
+        M.set_inflow(ng, nt, t0, rate, nc, rows, cols, gauge, z);
+        return 0;
+    });
+}
+
 int oracle_set_rain_clock(oracle_model* m, double a, double b, double t_previous) {
     return dispatch(m, [&](auto& M) {
         M.rain_a = a;
@@ -189,6 +197,7 @@ int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
         o->rain_t0 = M.rain_a;
         o->rain_t1 = M.rain_b;
         o->t_previous = M.t_prev;
+        o->inflow_volume = M.inflow_vol;
         return 0;
     });
 }

@@ -28,6 +28,12 @@ def literal_cfg(case):
         kw["ga"] = L.GAParams(ksat=s["ksat"][c], psi=s["psi"][c], dtheta=s["dtheta"][c], Lu=s["Lu"][c],
                               k_out=s["k_out"][c], Tr=s["Tr"][c], min_sm=s["min_soil_moisture"][c], active=act)
         kw["I0"] = case.I0
+    if case.inflow is not None:
+        f = case.inflow
+        masks = np.zeros((np.asarray(f["rates"]).reshape(len(f["t_start"]), -1).shape[1],) + case.shape)
+        for r, c, g in zip(f["rows"], f["cols"], f["gauge"]):
+            masks[g, r, c] += 1.0
+        kw["inflow_times_min"], kw["inflow_rates_mmh"], kw["inflow_cells"] = f["t_start"], f["rates"], masks
     return L.RunConfig(**kw)
 
 
