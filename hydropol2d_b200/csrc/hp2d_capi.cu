@@ -139,6 +139,10 @@ template <typename R> struct Impl : Base {
     Dev<int32_t> inf_off, inf_gauge;
     InflowDesc<R> inflow{};
     std::vector<double> host_gcells;
+    // map records
+    Dev<double> rec_times, rec_t;
+    Dev<R> rec_snap;
+    RecordDesc<R> rec{};
     Dev<float> maps;
     RainDesc rain{};
     Dev<StepScalars> sc;
@@ -576,6 +580,63 @@ template <typename R> struct Impl : Base {
         return HP2D_OK;
     }
 
+    // Map records at the reference's record times (save_output_maps.m): n_slots depth maps
+    // kept on the device, the oldest overwritten first; n_times = 0 switches them off.
+    hp2d_status set_map_records(int32_t nt, const double* times, int32_t nslots) {
+        if (nt < 0 || (nt > 0 && (!times || nslots < 1))) { ctx->err = "bad map record table"; return HP2D_INVALID_ARG; }
+        for (int q = 1; q < nt; ++q)
+            if (!(times[q] > times[q - 1])) { ctx->err = "record times must increase"; return HP2D_INVALID_ARG; }
+        rec = RecordDesc<R>{};
+        if (nt > 0) {
+            rec_times.alloc(size_t(nt));
+            upload(rec_times.p, std::vector<double>(times, times + nt));
+            rec_snap.alloc(size_t(nslots) * n);
+            rec_t.alloc(size_t(nslots));
+            rec = RecordDesc<R>{nt, nslots, rec_times.p, rec_snap.p, rec_t.p};
+        }
+        pull_sc();
+        hs.rec_count = 0;
+        hs.rec_pending = 0;
+        hs.rec_last = nt > 0 ? last_record_below(times, nt, hs.t_min) : 0;
+        push_sc();
+        invalidate_graph();
+        dirty = true;
+        return HP2D_OK;
+    }
+    // a record whose step had no successor copies the current depth now (hs pulled)
+    void flush_records() {
+        if (!rec.n_slots || !hs.rec_pending) return;
+        const int64_t slot = hs.rec_count % rec.n_slots;
+        k_record_depth<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, rec.snap + size_t(slot) * n);
+        HP_CK(cudaGetLastError());
+        hs.rec_count += 1;
+        hs.rec_pending = 0;
+        push_sc();
+    }
+    hp2d_status map_records(int64_t* count) {
+        pull_sc();
+        flush_records();
+        *count = hs.rec_count;
+        return HP2D_OK;
+    }
+    hp2d_status download_map_record(int64_t index, double* depth_mm, double* t_min) {
+        pull_sc();
+        flush_records();
+        if (!rec.n_slots || index < 0 || index >= hs.rec_count || index < hs.rec_count - rec.n_slots) {
+            ctx->err = "map record not held (never taken or overwritten)";
+            return HP2D_INVALID_ARG;
+        }
+        const size_t slot = size_t(index % rec.n_slots);
+        auto v = fetch(rec.snap + slot * n, n);
+        for (size_t k = 0; k < n; ++k) depth_mm[k] = double(v[k]) * 1000.0;
+        if (t_min) {
+            double t = 0;
+            HP_CK(cudaMemcpy(&t, rec.snap_t + slot, sizeof(double), cudaMemcpyDeviceToHost));
+            *t_min = t;
+        }
+        return HP2D_OK;
+    }
+
     void fold_accumulators() {
         pull_sc();
         double area = res * res;
@@ -732,6 +793,7 @@ template <typename R> struct Impl : Base {
         a.arrival = arrival.p;
         a.rain = rain;
         a.inflow = inflow;
+        a.rec = rec;
         a.sc = sc.p;
         return a;
     }
@@ -838,6 +900,7 @@ template <typename R> struct Impl : Base {
         HP_CK(cudaGetLastError());
         if (after) HP_CK(cudaEventRecord(after, st()));
         pull_sc();
+        flush_records();
         if (hs.status & 2u) {
             ctx->err = "a row copy into shared memory did not complete within its wait limit";
             return HP2D_TIMEOUT;
@@ -1263,7 +1326,10 @@ struct hp2d_ensemble {
         EnsQueue q{};
         HP_CK(cudaMemcpyAsync(&q, queue.p, sizeof(q), cudaMemcpyDeviceToHost, stream));
         HP_CK(cudaStreamSynchronize(stream));
-        for (int m = 0; m < nm; ++m) impl(m).pull_sc();
+        for (int m = 0; m < nm; ++m) {
+            impl(m).pull_sc();
+            impl(m).flush_records();
+        }
         if (n_active) *n_active = int32_t(q.n_active);
         if (q.stalled) {
             err = std::to_string(q.stalled) + " member(s) stopped: a row copy did not complete within its wait limit";
@@ -1464,6 +1530,20 @@ hp2d_status hp2d_set_inflow(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, co
                             const int32_t* gauge) {
     if (n_gauges > 0 && (!t_start || !rates || !rows || !cols || !gauge)) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.set_inflow(n_gauges, n_times, t_start, rates, n_cells, rows, cols, gauge); });
+}
+
+hp2d_status hp2d_set_map_records(hp2d_ctx* ctx, int32_t n_times, const double* time_records, int32_t n_slots) {
+    return with_impl(ctx, [&](auto& m) { return m.set_map_records(n_times, time_records, n_slots); });
+}
+
+hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count) {
+    if (!count) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) { return m.map_records(count); });
+}
+
+hp2d_status hp2d_download_map_record(hp2d_ctx* ctx, int64_t index, double* depth_mm, double* t_min) {
+    if (!depth_mm) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) { return m.download_map_record(index, depth_mm, t_min); });
 }
 
 hp2d_status hp2d_set_rain_clock(hp2d_ctx* ctx, double rain_t0, double rain_t1, double t_previous) {

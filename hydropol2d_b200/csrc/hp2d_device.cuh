@@ -148,7 +148,31 @@ struct StepScalars {
     int skip_next;         // fused step: some outlet cell ends below -1e-11 m after the next rain
     int pad2;
     double inflow_vol;     // cumulative inflow-hydrograph volume [m^3]
+    // map records (save_output_maps.m:25-27, :160-166): index of the last record time below
+    // t_save, records taken, and whether the next step's input depth is to be recorded
+    long long rec_count;
+    int rec_last, rec_pending;
 };
+
+// ---------------- map records (save_output_maps.m) -----------------------------------
+// After a step whose t_save = t + new dt passes a record time (time_records, 0-based index
+// above rec_last), the depth d_t after that step is kept in slot rec_count % n_slots (the next
+// step copies its input depth there, or the host when no step follows).
+template <typename R> struct RecordDesc {
+    int n_times, n_slots;
+    const double* times;   // [n_times] [min], increasing
+    R* snap;               // [n_slots][ny*nx] depth [m]
+    double* snap_t;        // [n_slots] clock t of the step whose result the slot holds [min]
+};
+// last index i with times[i] < t (-1 when none)
+__device__ __host__ inline int last_record_below(const double* times, int n, double t) {
+    int lo = 0, hi = n;   // first index with times[i] >= t, by bisection
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (times[mid] < t) lo = mid + 1; else hi = mid;
+    }
+    return lo - 1;
+}
 
 // non-negative floats/doubles order like their bit patterns
 __device__ __forceinline__ unsigned long long ord_bits(float v) { return (unsigned long long)__float_as_uint(v); }

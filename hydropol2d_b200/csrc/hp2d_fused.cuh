@@ -79,6 +79,7 @@ template <typename R> struct FusedArgs {
     R* arrival;
     RainDesc rain;
     InflowDesc<R> inflow;
+    RecordDesc<R> rec;
     StepScalars* sc;
 };
 
@@ -172,6 +173,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     __shared__ double s_tmin, s_dts;
     __shared__ int s_cur, s_skip, s_done, s_last;
     __shared__ int s_negn;   // an outlet cell would go below -1e-11 m after the next rain
+    __shared__ int s_rec;    // slot that receives this step's input depth (-1: none)
     __shared__ RainStep<R> s_rs, s_rsn;   // this step's rain and the next one's
     __shared__ R red_s2[NT / 32];
     __shared__ unsigned long long red_c[NT / 32];
@@ -189,6 +191,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         s_cur = sc->cur;
         s_skip = sc->skip_clamp;
         s_negn = 0;
+        s_rec = (sc->rec_pending && a.rec.n_slots > 0) ? int(sc->rec_count % a.rec.n_slots) : -1;
         s_done = !(s_tmin <= a.t_end);
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
         s_rs.make(a.rain, sc->rain_a, sc->rain_b);
@@ -333,6 +336,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 if (col_ok[h] && rok) {
                     const size_t c = size_t(r) * nx + j[h];
                     R hh = X[h].x;
+                    // a pending map record keeps the depth this step starts from
+                    if (s_rec >= 0 && own_lane[h] && own_row) a.rec.snap[size_t(s_rec) * (size_t(ny) * nx) + c] = hh;
                     const R rr = MAP ? RS.at(a.rain, r, j[h], ny, nx) : RS.depth;
                     hh = hh + rr;
                     const bool own = own_lane[h] && own_row;
@@ -619,6 +624,15 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->rain_a = sc->t_prev;
         sc->rain_b = t;
         sc->t_prev = sc->k == 1 ? tcr / 60.0 : t;
+        if (a.rec.n_times > 0) {   // save_output_maps.m:25-27 with t_save = t + new dt (:740)
+            if (sc->rec_pending) { sc->rec_count += 1; sc->rec_pending = 0; }   // recorded by this step
+            const int idx = last_record_below(a.rec.times, a.rec.n_times, t + tcr / 60.0);
+            if (idx > sc->rec_last && a.rec.n_slots > 0) {
+                sc->rec_pending = 1;
+                a.rec.snap_t[sc->rec_count % a.rec.n_slots] = t;
+            }
+            if (idx > sc->rec_last) sc->rec_last = idx;
+        }
         sc->time_step = tcr / 60.0;
         sc->t_min = tcr / 60.0 + t;
         sc->k += 1;
@@ -638,6 +652,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             a.inflow.depth[g] = R(inflow_integral(a.inflow, g, ra, rb) / 60000.0);
     }
     return cta_ok;
+}
+
+// a map record taken by the host when no step follows the one that triggered it
+template <typename R> __global__ void k_record_depth(size_t n, const typename Vec<R>::V4* st, R* dst) {
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x)
+        dst[c] = st[c].x;
 }
 
 // gauge depths of the current rain interval (after a host change of the inflow or clock)

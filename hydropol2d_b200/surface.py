@@ -138,6 +138,24 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_inflow(self._h, int(ng), int(t.size), _dp(t), _dp(r), int(rr.size),
                                             rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
 
+    def set_map_records(self, time_records, n_slots: int):
+        """Keep the depth map after each step that passes a record time [min]
+        (save_output_maps); ``n_slots`` maps are held on the device."""
+        t = _f64(time_records).ravel()
+        self._check(self._L.hp2d_set_map_records(self._h, int(t.size), _dp(t), int(n_slots)))
+
+    def map_records(self) -> int:
+        c = C.c_int64()
+        self._check(self._L.hp2d_map_records(self._h, C.byref(c)))
+        return c.value
+
+    def download_map_record(self, index: int):
+        """(depth [mm] as (ny, nx), clock [min]) of record ``index``."""
+        out = np.empty((self.ny, self.nx), dtype=np.float64)
+        t = C.c_double()
+        self._check(self._L.hp2d_download_map_record(self._h, int(index), _dp(out), C.byref(t)))
+        return out, t.value
+
     def set_rain_uniform(self, t_start, rate):
         t = _f64(t_start).ravel()
         r = _f64(rate).ravel()

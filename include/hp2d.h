@@ -199,6 +199,18 @@ hp2d_status hp2d_set_inflow(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, co
                             const double* rates, int32_t n_cells, const int32_t* rows, const int32_t* cols,
                             const int32_t* gauge);
 
+/* Map records (save_output_maps.m:25-27, :160-166): after a step whose t_save = t + the new
+ * step (HydroPol2D_Main_While.m:740) passes one or more of the record times
+ * (running_control.time_records [min], increasing), the depth d_t after that step is kept on
+ * the device with the step's clock t; n_slots maps are held, the oldest overwritten first.
+ * The first-step map the reference writes before any record event is overwritten by the first
+ * event there and is not kept here.  n_times = 0 switches the records off. */
+hp2d_status hp2d_set_map_records(hp2d_ctx* ctx, int32_t n_times, const double* time_records, int32_t n_slots);
+/* Records taken so far. */
+hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count);
+/* Record `index` (0-based, one of the last n_slots taken): depth [mm] (ny*nx) and clock [min]. */
+hp2d_status hp2d_download_map_record(hp2d_ctx* ctx, int64_t index, double* depth_mm, double* t_min);
+
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
 /* Hydrological_Model for this path: adds delta_p_agg (the rain of the current rain
  * interval, see hp2d_set_rain_uniform),

@@ -63,6 +63,9 @@ def _load():
             "oracle_set_depth": ([vp, dp], C.c_int),
             "oracle_set_clock": ([vp, C.c_double, C.c_double, C.c_int64], C.c_int),
             "oracle_set_rain_clock": ([vp, C.c_double, C.c_double, C.c_double], C.c_int),
+            "oracle_set_map_records": ([vp, C.c_int32, dp], C.c_int),
+            "oracle_map_records": ([vp], C.c_int64),
+            "oracle_download_map_record": ([vp, C.c_int64, dp, dp], C.c_int),
             "oracle_set_inflow": ([vp, C.c_int32, C.c_int32, dp, dp, C.c_int32, P(C.c_int32), P(C.c_int32),
                                    P(C.c_int32), dp], C.c_int),
             "oracle_set_rain_uniform": ([vp, C.c_int32, dp, dp], C.c_int),
@@ -153,6 +156,20 @@ class KernelFormOracle:
         self._L.oracle_set_inflow(self._h, int(r.shape[1]), int(t.size), _dp(t), _dp(r), int(rr.size),
                                   rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip),
                                   _dp(self._z))
+
+    def set_map_records(self, time_records, n_slots=None):
+        t = np.ascontiguousarray(time_records, dtype=np.float64).ravel()
+        self._L.oracle_set_map_records(self._h, int(t.size), _dp(t))
+
+    def map_records(self):
+        return int(self._L.oracle_map_records(self._h))
+
+    def download_map_record(self, index):
+        out = np.empty((self.ny, self.nx), dtype=np.float64)
+        t = C.c_double()
+        if self._L.oracle_download_map_record(self._h, int(index), _dp(out), C.byref(t)) != 0:
+            raise IndexError(index)
+        return out, t.value
 
     def set_rain_clock(self, rain_t0, rain_t1, t_previous):
         self._L.oracle_set_rain_clock(self._h, float(rain_t0), float(rain_t1), float(t_previous))

@@ -659,6 +659,26 @@ public:
         }
     }
 
+    // ---------------- map records (save_output_maps.m:25-27, :160-166) ----------------
+    // after a step whose t_save = t + new dt passes a record time (index above rec_last),
+    // the depth after the step is kept with the step's clock
+    std::vector<double> rec_times;
+    int rec_last = 0;
+    std::vector<std::vector<R>> rec_maps;
+    std::vector<double> rec_t;
+    void set_map_records(int nt, const double* times) {
+        rec_times.assign(times, times + nt);
+        rec_maps.clear();
+        rec_t.clear();
+        rec_last = nt > 0 ? last_below(t_min) : 0;
+    }
+    int last_below(double t) const {   // last index with rec_times[i] < t, -1 if none
+        int idx = -1;
+        for (size_t i = 0; i < rec_times.size(); ++i)
+            if (rec_times[i] < t) idx = int(i);
+        return idx;
+    }
+
     // ---------------- one accepted step (HydroPol2D_Main_While.m:403-782) ----------------
     // The step is carried in minutes, as the reference does (time_step, min), and the
     // seconds of the step are time_step*60 (Local_Inertial_Model_D4.m:201).
@@ -678,6 +698,14 @@ public:
             if (tcr == p.min_time_step) ++unstable;
         }
         track(t_min * 60.0 + dts);
+        if (!rec_times.empty()) {
+            const int idx = last_below(t_min + tcr / 60.0);
+            if (idx > rec_last) {
+                rec_maps.push_back(h);
+                rec_t.push_back(t_min);
+                rec_last = idx;
+            }
+        }
         // the next step's rain interval: [t_previous, t] (HydroPol2D_Main_While.m:721), then
         // t_previous <- the increment on the first step, t after it (:734-738)
         rain_a = t_prev;

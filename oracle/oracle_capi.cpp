@@ -72,6 +72,25 @@ int oracle_set_inflow(oracle_model* m, int32_t ng, int32_t nt, const double* t0,
     });
 }
 
+int oracle_set_map_records(oracle_model* m, int32_t n, const double* times) {
+    return dispatch(m, [&](auto& M) { M.set_map_records(n, times); return 0; });
+}
+
+int64_t oracle_map_records(oracle_model* m) {
+    return dispatch(m, [&](auto& M) { return int64_t(M.rec_maps.size()); });
+}
+
+// record `index`: depth [mm] as the library converts it (state precision -> double x 1000)
+int oracle_download_map_record(oracle_model* m, int64_t index, double* depth_mm, double* t_min) {
+    return dispatch(m, [&](auto& M) {
+        if (index < 0 || size_t(index) >= M.rec_maps.size()) return 1;
+        const auto& v = M.rec_maps[size_t(index)];
+        for (size_t k = 0; k < v.size(); ++k) depth_mm[k] = double(v[k]) * 1000.0;
+        *t_min = M.rec_t[size_t(index)];
+        return 0;
+    });
+}
+
 int oracle_set_rain_clock(oracle_model* m, double a, double b, double t_previous) {
     return dispatch(m, [&](auto& M) {
         M.rain_a = a;
