@@ -388,10 +388,13 @@ template <typename R> struct RainStep {
         if (!rd.n_maps) return depth;
         if (nm == 0) return R(0);
         R r = w[0] * map_rate<R>(rd, rd.maps + size_t(m[0]) * rd.my * rd.mx, i, j, ny, nx);
-        if (nm > 1) r = r + w[1] * map_rate<R>(rd, rd.maps + size_t(m[1]) * rd.my * rd.mx, i, j, ny, nx);
+#pragma unroll 1
+        for (int q = 1; q < nm; ++q)   // a step across a map boundary (one sampler in the code)
+            r = r + w[q] * map_rate<R>(rd, rd.maps + size_t(m[q]) * rd.my * rd.mx, i, j, ny, nx);
         return r;
     }
 };
+
 
 template <typename R>
 __device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i, int j, int ny, int nx) {

@@ -338,7 +338,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     R hh = X[h].x;
                     // a pending map record keeps the depth this step starts from
                     if (s_rec >= 0 && own_lane[h] && own_row) a.rec.snap[size_t(s_rec) * (size_t(ny) * nx) + c] = hh;
-                    const R rr = MAP ? RS.at(a.rain, r, j[h], ny, nx) : RS.depth;
+                    // map weights are read from shared memory where they are used
+                    const R rr = MAP ? s_rs.at(a.rain, r, j[h], ny, nx) : RS.depth;
                     hh = hh + rr;
                     const bool own = own_lane[h] && own_row;
                     // uniform rain volume comes from the count of finite cells at the end
@@ -471,7 +472,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         // infiltrating soils) stays negative after the next rain
                         // (Hydrological_Model.m:45-50); only outlet cells can end negative
                         if (!(a.ga && (mt2[h] & 255u) != 255u) &&
-                            hn + s_rsn.at(a.rain, rm2, j[h], ny, nx) < R(-1e-11))
+                            hn + (MAP ? s_rsn.at(a.rain, rm2, j[h], ny, nx) : s_rsn.depth) < R(-1e-11))
                             s_negn = 1;   // rare: kept in shared memory, not a register
                     }
                     const R dm = dm2[h];
