@@ -515,6 +515,31 @@ template <typename R> struct Impl : Base {
         return HP2D_OK;
     }
 
+    // Rain gauges: one IDW map per record interval of dt minutes, computed on the device and
+    // used as full-resolution rain maps
+    hp2d_status set_rain_gauges(int32_t ng, const double* xg, const double* yg, int32_t nt, double dt,
+                                const double* rate, double x_ul, double y_ul) {
+        if (ng <= 0 || nt <= 0 || !(dt > 0)) { ctx->err = "bad rain gauge table"; return HP2D_INVALID_ARG; }
+        if (dt * 60.0 < ctx->p.max_time_step) {
+            ctx->err = "rain record interval shorter than max_time_step";
+            return HP2D_INVALID_ARG;
+        }
+        Dev<double> dx, dy, dr;
+        dx.alloc(size_t(ng)); dy.alloc(size_t(ng)); dr.alloc(size_t(nt) * ng);
+        upload(dx.p, std::vector<double>(xg, xg + ng));
+        upload(dy.p, std::vector<double>(yg, yg + ng));
+        upload(dr.p, std::vector<double>(rate, rate + size_t(nt) * ng));
+        maps.alloc(size_t(nt) * n);
+        k_idw_maps<<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, res, x_ul, y_ul, ng, dx.p, dy.p, nt, dr.p, maps.p);
+        HP_CK(cudaGetLastError());
+        HP_CK(cudaStreamSynchronize(st()));
+        rain.n_maps = nt; rain.my = ny; rain.mx = nx; rain.map_dt = dt; rain.maps = maps.p;
+        rain.n_uniform = 0;
+        invalidate_graph();
+        dirty = true;
+        return HP2D_OK;
+    }
+
     // Inflow hydrographs: gauge rates [n_times][n_gauges] on the start-stamped table t_start,
     // (row, col, gauge) cells; replaces any earlier inflow (n_gauges = 0 removes it).
     hp2d_status set_inflow(int32_t ng, int32_t nt, const double* t0, const double* rate, int32_t nc,
@@ -1544,6 +1569,14 @@ hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count) {
 hp2d_status hp2d_download_map_record(hp2d_ctx* ctx, int64_t index, double* depth_mm, double* t_min) {
     if (!depth_mm) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.download_map_record(index, depth_mm, t_min); });
+}
+
+hp2d_status hp2d_set_rain_gauges(hp2d_ctx* ctx, int32_t n_gauges, const double* x_gauge, const double* y_gauge,
+                                 int32_t n_times, double record_dt, const double* rates, double x_ul, double y_ul) {
+    if (!x_gauge || !y_gauge || !rates) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) {
+        return m.set_rain_gauges(n_gauges, x_gauge, y_gauge, n_times, record_dt, rates, x_ul, y_ul);
+    });
 }
 
 hp2d_status hp2d_set_rain_clock(hp2d_ctx* ctx, double rain_t0, double rain_t1, double t_previous) {

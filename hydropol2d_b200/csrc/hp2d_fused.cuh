@@ -655,6 +655,35 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     return cta_ok;
 }
 
+// Rain maps from gauges by inverse-distance weighting, one full-resolution map per record
+// interval (Rainfall_Interpolator.m / idw_function.m with p = 2, the Euclidean norm and no
+// radius): cell (i, j) sits at (x_ul + res (j+1), y_ul - res (i+1))
+// (HydroPol2D_preprocessing.m:2420-2421); distance d = sqrt(dx^2 + dy^2), 0 -> eps, weight
+// 1/d^2; gauges whose record is NaN are left out of that interval's map, and an interval
+// without any gauge is dry.  Sums run over the gauges in order, in FP64.
+static __global__ void k_idw_maps(int ny, int nx, double res, double x_ul, double y_ul, int ng, const double* xg,
+                           const double* yg, int nt, const double* rate, float* maps) {
+    const size_t n = size_t(ny) * nx;
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(c / nx), j = int(c % nx);
+        const double X = x_ul + res * double(j + 1), Y = y_ul - res * double(i + 1);
+        for (int m = 0; m < nt; ++m) {
+            double num = 0.0, den = 0.0;
+            for (int g = 0; g < ng; ++g) {
+                const double r = rate[size_t(m) * ng + g];
+                if (isnan(r)) continue;
+                const double dx = fabs(X - xg[g]), dy = fabs(Y - yg[g]);
+                double d = sqrt(dx * dx + dy * dy);
+                if (d == 0.0) d = 2.220446049250313e-16;
+                const double w = 1.0 / (d * d);
+                num = num + w * r;
+                den = den + w;
+            }
+            maps[size_t(m) * n + c] = den > 0.0 ? float(num / den) : 0.0f;
+        }
+    }
+}
+
 // a map record taken by the host when no step follows the one that triggered it
 template <typename R> __global__ void k_record_depth(size_t n, const typename Vec<R>::V4* st, R* dst) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x)

@@ -138,6 +138,15 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_inflow(self._h, int(ng), int(t.size), _dp(t), _dp(r), int(rr.size),
                                             rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
 
+    def set_rain_gauges(self, x_gauge, y_gauge, rates, record_dt: float, x_ul: float = 0.0, y_ul: float = 0.0):
+        """Rain from gauges: ``rates`` (n_times, n_gauges) [mm/h] (NaN: no record) over intervals
+        of ``record_dt`` minutes, interpolated by inverse-distance weighting to every cell."""
+        x = _f64(x_gauge).ravel()
+        y = _f64(y_gauge).ravel()
+        r = np.ascontiguousarray(np.asarray(rates, dtype=np.float64).reshape(-1, x.size))
+        self._check(self._L.hp2d_set_rain_gauges(self._h, int(x.size), _dp(x), _dp(y), int(r.shape[0]),
+                                                 float(record_dt), _dp(r), float(x_ul), float(y_ul)))
+
     def set_map_records(self, time_records, n_slots: int):
         """Keep the depth map after each step that passes a record time [min]
         (save_output_maps); ``n_slots`` maps are held on the device."""

@@ -187,6 +187,16 @@ hp2d_status hp2d_set_rain_uniform(hp2d_ctx* ctx, int32_t n, const double* t_star
 hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx,
                                const float* rate, double map_dt);
 
+/* Rain from gauges (flags.flag_spatial_rainfall = 1; update_spatial_BC.m:494-517 with
+ * Rainfall_Interpolator.m / idw_function.m): n_gauges at eastings/northings x_gauge, y_gauge
+ * [m] record rates [mm/h] (row-major [n_times][n_gauges], NaN = no record) over intervals of
+ * record_dt minutes, interval m over [m, m+1) * record_dt.  The library interpolates one map
+ * per interval by inverse-distance weighting (power 2, Euclidean distance, no radius) at the
+ * cell centres (x_ul + res (j+1), y_ul - res (i+1)) (HydroPol2D_preprocessing.m:2420-2421) and
+ * uses them as rain maps (hp2d_set_rain_maps semantics; record_dt*60 >= max_time_step). */
+hp2d_status hp2d_set_rain_gauges(hp2d_ctx* ctx, int32_t n_gauges, const double* x_gauge, const double* y_gauge,
+                                 int32_t n_times, double record_dt, const double* rates, double x_ul, double y_ul);
+
 /* Inflow hydrographs (flags.flag_inflow = 1; update_spatial_BC.m:359-395): n_gauges rate
  * series [mm/h] (rates row-major [n_times][n_gauges]) on the start-stamped table t_start
  * [min] (rate q holds from t_start[q] up to t_start[q+1], the last for ever), and the

@@ -530,6 +530,38 @@ def average_rate_over_step(times_end, values, t0: float, t1: float) -> float:
     return acc / (t1 - t0)
 
 
+def idw_rain_maps(x_gauge, y_gauge, rates, ny: int, nx: int, res: float, x_ul: float = 0.0,
+                  y_ul: float = 0.0) -> np.ndarray:
+    """Rainfall_Interpolator.m + idw_function.m (p = 2, Euclidean norm, no radius) for every
+    record interval: (n_times, ny, nx) float32 maps [mm/h].  Cell (i, j) at
+    (x_ul + res (j+1), y_ul - res (i+1)) (HydroPol2D_preprocessing.m:2420-2421); gauges with a
+    NaN record are left out of that interval (update_spatial_BC.m:875-885), an interval without
+    gauges is dry; the distance's square root and the gauge sums in order, in FP64."""
+    xg = np.asarray(x_gauge, dtype=np.float64)
+    yg = np.asarray(y_gauge, dtype=np.float64)
+    r = np.asarray(rates, dtype=np.float64).reshape(-1, xg.size)
+    X = x_ul + res * (np.arange(nx, dtype=np.float64) + 1.0)[None, :]
+    Y = y_ul - res * (np.arange(ny, dtype=np.float64) + 1.0)[:, None]
+    out = np.zeros((r.shape[0], ny, nx), dtype=np.float32)
+    w = []
+    for g in range(xg.size):
+        dx = np.abs(X - xg[g])
+        dy = np.abs(Y - yg[g])
+        d = np.sqrt(dx * dx + dy * dy)
+        d[d == 0] = np.finfo(np.float64).eps
+        w.append(1.0 / (d * d))
+    for m in range(r.shape[0]):
+        num = np.zeros((ny, nx))
+        den = np.zeros((ny, nx))
+        for g in range(xg.size):
+            if np.isnan(r[m, g]):
+                continue
+            num = num + w[g] * r[m, g]
+            den = den + w[g]
+        out[m] = np.where(den > 0, num / np.where(den > 0, den, 1.0), 0.0).astype(np.float32)
+    return out
+
+
 def rain_depth_mm(cfg: RunConfig, t0: float, t1: float, ny: int, nx: int):
     """Rain depth [mm] a step receives from the clock interval [t0, t1] [min]: the exact
     integral of the piecewise-constant rate over the interval / 60, which is what

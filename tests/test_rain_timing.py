@@ -148,3 +148,21 @@ def test_oracle_set_clock_follows_the_loop(oracle_lib):
     d = o.diag()
     assert (d["rain_t0"], d["rain_t1"], d["t_previous"]) == (1.0, 2.0, 3.0)
     assert math.isfinite(d["t"])
+
+
+def test_idw_gauge_maps():
+    """Rainfall_Interpolator / idw_function restated: a cell centred on a gauge takes its value
+    (its weight is 1/eps^2), equal gauges give a uniform map, a NaN record drops the gauge for
+    that interval, an interval without records is dry."""
+    ny, nx, res = 12, 16, 10.0
+    xg = np.array([res * 3, res * 10, res * 15])          # cell centres of columns 2, 9, 14
+    yg = np.array([-res * 2, -res * 7, -res * 11])        # rows 1, 6, 10
+    rates = np.array([[10.0, 40.0, 70.0], [25.0, 25.0, 25.0], [np.nan, 40.0, 70.0], [np.nan] * 3])
+    maps = L.idw_rain_maps(xg, yg, rates, ny, nx, res)
+    assert maps.shape == (4, ny, nx) and maps.dtype == np.float32
+    assert maps[0, 1, 2] == np.float32(10.0) and maps[0, 6, 9] == np.float32(40.0)
+    assert np.all((maps[0] >= 10.0) & (maps[0] <= 70.0))
+    assert np.allclose(maps[1], 25.0, rtol=1e-6)
+    no0 = L.idw_rain_maps(xg[1:], yg[1:], rates[2:3, 1:], ny, nx, res)
+    assert np.array_equal(maps[2], no0[0])
+    assert np.all(maps[3] == 0.0)
