@@ -284,6 +284,9 @@ template <typename R> struct Impl : Base {
         n_out = int(outs.size());
         for (size_t k = 0; k < n; ++k) host_meta[k] &= 255u;   // outlets and inflow cells are set anew
         inflow.n_gauges = 0;
+        inflow.n_stage = 0;
+        inflow_cells_h = BcCells{};
+        stage_cells_h = BcCells{};
         std::vector<int32_t> cells(n_out);
         std::vector<R> coefs(n_out);
         std::vector<uint32_t> bits(size_t(ny) * bit_words, 0u);
@@ -540,32 +543,56 @@ template <typename R> struct Impl : Base {
         return HP2D_OK;
     }
 
-    // Inflow hydrographs: gauge rates [n_times][n_gauges] on the start-stamped table t_start,
-    // (row, col, gauge) cells; replaces any earlier inflow (n_gauges = 0 removes it).
-    hp2d_status set_inflow(int32_t ng, int32_t nt, const double* t0, const double* rate, int32_t nc,
-                           const int32_t* rows, const int32_t* cols, const int32_t* gauge) {
-        if (!static_ready) { ctx->err = "hp2d_upload_static must come before hp2d_set_inflow"; return HP2D_NOT_READY; }
-        if (ng < 0 || (ng > 0 && (nt < 1 || nc < 1))) { ctx->err = "bad inflow table shape"; return HP2D_INVALID_ARG; }
-        std::vector<std::vector<int32_t>> per(n);
-        std::vector<size_t> used;
+    // Boundary-condition cells: inflow hydrographs and stage hydrographs share one entry table
+    // (meta bit 31 + entry); each setter keeps its cell list and rebuilds the table.
+    struct BcCells { std::vector<size_t> cell; std::vector<int32_t> gauge; };
+    BcCells inflow_cells_h, stage_cells_h;
+    Dev<double> stage_t, stage_d;
+    Dev<R> stage_now;
+    Dev<int32_t> bc_stage;
+
+    hp2d_status check_bc_cells(int32_t ng, int32_t nc, const int32_t* rows, const int32_t* cols,
+                               const int32_t* gauge, BcCells& out, const char* what) {
+        out.cell.clear();
+        out.gauge.clear();
         for (int q = 0; q < (ng ? nc : 0); ++q) {
             if (rows[q] < 0 || rows[q] >= ny || cols[q] < 0 || cols[q] >= nx || gauge[q] < 0 || gauge[q] >= ng) {
-                ctx->err = "inflow cell or gauge out of range";
+                ctx->err = std::string(what) + " cell or gauge out of range";
                 return HP2D_INVALID_ARG;
             }
             const size_t k = size_t(rows[q]) * nx + cols[q];
             if (!(host_meta[k] & kInflowBit) && (host_meta[k] >> 8) != 0u) {
-                ctx->err = "an outlet cell cannot also be an inflow cell";
+                ctx->err = std::string("an outlet cell cannot also be an ") + what + " cell";
                 return HP2D_INVALID_ARG;
             }
-            if (per[k].empty()) used.push_back(k);
-            per[k].push_back(gauge[q]);
+            out.cell.push_back(k);
+            out.gauge.push_back(gauge[q]);
         }
-        if (used.size() >= (1u << 23)) { ctx->err = "too many inflow cells"; return HP2D_INVALID_ARG; }
+        return HP2D_OK;
+    }
+
+    void rebuild_bc_cells() {
+        const int ng = inflow.n_gauges;
+        std::vector<std::vector<int32_t>> per(n);
+        std::vector<int32_t> stg(n, -1);
+        std::vector<size_t> used;
+        auto mark = [&](size_t k) {
+            if (per[k].empty() && stg[k] < 0) used.push_back(k);
+        };
+        for (size_t q = 0; q < inflow_cells_h.cell.size(); ++q) {
+            mark(inflow_cells_h.cell[q]);
+            per[inflow_cells_h.cell[q]].push_back(inflow_cells_h.gauge[q]);
+        }
+        for (size_t q = 0; q < stage_cells_h.cell.size(); ++q) {   // the reference overwrites in
+            const size_t k = stage_cells_h.cell[q];                  // gauge order: the last wins
+            if (per[k].empty() && stg[k] < 0) used.push_back(k);
+            stg[k] = std::max(stg[k], stage_cells_h.gauge[q]);
+        }
         for (size_t k = 0; k < n; ++k)
             if (host_meta[k] & kInflowBit) host_meta[k] &= 255u;
         std::sort(used.begin(), used.end());
-        std::vector<int32_t> off(1, 0), gl;
+        used.erase(std::unique(used.begin(), used.end()), used.end());
+        std::vector<int32_t> off(1, 0), gl, st;
         host_gcells.assign(size_t(ng), 0.0);
         for (size_t e = 0; e < used.size(); ++e) {
             const size_t k = used[e];
@@ -576,32 +603,87 @@ template <typename R> struct Impl : Base {
                 if (std::isfinite(host_z[k])) host_gcells[size_t(g)] += 1.0;
             }
             off.push_back(int32_t(gl.size()));
+            st.push_back(stg[k]);
             host_meta[k] = (host_meta[k] & 255u) | kInflowBit | (uint32_t(e) << 8);
         }
         write_meta();
+        inf_off.alloc(off.size());
+        inf_gauge.alloc(std::max<size_t>(gl.size(), 1));
+        bc_stage.alloc(std::max<size_t>(st.size(), 1));
+        upload(inf_off.p, off);
+        if (!gl.empty()) upload(inf_gauge.p, gl);
+        if (!st.empty()) upload(bc_stage.p, st);
+        if (ng) {
+            inf_cells.alloc(size_t(ng));
+            upload(inf_cells.p, host_gcells);
+        }
+        inflow.cell_off = inf_off.p;
+        inflow.cell_gauge = inf_gauge.p;
+        inflow.cell_stage = bc_stage.p;
+        inflow.gauge_cells = inf_cells.p;
+        invalidate_graph();
+        dirty = true;
+    }
+
+    // Inflow hydrographs: gauge rates [n_times][n_gauges] on the start-stamped table t_start,
+    // (row, col, gauge) cells; replaces any earlier inflow (n_gauges = 0 removes it).
+    hp2d_status set_inflow(int32_t ng, int32_t nt, const double* t0, const double* rate, int32_t nc,
+                           const int32_t* rows, const int32_t* cols, const int32_t* gauge) {
+        if (!static_ready) { ctx->err = "hp2d_upload_static must come before hp2d_set_inflow"; return HP2D_NOT_READY; }
+        if (ng < 0 || (ng > 0 && (nt < 1 || nc < 1))) { ctx->err = "bad inflow table shape"; return HP2D_INVALID_ARG; }
+        BcCells cells;
+        hp2d_status s = check_bc_cells(ng, nc, rows, cols, gauge, cells, "inflow");
+        if (s != HP2D_OK) return s;
+        if (inflow_cells_h.cell.size() + stage_cells_h.cell.size() + cells.cell.size() >= (1u << 23)) {
+            ctx->err = "too many inflow cells";
+            return HP2D_INVALID_ARG;
+        }
         if (ng) {
             inf_t.alloc(size_t(nt));
             inf_r.alloc(size_t(nt) * ng);
-            inf_cells.alloc(size_t(ng));
             inf_depth.alloc(size_t(ng));
-            inf_off.alloc(off.size());
-            inf_gauge.alloc(std::max<size_t>(gl.size(), 1));
             upload(inf_t.p, std::vector<double>(t0, t0 + nt));
             upload(inf_r.p, std::vector<double>(rate, rate + size_t(nt) * ng));
-            upload(inf_cells.p, host_gcells);
-            upload(inf_off.p, off);
-            if (!gl.empty()) upload(inf_gauge.p, gl);
         }
         inflow.n_gauges = ng;
         inflow.n_times = nt;
         inflow.t_start = inf_t.p;
         inflow.rate = inf_r.p;
         inflow.depth = inf_depth.p;
-        inflow.cell_off = inf_off.p;
-        inflow.cell_gauge = inf_gauge.p;
-        inflow.gauge_cells = inf_cells.p;
-        invalidate_graph();
-        dirty = true;
+        inflow_cells_h = std::move(cells);
+        rebuild_bc_cells();
+        return HP2D_OK;
+    }
+
+    // Stage hydrographs: gauge water depths [m] [n_times][n_gauges] on the start-stamped table
+    // t_start, (row, col, gauge) cells; n_gauges = 0 removes them.
+    hp2d_status set_stage(int32_t ng, int32_t nt, const double* t0, const double* depth, int32_t nc,
+                          const int32_t* rows, const int32_t* cols, const int32_t* gauge) {
+        if (!static_ready) { ctx->err = "hp2d_upload_static must come before hp2d_set_stage"; return HP2D_NOT_READY; }
+        if (ng < 0 || (ng > 0 && (nt < 1 || nc < 1))) { ctx->err = "bad stage table shape"; return HP2D_INVALID_ARG; }
+        BcCells cells;
+        hp2d_status s = check_bc_cells(ng, nc, rows, cols, gauge, cells, "stage");
+        if (s != HP2D_OK) return s;
+        for (size_t k : cells.cell)
+            if (!std::isfinite(host_z[k])) { ctx->err = "a stage cell needs a finite elevation"; return HP2D_INVALID_ARG; }
+        if (inflow_cells_h.cell.size() + stage_cells_h.cell.size() + cells.cell.size() >= (1u << 23)) {
+            ctx->err = "too many stage cells";
+            return HP2D_INVALID_ARG;
+        }
+        if (ng) {
+            stage_t.alloc(size_t(nt));
+            stage_d.alloc(size_t(nt) * ng);
+            stage_now.alloc(size_t(ng));
+            upload(stage_t.p, std::vector<double>(t0, t0 + nt));
+            upload(stage_d.p, std::vector<double>(depth, depth + size_t(nt) * ng));
+        }
+        inflow.n_stage = ng;
+        inflow.n_stage_times = nt;
+        inflow.stage_t = stage_t.p;
+        inflow.stage_d = stage_d.p;
+        inflow.stage_now = stage_now.p;
+        stage_cells_h = std::move(cells);
+        rebuild_bc_cells();
         return HP2D_OK;
     }
 
@@ -848,7 +930,7 @@ template <typename R> struct Impl : Base {
         k_fused_step<R, kThreads, INF, MAP, CPL, INFL><<<a.n_ctas, kThreads, sm, st()>>>(a);
     }
     template <int INF, int CPL> void launch_i(const FusedArgs<R>& a) {
-        const bool map = rain.n_maps > 0, infl = inflow.n_gauges > 0;
+        const bool map = rain.n_maps > 0, infl = inflow.n_gauges > 0 || inflow.n_stage > 0;
         if (map) {
             if (infl) launch_one<INF, true, CPL, true>(a); else launch_one<INF, true, CPL, false>(a);
         } else {
@@ -885,7 +967,7 @@ template <typename R> struct Impl : Base {
         k_skip_flag<R><<<blocks_for(n), kThreads, 0, st()>>>(st4[hs.cur].p, stat.p, ny, nx, rain, ga() ? 1 : 0, res,
                                                            ctx->p.depth_tolerance, ctx->p.arrival_threshold, sc.p);
         HP_CK(cudaGetLastError());
-        if (inflow.n_gauges) {
+        if (inflow.n_gauges || inflow.n_stage) {
             k_inflow_depth<R><<<1, kThreads, 0, st()>>>(inflow, sc.p);
             HP_CK(cudaGetLastError());
         }
@@ -1165,6 +1247,7 @@ template <typename R> struct Impl : Base {
         o->rain_t1 = hs.rain_b;
         o->t_previous = hs.t_prev;
         o->inflow_volume = hs.inflow_vol;
+        o->stage_volume = hs.stage_vol;
         o->max_velocity = hs.vmax_last;
         o->rain_volume = hs.rain_vol;
         o->infiltration_volume = hs.inf_vol;
@@ -1284,7 +1367,7 @@ struct hp2d_ensemble {
             }
             const int mga = im.inf_mode(), mmap = im.rain.n_maps > 0 ? 1 : 0;
             if (m == 0) { ga = mga; map = mmap; infl = false; }
-            if (im.inflow.n_gauges > 0) infl = true;
+            if (im.inflow.n_gauges > 0 || im.inflow.n_stage > 0) infl = true;
             if (mga != ga || mmap != map) {
                 err = "members must agree on the infiltration model and on the kind of rain forcing";
                 return HP2D_INVALID_ARG;
@@ -1569,6 +1652,13 @@ hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count) {
 hp2d_status hp2d_download_map_record(hp2d_ctx* ctx, int64_t index, double* depth_mm, double* t_min) {
     if (!depth_mm) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.download_map_record(index, depth_mm, t_min); });
+}
+
+hp2d_status hp2d_set_stage(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, const double* t_start,
+                           const double* depth_m, int32_t n_cells, const int32_t* rows, const int32_t* cols,
+                           const int32_t* gauge) {
+    if (n_gauges > 0 && (!t_start || !depth_m || !rows || !cols || !gauge)) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) { return m.set_stage(n_gauges, n_times, t_start, depth_m, n_cells, rows, cols, gauge); });
 }
 
 hp2d_status hp2d_set_rain_gauges(hp2d_ctx* ctx, int32_t n_gauges, const double* x_gauge, const double* y_gauge,

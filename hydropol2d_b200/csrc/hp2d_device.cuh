@@ -148,6 +148,8 @@ struct StepScalars {
     int skip_next;         // fused step: some outlet cell ends below -1e-11 m after the next rain
     int pad2;
     double inflow_vol;     // cumulative inflow-hydrograph volume [m^3]
+    double stage_vol;      // cumulative volume the stage overwrites added [m^3]
+    double acc_stage;      // step sum [m] (times cell area later)
     // map records (save_output_maps.m:25-27, :160-166): index of the last record time below
     // t_save, records taken, and whether the next step's input depth is to be recorded
     long long rec_count;
@@ -322,6 +324,9 @@ __device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i,
 // Inflow cells carry kInflowBit in their meta word and, in bits 8..30, their entry e: the
 // cell's gauges are cell_gauge[cell_off[e] .. cell_off[e+1]) in increasing order.
 constexpr unsigned kInflowBit = 0x80000000u;
+// The same entries carry the stage-hydrograph cells (flag_stage_hydrograph,
+// update_spatial_BC.m:316-357): cell_stage[e] is the stage gauge whose depth overwrites the
+// cell's depth after the step (-1: none).
 template <typename R> struct InflowDesc {
     int n_gauges, n_times;
     const double* t_start;      // [n_times] [min]
@@ -330,7 +335,21 @@ template <typename R> struct InflowDesc {
     const int32_t* cell_off;    // [entries + 1]
     const int32_t* cell_gauge;
     const double* gauge_cells;  // [n_gauges] cells of the gauge with a finite elevation
+    int n_stage, n_stage_times;
+    const double* stage_t;      // [n_stage_times] [min], start-stamped
+    const double* stage_d;      // [n_stage_times][n_stage] water depth [m]
+    R* stage_now;               // [n_stage] this step's stage depth [m]
+    const int32_t* cell_stage;  // [entries]
 };
+// stage depth of gauge g at clock t: the last record starting at or before t, else the
+// first (update_spatial_BC.m:322-330)
+template <typename R>
+__device__ __host__ inline double stage_at(const InflowDesc<R>& d, int g, double t) {
+    int z = 0;
+    for (int q = 0; q < d.n_stage_times; ++q)
+        if (d.stage_t[q] <= t) z = q;
+    return d.stage_d[size_t(z) * d.n_stage + g];
+}
 template <typename R>
 __device__ __host__ inline double inflow_integral(const InflowDesc<R>& d, int g, double a, double b) {
     double acc = 0.0;
@@ -344,14 +363,16 @@ __device__ __host__ inline double inflow_integral(const InflowDesc<R>& d, int g,
     }
     return acc;
 }
-// inflow depth [m] of the cell with meta word `meta` (0 when it is no inflow cell)
-template <typename R> __device__ __forceinline__ R inflow_at(const InflowDesc<R>& d, unsigned meta) {
+// adds the inflow depth [m] of the cell with meta word `meta` to hh (BC_States.inflow is the
+// sum over the cell's gauges, added once); cells without inflow gauges are left alone
+template <typename R> __device__ __forceinline__ void add_inflow(const InflowDesc<R>& d, unsigned meta, R& hh) {
+    if (!(meta & kInflowBit)) return;
+    const unsigned e = (meta >> 8) & 0x7FFFFFu;
+    const int q0 = d.cell_off[e], q1 = d.cell_off[e + 1];
+    if (q0 == q1) return;
     R v = R(0);
-    if (meta & kInflowBit) {
-        const unsigned e = (meta >> 8) & 0x7FFFFFu;
-        for (int q = d.cell_off[e]; q < d.cell_off[e + 1]; ++q) v = v + d.depth[d.cell_gauge[q]];
-    }
-    return v;
+    for (int q = q0; q < q1; ++q) v = v + d.depth[d.cell_gauge[q]];
+    hh = hh + v;
 }
 // outlet entry + 1 of a meta word (0: not an outlet)
 __device__ __host__ inline unsigned outlet_ord(unsigned meta) { return (meta & kInflowBit) ? 0u : meta >> 8; }

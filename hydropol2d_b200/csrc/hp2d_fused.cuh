@@ -174,6 +174,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     __shared__ int s_cur, s_skip, s_done, s_last;
     __shared__ int s_negn;   // an outlet cell would go below -1e-11 m after the next rain
     __shared__ int s_rec;    // slot that receives this step's input depth (-1: none)
+    __shared__ double s_stage;   // depth the stage overwrites of this CTA added [m]
     __shared__ RainStep<R> s_rs, s_rsn;   // this step's rain and the next one's
     __shared__ R red_s2[NT / 32];
     __shared__ unsigned long long red_c[NT / 32];
@@ -191,6 +192,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         s_cur = sc->cur;
         s_skip = sc->skip_clamp;
         s_negn = 0;
+        s_stage = 0.0;
         s_rec = (sc->rec_pending && a.rec.n_slots > 0) ? int(sc->rec_count % a.rec.n_slots) : -1;
         s_done = !(s_tmin <= a.t_end);
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
@@ -359,7 +361,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         if (own) gout[c] = go;
                     }
                     // inflow hydrographs after the infiltration (Hydrological_Model.m:27-28)
-                    if (INFL && (meta[h] & kInflowBit)) hh = hh + inflow_at(a.inflow, meta[h]);
+                    if (INFL) add_inflow(a.inflow, meta[h], hh);
                     if (!skip && hh < R(1e-9)) hh = R(0);
                     if (hh < R(0)) hh = R(0);
                     hT0[h] = hh;
@@ -475,6 +477,16 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                             hn + (MAP ? s_rsn.at(a.rain, rm2, j[h], ny, nx) : s_rsn.depth) < R(-1e-11))
                             s_negn = 1;   // rare: kept in shared memory, not a register
                     }
+                    // stage hydrograph: the cell's depth becomes the gauge's stage
+                    // (update_spatial_BC.m:332-341, after the step's refreshing_timestep)
+                    if (INFL && (mt2[h] & kInflowBit)) {
+                        const int sg = a.inflow.cell_stage[(mt2[h] >> 8) & 0x7FFFFFu];
+                        if (sg >= 0) {
+                            const R sv = a.inflow.stage_now[sg];
+                            atomicAdd(&s_stage, double(sv) - double(hn));
+                            hn = sv;
+                        }
+                    }
                     const R dm = dm2[h];
                     if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
                     // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
@@ -570,6 +582,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         if (inf_acc != 0.0) atomicAdd(&sc->acc_inf, inf_acc);
         if (out_acc != 0.0) atomicAdd(&sc->acc_out, out_acc);
         if (negn) atomicOr(&sc->skip_next, 1);
+        if (INFL && s_stage != 0.0) atomicAdd(&sc->acc_stage, s_stage);
         __threadfence();
         const unsigned int ticket = atomicAdd(&sc->counter, 1u);
         s_last = (ticket == a.n_ctas - 1);
@@ -619,6 +632,10 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             for (int g = 0; g < a.inflow.n_gauges; ++g) v += double(a.inflow.depth[g]) * a.inflow.gauge_cells[g];
             sc->inflow_vol += v * area;
         }
+        if (a.inflow.n_stage) {
+            sc->stage_vol += __ldcg(&sc->acc_stage) * area;
+            sc->acc_stage = 0.0;
+        }
         // the next step's rain: update_spatial_BC over [t_previous, t]
         // (HydroPol2D_Main_While.m:721), then t_previous <- the clock increment on the first
         // step and t after it (:734-738), and the clock advances by the new step (:779)
@@ -646,11 +663,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->counter = 0u;
         sc->skip_clamp = atomicExch(&sc->skip_next, 0);   // gathered by every CTA's outlets
     }
-    if (a.inflow.n_gauges) {   // the next step's gauge depths over its rain interval
+    if (a.inflow.n_gauges || a.inflow.n_stage) {   // the next step's gauge depths and stages
         __syncthreads();
-        const double ra = a.sc->rain_a, rb = a.sc->rain_b;
+        const double ra = a.sc->rain_a, rb = a.sc->rain_b, tn = a.sc->t_min;
         for (int g = tid; g < a.inflow.n_gauges; g += NT)
             a.inflow.depth[g] = R(inflow_integral(a.inflow, g, ra, rb) / 60000.0);
+        for (int g = tid; g < a.inflow.n_stage; g += NT) a.inflow.stage_now[g] = R(stage_at(a.inflow, g, tn));
     }
     return cta_ok;
 }
@@ -692,9 +710,10 @@ template <typename R> __global__ void k_record_depth(size_t n, const typename Ve
 
 // gauge depths of the current rain interval (after a host change of the inflow or clock)
 template <typename R> __global__ void k_inflow_depth(InflowDesc<R> d, const StepScalars* sc) {
-    const double ra = sc->rain_a, rb = sc->rain_b;
+    const double ra = sc->rain_a, rb = sc->rain_b, t = sc->t_min;
     for (int g = threadIdx.x; g < d.n_gauges; g += blockDim.x)
         d.depth[g] = R(inflow_integral(d, g, ra, rb) / 60000.0);
+    for (int g = threadIdx.x; g < d.n_stage; g += blockDim.x) d.stage_now[g] = R(stage_at(d, g, t));
 }
 
 template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>

@@ -41,7 +41,7 @@ __global__ void k_hydro_rain_ga(GridView<R> g, double rain_a, double rain_b, dou
             T[c] = Tc;
             if (isfinite(fd)) iacc += double(fd);
         }
-        if (inflow.n_gauges) hh = hh + inflow_at(inflow, meta_bits(stat[c].w));   // Hydrological_Model.m:27-28
+        if (inflow.n_gauges) add_inflow(inflow, meta_bits(stat[c].w), hh);   // Hydrological_Model.m:27-28
         if (hh < R(-1e-11)) neg = 1;
         h[c] = hh;
     }

@@ -138,6 +138,18 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_inflow(self._h, int(ng), int(t.size), _dp(t), _dp(r), int(rr.size),
                                             rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
 
+    def set_stage(self, t_start, depth_m, rows, cols, gauge):
+        """Stage hydrographs: water depths ``depth_m`` (n_times, n_gauges) [m] on the start-stamped
+        ``t_start`` [min]; cells ``rows``/``cols`` of gauge ``gauge`` (Wshed_Properties.stage_mask)."""
+        t = _f64(t_start).ravel()
+        d = np.ascontiguousarray(np.asarray(depth_m, dtype=np.float64).reshape(t.size, -1))
+        rr = np.ascontiguousarray(rows, dtype=np.int32).ravel()
+        cc = np.ascontiguousarray(cols, dtype=np.int32).ravel()
+        gg = np.ascontiguousarray(gauge, dtype=np.int32).ravel()
+        ip = C.POINTER(C.c_int32)
+        self._check(self._L.hp2d_set_stage(self._h, int(d.shape[1]), int(t.size), _dp(t), _dp(d), int(rr.size),
+                                           rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
+
     def set_rain_gauges(self, x_gauge, y_gauge, rates, record_dt: float, x_ul: float = 0.0, y_ul: float = 0.0):
         """Rain from gauges: ``rates`` (n_times, n_gauges) [mm/h] (NaN: no record) over intervals
         of ``record_dt`` minutes, interpolated by inverse-distance weighting to every cell."""

@@ -39,6 +39,7 @@ class Case:
     I0: np.ndarray | None = None            # mm
     meta: dict = field(default_factory=dict)
     inflow: dict | None = None              # set_inflow kwargs (t_start, rates, rows, cols, gauge)
+    stage: dict | None = None               # set_stage kwargs (t_start, depth_m, rows, cols, gauge)
 
     @property
     def shape(self):
@@ -56,6 +57,8 @@ class Case:
             sf.set_rain_maps(self.rain_maps, self.rain_map_dt)
         if self.inflow is not None:
             sf.set_inflow(**self.inflow)
+        if self.stage is not None:
+            sf.set_stage(**self.stage)
         return sf
 
 

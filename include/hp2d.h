@@ -110,6 +110,7 @@ typedef struct hp2d_diag {
     double rain_t0, rain_t1;      /* clock interval whose rain the next step applies [min] */
     double t_previous;            /* the loop's t_previous [min] */
     double inflow_volume;         /* cumulative inflow-hydrograph volume [m^3] */
+    double stage_volume;          /* cumulative volume the stage overwrites added [m^3] */
 } hp2d_diag;
 
 typedef struct hp2d_ctx hp2d_ctx;
@@ -220,6 +221,18 @@ hp2d_status hp2d_set_map_records(hp2d_ctx* ctx, int32_t n_times, const double* t
 hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count);
 /* Record `index` (0-based, one of the last n_slots taken): depth [mm] (ny*nx) and clock [min]. */
 hp2d_status hp2d_download_map_record(hp2d_ctx* ctx, int64_t index, double* depth_mm, double* t_min);
+
+/* Stage hydrographs (flags.flag_stage_hydrograph = 1; update_spatial_BC.m:316-357): n_gauges
+ * water-depth series [m] (row-major [n_times][n_gauges]) on the start-stamped table t_start
+ * [min] (the record in force is the last starting at or before the clock, else the first),
+ * and the n_cells (rows, cols, gauge) of Wshed_Properties.stage_mask(:,:,gauge).  After each
+ * fused step (after its timestep refresh, before the maxima) a stage cell's depth becomes its
+ * gauge's depth at the step's clock; a cell in several masks takes the highest gauge.  Call
+ * after hp2d_upload_static; outlet and NaN-elevation cells cannot be stage cells; the unfused
+ * entry points leave the stage to the caller (it is update_spatial_BC's). */
+hp2d_status hp2d_set_stage(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, const double* t_start,
+                           const double* depth_m, int32_t n_cells, const int32_t* rows, const int32_t* cols,
+                           const int32_t* gauge);
 
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
 /* Hydrological_Model for this path: adds delta_p_agg (the rain of the current rain

@@ -64,6 +64,8 @@ def _load():
             "oracle_set_clock": ([vp, C.c_double, C.c_double, C.c_int64], C.c_int),
             "oracle_set_rain_clock": ([vp, C.c_double, C.c_double, C.c_double], C.c_int),
             "oracle_set_map_records": ([vp, C.c_int32, dp], C.c_int),
+            "oracle_set_stage": ([vp, C.c_int32, C.c_int32, dp, dp, C.c_int32, P(C.c_int32), P(C.c_int32),
+                                  P(C.c_int32)], C.c_int),
             "oracle_map_records": ([vp], C.c_int64),
             "oracle_download_map_record": ([vp, C.c_int64, dp, dp], C.c_int),
             "oracle_set_inflow": ([vp, C.c_int32, C.c_int32, dp, dp, C.c_int32, P(C.c_int32), P(C.c_int32),
@@ -156,6 +158,16 @@ class KernelFormOracle:
         self._L.oracle_set_inflow(self._h, int(r.shape[1]), int(t.size), _dp(t), _dp(r), int(rr.size),
                                   rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip),
                                   _dp(self._z))
+
+    def set_stage(self, t_start, depth_m, rows, cols, gauge):
+        t = np.ascontiguousarray(t_start, dtype=np.float64).ravel()
+        d = np.ascontiguousarray(np.asarray(depth_m, dtype=np.float64).reshape(t.size, -1))
+        rr = np.ascontiguousarray(rows, dtype=np.int32).ravel()
+        cc = np.ascontiguousarray(cols, dtype=np.int32).ravel()
+        gg = np.ascontiguousarray(gauge, dtype=np.int32).ravel()
+        ip = C.POINTER(C.c_int32)
+        self._L.oracle_set_stage(self._h, int(d.shape[1]), int(t.size), _dp(t), _dp(d), int(rr.size),
+                                 rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip))
 
     def set_map_records(self, time_records, n_slots=None):
         t = np.ascontiguousarray(time_records, dtype=np.float64).ravel()

@@ -401,6 +401,44 @@ public:
         }
     }
 
+    // ---------------- stage hydrographs (update_spatial_BC.m:316-357) ----------------
+    // after the step's timestep refresh, a stage cell's depth becomes its gauge's water depth
+    // at the step's clock (the last record starting at or before it, else the first); a cell
+    // of several masks takes the highest gauge (the reference overwrites in gauge order)
+    int stg_ng = 0, stg_nt = 0;
+    std::vector<double> stg_t, stg_d;
+    std::vector<int32_t> stg_cell;   // per cell: gauge or -1
+    double stage_vol = 0;
+    void set_stage(int ng, int nt, const double* t0, const double* d, int nc, const int32_t* rows,
+                   const int32_t* cols, const int32_t* gauge) {
+        stg_ng = ng; stg_nt = nt;
+        stg_t.assign(t0, t0 + (ng ? nt : 0));
+        stg_d.assign(d, d + (ng ? size_t(nt) * ng : 0));
+        stg_cell.assign(size_t(ny) * nx, -1);
+        for (int q = 0; q < (ng ? nc : 0); ++q) {
+            int32_t& c = stg_cell[at(rows[q], cols[q])];
+            c = std::max(c, gauge[q]);
+        }
+    }
+    void apply_stage() {
+        if (!stg_ng) return;
+        std::vector<R> now(static_cast<size_t>(stg_ng), R(0));
+        for (int g = 0; g < stg_ng; ++g) {
+            int z = 0;
+            for (int q = 0; q < stg_nt; ++q)
+                if (stg_t[q] <= t_min) z = q;
+            now[g] = R(stg_d[size_t(z) * stg_ng + g]);
+        }
+        double v = 0;
+        for (size_t c = 0; c < h.size(); ++c) {
+            if (stg_cell[c] < 0) continue;
+            const R sv = now[size_t(stg_cell[c])];
+            v += double(sv) - double(h[c]);
+            h[c] = sv;
+        }
+        stage_vol += v * res * res;
+    }
+
     // ---------------- hydrology: rain + Green-Ampt + clamp ----------------
     void hydrology(double dts) {
         Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
@@ -697,6 +735,7 @@ public:
             vmax_last = vm;
             if (tcr == p.min_time_step) ++unstable;
         }
+        apply_stage();
         track(t_min * 60.0 + dts);
         if (!rec_times.empty()) {
             const int idx = last_below(t_min + tcr / 60.0);

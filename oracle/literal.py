@@ -474,6 +474,11 @@ class RunConfig:
     inflow_times_min: np.ndarray | None = None
     inflow_rates_mmh: np.ndarray | None = None
     inflow_cells: np.ndarray | None = None
+    # stage hydrographs: start-stamped times [min], water depths (n_times, n_gauges) [m] and
+    # Wshed_Properties.stage_mask as (n_gauges, ny, nx) 0/1 masks
+    stage_times_min: np.ndarray | None = None
+    stage_depth_m: np.ndarray | None = None
+    stage_cells: np.ndarray | None = None
     fixed_time_step_s: float | None = None      # bypass refreshing_timestep
 
 
@@ -642,6 +647,7 @@ class RunState:
     infiltration_volume: float = 0.0
     outlet_volume: float = 0.0
     inflow_volume: float = 0.0
+    stage_volume: float = 0.0
     # rain interval [rain_a, rain_b] of the current step and the loop's t_previous [min]; the
     # first step's comes from the call before the loop (HydroPol2D_Main_While.m:115) with
     # t_previous = 0 (:120)
@@ -713,6 +719,16 @@ def step(cfg: RunConfig, st: RunState) -> None:
         else:
             tcr = time_step * 60
             cfl = None
+    # update_spatial_BC.m:316-357: stage cells take the gauge's depth at the clock t
+    if cfg.stage_cells is not None:
+        times = np.asarray(cfg.stage_times_min, dtype=np.float64)
+        depth = np.asarray(cfg.stage_depth_m, dtype=np.float64).reshape(times.size, -1)
+        hit = np.nonzero(times <= st.t)[0]
+        z2 = int(hit[-1]) if hit.size else 0
+        before = out.d_t.copy()
+        for i in range(depth.shape[1]):
+            out.d_t[np.asarray(cfg.stage_cells[i], dtype=bool)] = 1000.0 * depth[z2, i]
+        st.stage_volume += float(np.nansum(out.d_t - before)) * A / 1000
     # save_output_maps.m:588-600 (running maximum depth) + arrival-time definition
     t_end_s = st.t * 60 + time_step * 60
     newly = (st.dmax < cfg.arrival_threshold_mm) & (out.d_t >= cfg.arrival_threshold_mm)

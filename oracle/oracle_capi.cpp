@@ -72,6 +72,11 @@ int oracle_set_inflow(oracle_model* m, int32_t ng, int32_t nt, const double* t0,
     });
 }
 
+int oracle_set_stage(oracle_model* m, int32_t ng, int32_t nt, const double* t0, const double* d, int32_t nc,
+                     const int32_t* rows, const int32_t* cols, const int32_t* gauge) {
+    return dispatch(m, [&](auto& M) { M.set_stage(ng, nt, t0, d, nc, rows, cols, gauge); return 0; });
+}
+
 int oracle_set_map_records(oracle_model* m, int32_t n, const double* times) {
     return dispatch(m, [&](auto& M) { M.set_map_records(n, times); return 0; });
 }
@@ -217,6 +222,7 @@ int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
         o->rain_t1 = M.rain_b;
         o->t_previous = M.t_prev;
         o->inflow_volume = M.inflow_vol;
+        o->stage_volume = M.stage_vol;
         return 0;
     });
 }

@@ -124,3 +124,32 @@ def test_ensemble_member_with_inflow(hp2d_lib):
             assert same_bits(m.download_native(f), s.download_native(f)), f
         assert m.diag()["t"] == s.diag()["t"]
     ens.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_stage_hydrograph_bit_exact(precision, hp2d_lib, oracle_lib):
+    from tests.test_inflow import stage_case
+    case = stage_case(40, 48, minutes=8.0)
+    g, o = make_pair(case, precision)
+    for chunk in (1, 5, 64, 300):
+        g.fused_steps(chunk)
+        o.fused_steps(chunk)
+        assert_same_state(g, o, FIELDS, f"after chunk {chunk}")
+        assert_same_clock(g, o)
+    rel = 1e-5 if precision == "fp32" else 1e-12
+    assert g.diag()["stage_volume"] == pytest.approx(o.diag()["stage_volume"], rel=rel)
+
+
+def test_stage_and_inflow_together(hp2d_lib, oracle_lib):
+    from tests.test_inflow import stage_case
+    case = stage_case(40, 48, minutes=6.0)
+    flood = S.inflow_case(40, 48, minutes=6.0).inflow
+    keep = flood["gauge"] == 1                      # the plane block, away from the stage cells
+    case.inflow = dict(t_start=flood["t_start"], rates=flood["rates"][:, 1:], rows=flood["rows"][keep],
+                       cols=flood["cols"][keep], gauge=np.zeros(keep.sum(), np.int32))
+    g, o = make_pair(case, "fp32")
+    g.fused_steps(400)
+    o.fused_steps(400)
+    assert_same_state(g, o, FIELDS)
+    assert_same_clock(g, o)
+    assert g.diag()["inflow_volume"] > 0 and g.diag()["stage_volume"] > 0

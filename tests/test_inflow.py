@@ -60,3 +60,44 @@ def test_water_balance_with_inflow(oracle_lib):
     # the 1e-6 mm clamp (Hydrological_Model.m:49) removes the thinnest films at the wave's edge
     assert lhs == pytest.approx(rhs, rel=1e-7)
     assert lhs <= rhs
+
+
+def stage_case(ny=32, nx=32, minutes=8.0):
+    """The V-tilted catchment, dry, with a stage hydrograph on the channel's upstream cells
+    (0.2 m from minute 0, 0.6 m from minute 2, 0.1 m from minute 5) and a second gauge on one
+    plane cell that is also in the first mask (the higher gauge wins)."""
+    case = S.inflow_case(ny, nx, minutes=minutes)
+    case.inflow = None
+    ch = case.outlet_cols
+    rows = np.concatenate([np.full(ch.size, ny - 1), [ny - 1]]).astype(np.int32)
+    cols = np.concatenate([ch, [ch[0]]]).astype(np.int32)
+    gauge = np.concatenate([np.zeros(ch.size), [1]]).astype(np.int32)
+    case.stage = dict(t_start=np.array([0.0, 2.0, 5.0]),
+                      depth_m=np.array([[0.2, 0.05], [0.6, 0.3], [0.1, 0.0]]),
+                      rows=rows, cols=cols, gauge=gauge)
+    return case
+
+
+def test_stage_kernel_form_follows_literal(oracle_lib):
+    case = stage_case()
+    cfg = literal_cfg(case)
+    st = L.init_state(cfg)
+    o = kernel_form(case)
+    for k in range(400):
+        if st.t > cfg.routing_time + cfg.min_time_step / 60:
+            break
+        L.step(cfg, st)
+        o.fused_steps(1)
+        if k % 40 == 0:
+            h = o.download_native("h") * 1000
+            assert np.allclose(h, st.d, rtol=1e-9, atol=1e-9), k
+    d = o.diag()
+    assert d["t"] == pytest.approx(st.t, rel=1e-12)
+    assert d["stage_volume"] == pytest.approx(st.stage_volume, rel=1e-9)
+    assert st.stage_volume > 0
+    # the last record in force at the end (0.1 m) sits on the stage cells
+    h = o.download_native("h")
+    assert case.stage["cols"].size >= 3
+    assert h[case.stage["rows"][1], case.stage["cols"][1]] == pytest.approx(0.1)
+    # the shared cell takes gauge 1
+    assert h[case.stage["rows"][-1], case.stage["cols"][-1]] == pytest.approx(0.0)

@@ -34,6 +34,13 @@ def literal_cfg(case):
         for r, c, g in zip(f["rows"], f["cols"], f["gauge"]):
             masks[g, r, c] += 1.0
         kw["inflow_times_min"], kw["inflow_rates_mmh"], kw["inflow_cells"] = f["t_start"], f["rates"], masks
+    stage = getattr(case, "stage", None)
+    if stage is not None:
+        d = np.asarray(stage["depth_m"]).reshape(len(stage["t_start"]), -1)
+        masks = np.zeros((d.shape[1],) + case.shape)
+        for r, c, g in zip(stage["rows"], stage["cols"], stage["gauge"]):
+            masks[g, r, c] = 1.0
+        kw["stage_times_min"], kw["stage_depth_m"], kw["stage_cells"] = stage["t_start"], d, masks
     return L.RunConfig(**kw)
 
 
