@@ -313,13 +313,16 @@ def main():
     t0 = time.perf_counter()
     sf = SurfaceFlow(ny, nx, DX, "fp32", device=local, **case.params)
     case.apply(sf)
+    t1 = time.perf_counter()
     q_hydro = []
     for _ in range(e2e_steps):
         sf.fused_steps(1)
         q_hydro.append(sf.download_native("qo"))
+    t2 = time.perf_counter()
     d_final = sf.download("depth")
     dmax = sf.download("dmax")
     e2e_s = time.perf_counter() - t0
+    e2e_split = {"setup_s": t1 - t0, "steps_s": t2 - t1, "readback_s": e2e_s - (t2 - t0)}
     n_out = sf.n_outlets
     sf.close()
     # H2D per run: context set-up (static + 2 state records + arrival, 52 B/cell), static
@@ -369,7 +372,7 @@ def main():
                      "traffic": None if traffic_pc is None else traffic_pc * cells},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d_per_step,
-                "d2h_bytes_per_step": d2h_per_step, "steps": e2e_steps,
+                "d2h_bytes_per_step": d2h_per_step, "steps": e2e_steps, **e2e_split,
                 "includes": "input generation excluded; static+state upload, per-step hydrograph "
                             "and clock readback, final depth and dmax readback"},
         "late_window": late,
