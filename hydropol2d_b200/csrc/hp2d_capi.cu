@@ -192,15 +192,11 @@ template <typename R> struct Impl : Base {
         hs.t_prev = 0.0;
         push_sc();
         // closed faces everywhere until hp2d_upload_static, dry state
-        std::vector<V4> s(n), x(n);
         const R qn = std::numeric_limits<R>::quiet_NaN();
-        for (size_t k = 0; k < n; ++k) {
-            s[k] = V4{qn, qn, R(0), make_meta<R>(255u)};
-            x[k] = V4{R(0), R(0), R(0), -std::numeric_limits<R>::infinity()};
-        }
-        upload(stat.p, s);
-        upload(st4[0].p, x);
-        upload(st4[1].p, x);
+        fill(stat.p, n, V4{qn, qn, R(0), make_meta<R>(255u)});
+        const V4 dry{R(0), R(0), R(0), -std::numeric_limits<R>::infinity()};
+        fill(st4[0].p, n, dry);
+        fill(st4[1].p, n, dry);
         fill(arrival.p, n, std::numeric_limits<R>::infinity());
     }
     ~Impl() override {
@@ -224,7 +220,12 @@ template <typename R> struct Impl : Base {
         }
         return v;
     }
-    void fill(R* p, size_t count, R v) { upload(p, std::vector<R>(count, v)); }
+    template <typename T> void fill(T* p, size_t count, T v) {   // on the device, no host staging
+        if (!count) return;
+        k_fill<T><<<blocks_for(count), kThreads, 0, st()>>>(count, p, v);
+        HP_CK(cudaGetLastError());
+        HP_CK(cudaStreamSynchronize(st()));
+    }
     GridView<R> view() const {
         GridView<R> gv;
         gv.ny = ny; gv.nx = nx; gv.res = res;
@@ -297,20 +298,22 @@ template <typename R> struct Impl : Base {
             int i = cells[o] / nx, j = cells[o] % nx;
             bits[size_t(i) * bit_words + (j >> 5)] |= 1u << (j & 31);
         }
-        std::vector<V4> s(n);
-        std::vector<R> a(n), b(n), c(n);
-        for (int i = 0; i < ny; ++i)
-            for (int j = 0; j < nx; ++j) {
-                size_t k = size_t(i) * nx + j;
-                a[k] = R((j + 1 < nx) ? z[k + 1] - z[k] : edge);
-                b[k] = R((i >= 1) ? z[k - nx] - z[k] : edge);
-                c[k] = R(rough[k] * rough[k]);
-                s[k] = V4{a[k], b[k], c[k], make_meta<R>(host_meta[k])};
-            }
-        upload(stat.p, s);
-        // structure-of-arrays copies for the unfused entry points
-        dzx.alloc(n); dzy.alloc(n); n2.alloc(n);
-        upload(dzx.p, a); upload(dzy.p, b); upload(n2.p, c);
+        // the records (and the unfused entry points' structure-of-arrays copies) are built
+        // on the device from the caller's FP64 arrays
+        {
+            Dev<double> dz_, dr_;
+            Dev<uint32_t> dm_;
+            dz_.alloc(n); dr_.alloc(n); dm_.alloc(n);
+            HP_CK(cudaMemcpy(dz_.p, z, n * sizeof(double), cudaMemcpyHostToDevice));
+            HP_CK(cudaMemcpy(dr_.p, rough, n * sizeof(double), cudaMemcpyHostToDevice));
+            upload(dm_.p, host_meta);
+            dzx.alloc(n); dzy.alloc(n); n2.alloc(n);
+            k_build_static<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, dz_.p, dr_.p, dm_.p, stat.p, dzx.p,
+                                                                     dzy.p, n2.p);
+            HP_CK(cudaGetLastError());
+            HP_CK(cudaStreamSynchronize(st()));
+        }
+        (void)edge;
         outlet_bits.alloc(bits.size());
         upload(outlet_bits.p, bits);
         outlet_cells.alloc(std::max(n_out, 1));
@@ -423,15 +426,19 @@ template <typename R> struct Impl : Base {
 
     hp2d_status set_state(const double* d, const double* outflow, const double* Imm) {
         pull_sc();
-        std::vector<V4> x(n);
-        for (size_t k = 0; k < n; ++k) {
-            x[k].x = R(d[k] / 1000.0);
-            // outflow_bates [mm/h] -> q [m^2/s]: mm/h / 1000 / 3600 * dx (LIM_D4.m:198)
-            x[k].y = outflow ? R(outflow[k] / 3.6e6 * res) : R(0);
-            x[k].z = outflow ? R(outflow[n + k] / 3.6e6 * res) : R(0);
-            x[k].w = -std::numeric_limits<R>::infinity();
+        {   // records built on the device from the caller's arrays
+            Dev<double> dd, dq;
+            dd.alloc(n);
+            HP_CK(cudaMemcpy(dd.p, d, n * sizeof(double), cudaMemcpyHostToDevice));
+            if (outflow) {
+                dq.alloc(2 * n);
+                HP_CK(cudaMemcpy(dq.p, outflow, 2 * n * sizeof(double), cudaMemcpyHostToDevice));
+            }
+            k_build_state<R><<<blocks_for(n), kThreads, 0, st()>>>(n, dd.p, outflow ? dq.p : nullptr, res,
+                                                                    st4[hs.cur].p);
+            HP_CK(cudaGetLastError());
+            HP_CK(cudaStreamSynchronize(st()));
         }
-        upload(st4[hs.cur].p, x);
         if (Imm || gs2[0].p) {
             for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
             std::vector<V2> g(n);
@@ -1135,6 +1142,15 @@ template <typename R> struct Impl : Base {
     }
 
     // ---------------- outputs ----------------
+    // one component of the current state records (a quarter of the record bytes cross)
+    std::vector<R> fetch_component(int comp) {
+        pull_sc();
+        Dev<R> tmp;
+        tmp.alloc(n);
+        k_state_component<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, comp, tmp.p);
+        HP_CK(cudaGetLastError());
+        return fetch(tmp.p, n);
+    }
     std::vector<V4> fetch_state() {
         pull_sc();
         return fetch(st4[hs.cur].p, n);
@@ -1151,9 +1167,9 @@ template <typename R> struct Impl : Base {
             for (int o = 0; o < n_out; ++o) out[cells[o]] = double(v[o]) * scale_;
         };
         switch (field) {
-            case HP2D_FIELD_DEPTH: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].x) * 1000.0; break; }
-            case HP2D_FIELD_QOUT_RIGHT: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].y) * to_mmh; break; }
-            case HP2D_FIELD_QOUT_UP: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].z) * to_mmh; break; }
+            case HP2D_FIELD_DEPTH: { auto v = fetch_component(0); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0; break; }
+            case HP2D_FIELD_QOUT_RIGHT: { auto v = fetch_component(1); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * to_mmh; break; }
+            case HP2D_FIELD_QOUT_UP: { auto v = fetch_component(2); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * to_mmh; break; }
             case HP2D_FIELD_QOUT_LEFT: {
                 auto v = fetch_state();
                 for (int i = 0; i < ny; ++i)
@@ -1176,7 +1192,7 @@ template <typename R> struct Impl : Base {
                 break;
             }
             case HP2D_FIELD_HF_OUTLET: per_outlet_map(hf3, 1.0); break;
-            case HP2D_FIELD_DMAX: { auto v = fetch_state(); for (size_t k = 0; k < n; ++k) out[k] = double(v[k].w) * 1000.0; break; }
+            case HP2D_FIELD_DMAX: { auto v = fetch_component(3); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0; break; }
             case HP2D_FIELD_ARRIVAL: { auto v = fetch(arrival.p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) / 60.0; break; }
             case HP2D_FIELD_SOIL_STORAGE: {
                 if (!gs2[0].p) { ctx->err = "no soil storage (hp2d_set_soil not called)"; return HP2D_NOT_READY; }

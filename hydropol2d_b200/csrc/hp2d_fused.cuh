@@ -702,6 +702,54 @@ static __global__ void k_idw_maps(int ny, int nx, double res, double x_ul, doubl
     }
 }
 
+// ---------------- host boundary on the device: records built from the caller's arrays ----
+// static record {dz_x, dz_y, n^2, meta} and the unfused path's copies, from the elevation and
+// roughness in FP64 (dz formed in FP64 and rounded once; the closed domain edges +inf)
+template <typename R>
+__global__ void k_build_static(int ny, int nx, const double* z, const double* rough, const uint32_t* meta,
+                               typename Vec<R>::V4* stat, R* dzx, R* dzy, R* n2) {
+    const size_t n = size_t(ny) * nx;
+    const double edge = __longlong_as_double(0x7ff0000000000000ll);   // +inf
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(k / nx), j = int(k % nx);
+        const R a = R((j + 1 < nx) ? z[k + 1] - z[k] : edge);
+        const R b = R((i >= 1) ? z[k - nx] - z[k] : edge);
+        const R c = R(rough[k] * rough[k]);
+        stat[k] = typename Vec<R>::V4{a, b, c, make_meta<R>(meta[k])};
+        dzx[k] = a;
+        dzy[k] = b;
+        n2[k] = c;
+    }
+}
+// state record {h, q_x, q_y, dmax = -inf} from depths.d_t [mm] and outflow_bates pages 1-2
+// [mm/h] (NULL: zero fluxes)
+template <typename R>
+__global__ void k_build_state(size_t n, const double* d, const double* outflow, double res,
+                              typename Vec<R>::V4* st) {
+    const R ninf = R(__longlong_as_double(0xfff0000000000000ll));
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        typename Vec<R>::V4 x;
+        x.x = R(d[k] / 1000.0);
+        // outflow_bates [mm/h] -> q [m^2/s]: mm/h / 1000 / 3600 * dx (LIM_D4.m:198)
+        x.y = outflow ? R(outflow[k] / 3.6e6 * res) : R(0);
+        x.z = outflow ? R(outflow[n + k] / 3.6e6 * res) : R(0);
+        x.w = ninf;
+        st[k] = x;
+    }
+}
+template <typename R> __global__ void k_fill(size_t n, R* p, R v) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
+        p[k] = v;
+}
+// one component of the state records (0..3 = h, q_x, q_y, dmax), for read-back
+template <typename R>
+__global__ void k_state_component(size_t n, const typename Vec<R>::V4* st, int comp, R* out) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const auto v = st[k];
+        out[k] = comp == 0 ? v.x : comp == 1 ? v.y : comp == 2 ? v.z : v.w;
+    }
+}
+
 // a map record taken by the host when no step follows the one that triggered it
 template <typename R> __global__ void k_record_depth(size_t n, const typename Vec<R>::V4* st, R* dst) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x)
