@@ -325,12 +325,12 @@ def main():
     e2e_split = {"setup_s": t1 - t0, "steps_s": t2 - t1, "readback_s": e2e_s - (t2 - t0)}
     n_out = sf.n_outlets
     sf.close()
-    # H2D per run: context set-up (static + 2 state records + arrival, 52 B/cell), static
-    # upload (record + unfused-path copies, 28 B/cell), state upload (record + arrival,
-    # 20 B/cell); D2H: outlet hydrograph (4 B per outlet) and the clock block every step,
-    # then the depth and dmax (state record twice, 32 B/cell) once
-    h2d_per_step = 100 * cells / e2e_steps
-    d2h_per_step = n_out * 4 + 2 * 184 + 32 * cells / e2e_steps
+    # H2D per run: the static upload (FP64 elevation and roughness and the 4-byte meta word,
+    # 20 B/cell) and the state upload (FP64 depth, 8 B/cell); the context's records are built
+    # and filled on the device.  D2H: outlet hydrograph (4 B per outlet) and the clock block
+    # every step, then the depth and dmax components (FP32, 8 B/cell) once
+    h2d_per_step = 28 * cells / e2e_steps
+    d2h_per_step = n_out * 4 + 2 * 224 + 8 * cells / e2e_steps   # 224 B: the clock block
     e2e = cells * e2e_steps / e2e_s / 1e9
     if dist is not None:
         t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)

@@ -304,8 +304,8 @@ template <typename R> struct Impl : Base {
             Dev<double> dz_, dr_;
             Dev<uint32_t> dm_;
             dz_.alloc(n); dr_.alloc(n); dm_.alloc(n);
-            HP_CK(cudaMemcpy(dz_.p, z, n * sizeof(double), cudaMemcpyHostToDevice));
-            HP_CK(cudaMemcpy(dr_.p, rough, n * sizeof(double), cudaMemcpyHostToDevice));
+            HP_CK(cudaMemcpyAsync(dz_.p, z, n * sizeof(double), cudaMemcpyHostToDevice, st()));
+            HP_CK(cudaMemcpyAsync(dr_.p, rough, n * sizeof(double), cudaMemcpyHostToDevice, st()));
             upload(dm_.p, host_meta);
             dzx.alloc(n); dzy.alloc(n); n2.alloc(n);
             k_build_static<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, dz_.p, dr_.p, dm_.p, stat.p, dzx.p,
@@ -429,10 +429,10 @@ template <typename R> struct Impl : Base {
         {   // records built on the device from the caller's arrays
             Dev<double> dd, dq;
             dd.alloc(n);
-            HP_CK(cudaMemcpy(dd.p, d, n * sizeof(double), cudaMemcpyHostToDevice));
+            HP_CK(cudaMemcpyAsync(dd.p, d, n * sizeof(double), cudaMemcpyHostToDevice, st()));
             if (outflow) {
                 dq.alloc(2 * n);
-                HP_CK(cudaMemcpy(dq.p, outflow, 2 * n * sizeof(double), cudaMemcpyHostToDevice));
+                HP_CK(cudaMemcpyAsync(dq.p, outflow, 2 * n * sizeof(double), cudaMemcpyHostToDevice, st()));
             }
             k_build_state<R><<<blocks_for(n), kThreads, 0, st()>>>(n, dd.p, outflow ? dq.p : nullptr, res,
                                                                     st4[hs.cur].p);
@@ -745,7 +745,8 @@ template <typename R> struct Impl : Base {
         for (size_t k = 0; k < n; ++k) depth_mm[k] = double(v[k]) * 1000.0;
         if (t_min) {
             double t = 0;
-            HP_CK(cudaMemcpy(&t, rec.snap_t + slot, sizeof(double), cudaMemcpyDeviceToHost));
+            HP_CK(cudaMemcpyAsync(&t, rec.snap_t + slot, sizeof(double), cudaMemcpyDeviceToHost, st()));
+            HP_CK(cudaStreamSynchronize(st()));
             *t_min = t;
         }
         return HP2D_OK;
