@@ -161,6 +161,27 @@ template <typename R> struct Impl : Base {
     bool static_ready = false, dirty = true;
     double last_dt_s = 0;
     int rows_per_warp = 64;
+    bool rpw_chosen = false;   // set by hp2d_set_tuning / hp2d_autotune / an ensemble
+    int n_sms = 0;
+    // Rows per warp when none was chosen.  FP32 two-cell strips: of 40, 32, 24 and 16 rows the
+    // one that best fills whole waves of resident CTAs (4 per SM) after the 4 halo rows per
+    // block -- on a 4096 x 8192 grid 40 (3528 CTAs, 5.96 waves), on 2048 x 2048 32 (560 CTAs,
+    // one wave; 40 rows leave 455 CTAs for 592 slots).  Other layouts keep rows_per_warp.
+    int default_rows(int cpl) {
+        if (sizeof(R) != 4 || cpl != 2) return rows_per_warp;
+        if (!n_sms) HP_CK(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        const double slots = double(FusedOcc<float, 2>::minb) * n_sms;
+        const int strips = (nx + 59) / 60;
+        int best = rows_per_warp;
+        double best_score = -1.0;
+        for (int r : {40, 32, 24, 16}) {
+            const double ctas = std::ceil(double(strips) * ((ny + r - 1) / r) / 4.0);
+            const double waves = std::ceil(ctas / slots);
+            const double score = ctas / (waves * slots) * double(r) / double(r + 4);
+            if (score > best_score + 1e-12) { best_score = score; best = r; }
+        }
+        return best;
+    }
     int cells_per_lane = 1;   // fused-step layout: 1 (32-column strips) or 2 (64-column strips)
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -892,7 +913,7 @@ template <typename R> struct Impl : Base {
         a.flag_critical = p.flag_critical; a.outlet_type = p.outlet_type; a.ga = ga() ? 1 : 0;
         const int out_cols = 32 * cpl - 4;   // a strip's output columns (2-column apron each side)
         a.n_strips = (nx + out_cols - 1) / out_cols;
-        const int rpw = rows_per_warp;
+        const int rpw = rpw_chosen ? rows_per_warp : default_rows(cpl);
         a.rows_per_warp = rpw;
         a.n_warps_total = a.n_strips * ((ny + rpw - 1) / rpw);
         a.n_ctas = unsigned((a.n_warps_total + kThreads / 32 - 1) / (kThreads / 32));
@@ -1091,7 +1112,9 @@ template <typename R> struct Impl : Base {
         prologue();
         Snapshot snap;
         take(snap);
-        const int cands[] = {16, 24, 32, 48, 64, 96, 128};
+        const int cands[] = {16, 24, 32, 40, 48, 64, 96, 128};
+        if (!rpw_chosen) rows_per_warp = default_rows(cells_per_lane);
+        rpw_chosen = true;
         const int keep = rows_per_warp, keep_cpl = cells_per_lane;
         int best = keep, best_cpl = keep_cpl;
         float best_ms = std::numeric_limits<float>::infinity();
@@ -1390,8 +1413,9 @@ struct hp2d_ensemble {
                 return HP2D_INVALID_ARG;
             }
             HP_CK(cudaSetDevice(device));
-            if (im.rows_per_warp != rows_per_warp) {
+            if (im.rows_per_warp != rows_per_warp || !im.rpw_chosen) {
                 im.rows_per_warp = rows_per_warp;
+                im.rpw_chosen = true;
                 im.invalidate_graph();
             }
             im.prologue();
@@ -1740,6 +1764,7 @@ hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp) {
     if (rows_per_warp < 4) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) {
         m.rows_per_warp = rows_per_warp;
+        m.rpw_chosen = true;
         m.invalidate_graph();
         return HP2D_OK;
     });
