@@ -101,6 +101,20 @@ __device__ __host__ inline double finalize_dt(double vmax, double cmax, double r
     return fmin(tcr, max_dt);
 }
 
+// compensated (Kahan) running sum: s + c tracks the exact sum of the added terms to about one
+// rounding of the state precision, however many terms (the library builds without contraction,
+// so the compensation is not folded away)
+template <typename R> struct Kahan {
+    R s = R(0), c = R(0);
+    __device__ __forceinline__ void add(R x) {
+        const R y = x - c;
+        const R t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return double(s) - double(c); }
+};
+
 template <typename R> __device__ __forceinline__ R warp_max(R v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -221,7 +235,9 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     const int wg = int(blk) * (NT / 32) + warp;
 
     double rain_acc = 0.0, inf_acc = 0.0, out_acc = 0.0;
-    R rain_acc_r = R(0), inf_acc_r = R(0), out_acc_r = R(0);   // per-lane partial sums (ledger only)
+    // per-lane partial sums of the volume ledger in the state precision, Kahan-compensated
+    // (the warps' sums and everything after them are FP64)
+    Kahan<R> rain_acc_r, inf_acc_r, out_acc_r;
     unsigned dry = 0u;                        // bit i: row r-i dry across the strip
     R s2max = R(0);
     R cmaxv = R(-1);   // largest celerity term of a non-stagnant cell (-1: none yet)
@@ -345,7 +361,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     hh = hh + rr;
                     const bool own = own_lane[h] && own_row;
                     // uniform rain volume comes from the count of finite cells at the end
-                    if (MAP && own && isfinite(hh)) rain_acc_r += rr;
+                    if (MAP && own && isfinite(hh)) rain_acc_r.add(rr);
                     if (INF) {
                         const unsigned sc = meta[h] & 255u;
                         V2 go = Gs;
@@ -356,7 +372,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                                                   : vg_infiltration(hh, Ic, Tc, a.classes_vg[sc], a.vg, K);
                             go.x = Ic;
                             go.y = Tc;
-                            if (own && isfinite(fd)) inf_acc_r += fd;
+                            if (own && isfinite(fd)) inf_acc_r.add(fd);
                         }
                         if (own) gout[c] = go;
                     }
@@ -469,7 +485,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         hf3 = ho;
                         a.hf3[o] = ho;
                         a.qo[o] = qq;
-                        out_acc_r += qq * K.dt;
+                        out_acc_r.add(qq * K.dt);
                         // the next step's clamp is skipped when an outlet cell (outside the
                         // infiltrating soils) stays negative after the next rain
                         // (Hydrological_Model.m:45-50); only outlet cells can end negative
@@ -542,9 +558,9 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     // ---- CTA reductions ---------------------------------------------------------------
     // (the last CTA reads only the step accumulators, which thread 0 publishes before its
     // ticket; the state records reach the next launch through the kernel boundary)
-    rain_acc += double(rain_acc_r);
-    inf_acc += double(inf_acc_r);
-    out_acc += double(out_acc_r);
+    rain_acc += rain_acc_r.value();
+    inf_acc += inf_acc_r.value();
+    out_acc += out_acc_r.value();
     const int lane_ = tid & 31, warp_ = tid >> 5;
     s2max = warp_max(s2max);
     // 0: no non-stagnant cell; else the bits of the (non-negative, +0 for -0) maximum + 1

@@ -166,6 +166,28 @@ def inflow_case(ny: int = 96, nx: int = 96, dx: float = 10.0, minutes: float = 4
                 np.zeros((ny, nx)), inflow=inflow)
 
 
+def breach_inflow_case(ny: int = 128, nx: int = 512, dx: float = 5.0, seed: int = 11, minutes: float = 30.0,
+                       breach_factor: float = 0.5, reservoir_depth: float = 20.0) -> Case:
+    """The dam-break valley, dry, fed at its upstream edge by the breach outflow of a
+    rectangular reservoir (``breach.breach_hydrograph_cav``: depth ``reservoir_depth``, dam length
+    the valley width, breach ``breach_factor`` of it, 2 km^2 of surface, 1-min samples), as
+    HydroPol2D_Main_While_Ensemble.m:141-160 feeds its breach members.  The inflow cells are the
+    first column's cells within 2 m of the thalweg's elevation."""
+    from .breach import breach_hydrograph_cav, inflow_table
+    c = dambreak_case(ny, nx, dx, seed=seed, hours=minutes / 60.0)
+    W = ny * dx
+    area = 2.0e6
+    t_min, q, _ = breach_hydrograph_cav(reservoir_depth, W, breach_factor * W, 60.0, minutes * 60.0,
+                                        lambda h: area, lambda h: area * h)
+    z0 = c.z[:, 0]
+    rows = np.nonzero(z0 <= z0.min() + 2.0)[0]
+    c.d0 = np.zeros_like(c.d0)
+    c.inflow = inflow_table(t_min, q, rows, np.zeros(rows.size, np.int32), dx)
+    c.name = f"breach_inflow_{ny}x{nx}"
+    c.meta = dict(peak_m3s=float(q.max()), inflow_cells=int(rows.size))
+    return c
+
+
 def urban_case(n: int = 2048, dx: float = 2.0, seed: int = 7, hours: float = 2.0) -> Case:
     rng = np.random.default_rng(seed)
     grf = gaussian_random_field(n, n, -3.0, seed)

@@ -153,3 +153,16 @@ def test_stage_and_inflow_together(hp2d_lib, oracle_lib):
     assert_same_state(g, o, FIELDS)
     assert_same_clock(g, o)
     assert g.diag()["inflow_volume"] > 0 and g.diag()["stage_volume"] > 0
+
+
+def test_breach_hydrograph_member(hp2d_lib, oracle_lib):
+    """A dam-break member fed by the breach outflow hydrograph through the inflow cells."""
+    case = S.breach_inflow_case(64, 256, minutes=6.0)
+    assert case.meta["inflow_cells"] >= 1
+    g, o = make_pair(case, "fp32")
+    for chunk in (10, 200, 400):
+        g.fused_steps(chunk)
+        o.fused_steps(chunk)
+        assert_same_state(g, o, FIELDS, f"after chunk {chunk}")
+        assert_same_clock(g, o)
+    assert g.diag()["inflow_volume"] > 0
