@@ -38,6 +38,7 @@ EXPORTS = [
     "hp2d_create", "hp2d_destroy", "hp2d_last_error", "hp2d_create_error",
     "hp2d_upload_static", "hp2d_set_soil", "hp2d_set_soil_vg", "hp2d_set_state", "hp2d_set_clock", "hp2d_set_rain_clock",
     "hp2d_set_rain_uniform", "hp2d_set_rain_maps", "hp2d_set_rain_gauges", "hp2d_set_inflow", "hp2d_set_stage",
+    "hp2d_set_reservoirs",
     "hp2d_set_map_records", "hp2d_map_records", "hp2d_download_map_record", "hp2d_hydrology_step", "hp2d_li_step",
     "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed",
     "hp2d_set_tuning", "hp2d_set_layout", "hp2d_run",
@@ -90,6 +91,7 @@ class Diag(C.Structure):
         ("status_bits", C.c_int64),
         ("rain_t0", C.c_double), ("rain_t1", C.c_double), ("t_previous", C.c_double),
         ("inflow_volume", C.c_double), ("stage_volume", C.c_double),
+        ("structure_volume", C.c_double),
     ]
 
 
@@ -138,6 +140,9 @@ def lib() -> C.CDLL:
         "hp2d_set_map_records": ([vp, C.c_int32, P(C.c_double), C.c_int32], C.c_int),
         "hp2d_set_stage": ([vp, C.c_int32, C.c_int32, P(C.c_double), P(C.c_double), C.c_int32,
                             P(C.c_int32), P(C.c_int32), P(C.c_int32)], C.c_int),
+        "hp2d_set_reservoirs": ([vp, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_double), P(C.c_double),
+                                 P(C.c_double), P(C.c_int32), P(C.c_int32), P(C.c_double), P(C.c_double),
+                                 P(C.c_double), P(C.c_int32), P(C.c_int32)], C.c_int),
         "hp2d_set_rain_gauges": ([vp, C.c_int32, P(C.c_double), P(C.c_double), C.c_int32, C.c_double,
                                   P(C.c_double), C.c_double, C.c_double], C.c_int),
         "hp2d_map_records": ([vp, P(C.c_int64)], C.c_int),

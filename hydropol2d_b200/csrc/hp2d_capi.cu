@@ -309,6 +309,8 @@ template <typename R> struct Impl : Base {
         inflow.n_stage = 0;
         inflow_cells_h = BcCells{};
         stage_cells_h = BcCells{};
+        strct = StructDesc<R>{};   // the structures' cells are set anew too
+        struct_cells_h.clear();
         std::vector<int32_t> cells(n_out);
         std::vector<R> coefs(n_out);
         std::vector<uint32_t> bits(size_t(ny) * bit_words, 0u);
@@ -616,11 +618,12 @@ template <typename R> struct Impl : Base {
             if (per[k].empty() && stg[k] < 0) used.push_back(k);
             stg[k] = std::max(stg[k], stage_cells_h.gauge[q]);
         }
+        for (size_t q = 0; q < struct_cells_h.size(); ++q) used.push_back(struct_cells_h[q]);
         for (size_t k = 0; k < n; ++k)
             if (host_meta[k] & kInflowBit) host_meta[k] &= 255u;
         std::sort(used.begin(), used.end());
         used.erase(std::unique(used.begin(), used.end()), used.end());
-        std::vector<int32_t> off(1, 0), gl, st;
+        std::vector<int32_t> off(1, 0), gl, st, ss;
         host_gcells.assign(size_t(ng), 0.0);
         for (size_t e = 0; e < used.size(); ++e) {
             const size_t k = used[e];
@@ -632,15 +635,19 @@ template <typename R> struct Impl : Base {
             }
             off.push_back(int32_t(gl.size()));
             st.push_back(stg[k]);
+            const auto it = std::find(struct_cells_h.begin(), struct_cells_h.end(), k);
+            ss.push_back(it == struct_cells_h.end() ? -1 : int32_t(it - struct_cells_h.begin()));
             host_meta[k] = (host_meta[k] & 255u) | kInflowBit | (uint32_t(e) << 8);
         }
         write_meta();
         inf_off.alloc(off.size());
         inf_gauge.alloc(std::max<size_t>(gl.size(), 1));
         bc_stage.alloc(std::max<size_t>(st.size(), 1));
+        bc_struct.alloc(std::max<size_t>(ss.size(), 1));
         upload(inf_off.p, off);
         if (!gl.empty()) upload(inf_gauge.p, gl);
         if (!st.empty()) upload(bc_stage.p, st);
+        if (!ss.empty()) upload(bc_struct.p, ss);
         if (ng) {
             inf_cells.alloc(size_t(ng));
             upload(inf_cells.p, host_gcells);
@@ -648,6 +655,7 @@ template <typename R> struct Impl : Base {
         inflow.cell_off = inf_off.p;
         inflow.cell_gauge = inf_gauge.p;
         inflow.cell_stage = bc_stage.p;
+        inflow.cell_struct = bc_struct.p;
         inflow.gauge_cells = inf_cells.p;
         invalidate_graph();
         dirty = true;
@@ -711,6 +719,85 @@ template <typename R> struct Impl : Base {
         inflow.stage_d = stage_d.p;
         inflow.stage_now = stage_now.p;
         stage_cells_h = std::move(cells);
+        rebuild_bc_cells();
+        return HP2D_OK;
+    }
+
+    // Reservoir / control structures (flag_reservoir, Local_Inertial_Model_D4.m:318-344):
+    // structure i drains cell (res_row, res_col) through rating curve (k1, h1, k2) into
+    // (ds1_row, ds1_col) and, when ds2_row >= 0, through (k3, h2, k4) into (ds2_row, ds2_col);
+    // 0-based cells, ds1_row < 0 for none.  n = 0 removes them.
+    StructDesc<R> strct{};
+    std::vector<size_t> struct_cells_h;   // slot -> cell
+    Dev<double> st_coef, st_acc;
+    Dev<int32_t> st_slot, st_slot_cell, bc_struct;
+    Dev<R> st_hres, st_extra;
+
+    hp2d_status set_reservoirs(int32_t ns, const int32_t* rr, const int32_t* rc, const double* k1, const double* h1,
+                               const double* k2, const int32_t* d1r, const int32_t* d1c, const double* k3,
+                               const double* h2, const double* k4, const int32_t* d2r, const int32_t* d2c) {
+        if (!static_ready) { ctx->err = "hp2d_upload_static must come before hp2d_set_reservoirs"; return HP2D_NOT_READY; }
+        if (ns < 0) { ctx->err = "negative structure count"; return HP2D_INVALID_ARG; }
+        if (ns > 0 && ctx->p.flag_reservoir != 1) { ctx->err = "structures need flag_reservoir = 1"; return HP2D_INVALID_ARG; }
+        std::vector<size_t> cells;
+        std::vector<int32_t> slot(size_t(ns) * 3, -1);
+        std::vector<double> coef(size_t(ns) * 6);
+        auto slot_of = [&](int32_t r, int32_t c, int32_t& out) -> hp2d_status {
+            if (r < 0 || r >= ny || c < 0 || c >= nx) { ctx->err = "structure cell out of range"; return HP2D_INVALID_ARG; }
+            const size_t k = size_t(r) * nx + c;
+            if (!(host_meta[k] & kInflowBit) && (host_meta[k] >> 8) != 0u) {
+                ctx->err = "an outlet cell cannot also be a structure cell";
+                return HP2D_INVALID_ARG;
+            }
+            if (!std::isfinite(host_z[k])) { ctx->err = "a structure cell needs a finite elevation"; return HP2D_INVALID_ARG; }
+            auto it = std::find(cells.begin(), cells.end(), k);
+            out = int32_t(it - cells.begin());
+            if (it == cells.end()) cells.push_back(k);
+            return HP2D_OK;
+        };
+        for (int i = 0; i < ns; ++i) {
+            const double cf[6] = {k1[i], h1[i], k2[i], k3[i], h2[i], k4[i]};
+            for (int q = 0; q < 6; ++q) coef[size_t(i) * 6 + q] = cf[q];
+            hp2d_status s = slot_of(rr[i], rc[i], slot[3 * i]);
+            if (s != HP2D_OK) return s;
+            if (d1r[i] >= 0) {
+                if (!(std::isfinite(k1[i]) && std::isfinite(h1[i]) && std::isfinite(k2[i]))) {
+                    ctx->err = "non-finite rating curve";
+                    return HP2D_INVALID_ARG;
+                }
+                if ((s = slot_of(d1r[i], d1c[i], slot[3 * i + 1])) != HP2D_OK) return s;
+            }
+            if (d2r[i] >= 0) {
+                // the reference indexes ds1 in the second structure's branch
+                if (d1r[i] < 0) { ctx->err = "a second structure needs a first downstream cell"; return HP2D_INVALID_ARG; }
+                if (!(std::isfinite(k3[i]) && std::isfinite(h2[i]) && std::isfinite(k4[i]))) {
+                    ctx->err = "non-finite rating curve";
+                    return HP2D_INVALID_ARG;
+                }
+                if ((s = slot_of(d2r[i], d2c[i], slot[3 * i + 2])) != HP2D_OK) return s;
+            }
+        }
+        if (inflow_cells_h.cell.size() + stage_cells_h.cell.size() + cells.size() >= (1u << 23)) {
+            ctx->err = "too many boundary cells";
+            return HP2D_INVALID_ARG;
+        }
+        strct = StructDesc<R>{};
+        if (ns > 0) {
+            const size_t m = cells.size();
+            st_coef.alloc(coef.size());
+            st_slot.alloc(slot.size());
+            st_slot_cell.alloc(m);
+            st_hres.alloc(size_t(ns));
+            st_acc.alloc(2 * m);
+            st_extra.alloc(m);
+            upload(st_coef.p, coef);
+            upload(st_slot.p, slot);
+            std::vector<int32_t> sc32(cells.begin(), cells.end());
+            upload(st_slot_cell.p, sc32);
+            fill(st_extra.p, m, R(0));
+            strct = StructDesc<R>{ns, int(m), st_coef.p, st_slot.p, st_slot_cell.p, st_hres.p, st_acc.p, st_extra.p};
+        }
+        struct_cells_h = std::move(cells);
         rebuild_bc_cells();
         return HP2D_OK;
     }
@@ -849,6 +936,10 @@ template <typename R> struct Impl : Base {
         HP_CK(cudaGetLastError());
         k_limit<R><<<nb, kThreads, 0, st()>>>(gv, qxu.p, qyu.p, scale.p, qx.p, qy.p);
         HP_CK(cudaGetLastError());
+        if (strct.n) {
+            k_struct_unfused<R><<<1, 32, 0, st()>>>(strct, h.p, time_step, res * res, sc.p);
+            HP_CK(cudaGetLastError());
+        }
         k_continuity<R><<<nb, kThreads, 0, st()>>>(gv, dts, h.p, qx.p, qy.p);
         HP_CK(cudaGetLastError());
         if (n_out) {
@@ -930,6 +1021,7 @@ template <typename R> struct Impl : Base {
         a.rain = rain;
         a.inflow = inflow;
         a.rec = rec;
+        a.strct = strct;
         a.sc = sc.p;
         return a;
     }
@@ -959,7 +1051,7 @@ template <typename R> struct Impl : Base {
         k_fused_step<R, kThreads, INF, MAP, CPL, INFL><<<a.n_ctas, kThreads, sm, st()>>>(a);
     }
     template <int INF, int CPL> void launch_i(const FusedArgs<R>& a) {
-        const bool map = rain.n_maps > 0, infl = inflow.n_gauges > 0 || inflow.n_stage > 0;
+        const bool map = rain.n_maps > 0, infl = bc_kernel();
         if (map) {
             if (infl) launch_one<INF, true, CPL, true>(a); else launch_one<INF, true, CPL, false>(a);
         } else {
@@ -976,6 +1068,14 @@ template <typename R> struct Impl : Base {
     void launch_fused(const FusedArgs<R>& a) {
         if (cells_per_lane == 2) launch_fused_t<2>(a);
         else launch_fused_t<1>(a);
+    }
+
+    // the fused kernel variant with boundary-condition cells (inflow, stage, structures)
+    bool bc_kernel() const { return inflow.n_gauges > 0 || inflow.n_stage > 0 || strct.n > 0; }
+
+    template <int INF> void struct_prime_t(const FusedArgs<R>& a) {
+        if (rain.n_maps > 0) k_struct_prime<R, INF, true><<<1, kThreads, 0, st()>>>(a);
+        else k_struct_prime<R, INF, false><<<1, kThreads, 0, st()>>>(a);
     }
 
     void invalidate_graph() {
@@ -998,6 +1098,15 @@ template <typename R> struct Impl : Base {
         HP_CK(cudaGetLastError());
         if (inflow.n_gauges || inflow.n_stage) {
             k_inflow_depth<R><<<1, kThreads, 0, st()>>>(inflow, sc.p);
+            HP_CK(cudaGetLastError());
+        }
+        if (strct.n) {   // after the gauge depths and the skip flag it reads
+            const FusedArgs<R> a = fused_args();
+            switch (inf_mode()) {
+                case 1: struct_prime_t<1>(a); break;
+                case 2: struct_prime_t<2>(a); break;
+                default: struct_prime_t<0>(a);
+            }
             HP_CK(cudaGetLastError());
         }
         dirty = false;
@@ -1288,6 +1397,7 @@ template <typename R> struct Impl : Base {
         o->t_previous = hs.t_prev;
         o->inflow_volume = hs.inflow_vol;
         o->stage_volume = hs.stage_vol;
+        o->structure_volume = hs.struct_vol;
         o->max_velocity = hs.vmax_last;
         o->rain_volume = hs.rain_vol;
         o->infiltration_volume = hs.inf_vol;
@@ -1407,7 +1517,7 @@ struct hp2d_ensemble {
             }
             const int mga = im.inf_mode(), mmap = im.rain.n_maps > 0 ? 1 : 0;
             if (m == 0) { ga = mga; map = mmap; infl = false; }
-            if (im.inflow.n_gauges > 0 || im.inflow.n_stage > 0) infl = true;
+            if (im.bc_kernel()) infl = true;
             if (mga != ga || mmap != map) {
                 err = "members must agree on the infiltration model and on the kind of rain forcing";
                 return HP2D_INVALID_ARG;
@@ -1581,7 +1691,7 @@ hp2d_status hp2d_create(const hp2d_grid* grid, const hp2d_params* params, int32_
     if (grid->precision != HP2D_FP32 && grid->precision != HP2D_FP64) { g_create_error = "precision must be HP2D_FP32 or HP2D_FP64"; return HP2D_INVALID_ARG; }
     if (p.flag_subgrid != 0) { g_create_error = "flag_subgrid=1 is not supported"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_D8 != 0) { g_create_error = "flag_D8=1 is not supported"; return HP2D_UNSUPPORTED_FLAG; }
-    if (p.flag_reservoir != 0) { g_create_error = "flag_reservoir=1 is not supported"; return HP2D_UNSUPPORTED_FLAG; }
+    if (p.flag_reservoir != 0 && p.flag_reservoir != 1) { g_create_error = "flag_reservoir must be 0 or 1"; return HP2D_INVALID_ARG; }
     if (p.flag_numerical_scheme != 1) { g_create_error = "only flag_numerical_scheme=1 (Bates) is supported"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_infiltration < 0 || p.flag_infiltration > 2) { g_create_error = "flag_infiltration must be 0, 1 (Green-Ampt) or 2 (van Genuchten)"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_critical != 0 && p.flag_critical != 1) { g_create_error = "flag_critical must be 0 or 1"; return HP2D_INVALID_ARG; }
@@ -1693,6 +1803,18 @@ hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count) {
 hp2d_status hp2d_download_map_record(hp2d_ctx* ctx, int64_t index, double* depth_mm, double* t_min) {
     if (!depth_mm) return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) { return m.download_map_record(index, depth_mm, t_min); });
+}
+
+hp2d_status hp2d_set_reservoirs(hp2d_ctx* ctx, int32_t n, const int32_t* res_row, const int32_t* res_col,
+                                const double* k1, const double* h1, const double* k2, const int32_t* ds1_row,
+                                const int32_t* ds1_col, const double* k3, const double* h2, const double* k4,
+                                const int32_t* ds2_row, const int32_t* ds2_col) {
+    if (n > 0 && (!res_row || !res_col || !k1 || !h1 || !k2 || !ds1_row || !ds1_col || !k3 || !h2 || !k4 || !ds2_row ||
+                  !ds2_col))
+        return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) {
+        return m.set_reservoirs(n, res_row, res_col, k1, h1, k2, ds1_row, ds1_col, k3, h2, k4, ds2_row, ds2_col);
+    });
 }
 
 hp2d_status hp2d_set_stage(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, const double* t_start,

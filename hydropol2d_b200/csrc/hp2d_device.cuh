@@ -154,6 +154,7 @@ struct StepScalars {
     // t_save, records taken, and whether the next step's input depth is to be recorded
     long long rec_count;
     int rec_last, rec_pending;
+    double struct_vol;     // cumulative volume the control structures added [m^3]
 };
 
 // ---------------- map records (save_output_maps.m) -----------------------------------
@@ -340,6 +341,7 @@ template <typename R> struct InflowDesc {
     const double* stage_d;      // [n_stage_times][n_stage] water depth [m]
     R* stage_now;               // [n_stage] this step's stage depth [m]
     const int32_t* cell_stage;  // [entries]
+    const int32_t* cell_struct; // [entries] control-structure slot of the cell (-1: none)
 };
 // stage depth of gauge g at clock t: the last record starting at or before t, else the
 // first (update_spatial_BC.m:322-330)
@@ -373,6 +375,65 @@ template <typename R> __device__ __forceinline__ void add_inflow(const InflowDes
     R v = R(0);
     for (int q = q0; q < q1; ++q) v = v + d.depth[d.cell_gauge[q]];
     hh = hh + v;
+}
+// ---------------- reservoir / control structures (flag_reservoir) ----------------------
+// Local_Inertial_Model_D4.m:318-344: structure i drains its reservoir cell through up to two
+// rating curves Q = k (h - h_crest)^p into downstream cells ds1 and ds2, once per step, from
+// the depth d_tot entering the step's fluxes.  As the reference, in structure order:
+//   dtsup = d_tot(res)/1000 (with the earlier structures' additions to d_tot);
+//   dh = min(k1 max(dtsup-h1,0)^k2 / A 1000 3600, 1000 max(dtsup-h1,0)/dt_h) dt_h [mm];
+//   Vol_Flux(res) += dh/1000 A (the reservoir cell GAINS dh: the reference's sign);
+//   dtsup -= dh/1000; d_tot(ds1) += dh; with a second structure d_tot(ds1) += dh again (the
+//   reference adds the first transfer twice), then dh2 from (h2, k3, k4) as above,
+//   Vol_Flux(res) += dh2/1000 A, d_tot(ds2) += dh2.
+// Every addition lands in d_t = d_tot + 1000 Vol_Flux / A after the fluxes, so each taking
+// cell ("slot") gets one extra depth that enters its continuity: hn = (h + extra) + flux term.
+template <typename R> struct StructDesc {
+    int n, n_slots;
+    const double* coef;       // [n][6]: k1, h1, k2, k3, h2, k4
+    const int32_t* slot;      // [n][3]: slot of the reservoir, ds1 and ds2 cells (-1: none)
+    const int32_t* slot_cell; // [n_slots] linear cell index
+    R* hres;                  // [n] depth of the reservoir cell entering the step [m] (scratch)
+    double* acc;              // [2][n_slots] ds additions, Vol_Flux additions [mm] (scratch)
+    R* extra;                 // [n_slots] the step's extra depth of the cell [m]
+};
+// time_step [min] of the step; area = cell area [m^2]; fills s.extra from s.hres; returns
+// the volume [m^3] the extras add
+template <typename R>
+__device__ __host__ inline double structure_transfers(const StructDesc<R>& s, double time_step, double area) {
+    double* ds = s.acc;
+    double* rv = s.acc + s.n_slots;
+    for (int q = 0; q < s.n_slots; ++q) ds[q] = rv[q] = 0.0;
+    const double dt_h = time_step / 60.0;
+    for (int i = 0; i < s.n; ++i) {
+        const double* c = s.coef + 6 * size_t(i);
+        const int sr = s.slot[3 * i], s1 = s.slot[3 * i + 1], s2 = s.slot[3 * i + 2];
+        double dh = 0.0, dtsup = 0.0;
+        if (s1 >= 0) {
+            dtsup = (double(s.hres[i]) * 1000.0 + ds[sr]) / 1000.0;
+            const double q = fmax(dtsup - c[1], 0.0);
+            const double avail = 1000.0 * q / dt_h;
+            dh = fmin(c[0] * pow(q, c[2]) / area * 1000.0 * 3600.0, avail) * dt_h;
+            rv[sr] += dh;
+            dtsup = dtsup - dh / 1000.0;
+            ds[s1] += dh;
+        }
+        if (s2 >= 0) {
+            ds[s1] += dh;
+            const double q = fmax(dtsup - c[4], 0.0);
+            const double avail = 1000.0 * q / dt_h;
+            const double dh2 = fmin(c[3] * pow(q, c[5]) / area * 1000.0 * 3600.0, avail) * dt_h;
+            rv[sr] += dh2;
+            ds[s2] += dh2;
+        }
+    }
+    double vol = 0.0;
+    for (int q = 0; q < s.n_slots; ++q) {
+        const R e = R((ds[q] + rv[q]) / 1000.0);
+        s.extra[q] = e;
+        vol += double(e) * area;
+    }
+    return vol;
 }
 // outlet entry + 1 of a meta word (0: not an outlet)
 __device__ __host__ inline unsigned outlet_ord(unsigned meta) { return (meta & kInflowBit) ? 0u : meta >> 8; }

@@ -80,6 +80,7 @@ template <typename R> struct FusedArgs {
     RainDesc rain;
     InflowDesc<R> inflow;
     RecordDesc<R> rec;
+    StructDesc<R> strct;         // reservoir / control structures (n = 0: none)
     StepScalars* sc;
 };
 
@@ -178,6 +179,39 @@ template <int CPL> struct FusedOcc<double, CPL> { static constexpr int minb = CP
 // INF: infiltration model (0 none, 1 Green-Ampt, 2 van Genuchten); MAP: rain from coarse
 // maps (else a uniform rate); INFL: inflow hydrographs present (the grids without them do not
 // carry the lookup)
+// The depth d_tot a step hands to its fluxes at each control structure's reservoir cell --
+// phase (A) of that cell restated: rain, infiltration, inflow, clamps, from the state and
+// soil records `st`/`gs` the step starts from -- then the structures' transfers (one thread,
+// in structure order).  The last CTA of a step runs it for the next step; k_struct_prime for
+// the first step of a call.
+template <typename R, int INF, bool MAP, bool INFL>
+__device__ __noinline__ void structure_prepare(const FusedArgs<R>& a, const RainStep<R>& rs, bool skip,
+                                               const StepConsts<R>& K, const typename Vec<R>::V4* st,
+                                               const typename Vec<R>::V2* gs, int tid, int nt, double time_step) {
+    for (int i = tid; i < a.strct.n; i += nt) {
+        const int c = a.strct.slot_cell[a.strct.slot[3 * i]];
+        const int r = c / a.nx, j = c % a.nx;
+        R hh = st[c].x;
+        const R rr = MAP ? rs.at(a.rain, r, j, a.ny, a.nx) : rs.depth;
+        hh = hh + rr;
+        const unsigned meta = meta_bits(a.stat[c].w);
+        if (INF) {
+            const unsigned scl = meta & 255u;
+            if (scl != 255u) {
+                R Ic = gs[c].x, Tc = gs[c].y;
+                if (INF == 1) green_ampt(hh, Ic, Tc, a.classes[scl], K);
+                else vg_infiltration(hh, Ic, Tc, a.classes_vg[scl], a.vg, K);
+            }
+        }
+        if (INFL) add_inflow(a.inflow, meta, hh);
+        if (!skip && hh < R(1e-9)) hh = R(0);
+        if (hh < R(0)) hh = R(0);
+        a.strct.hres[i] = hh;
+    }
+    __syncthreads();
+    if (tid == 0) structure_transfers(a.strct, time_step, a.res * a.res);
+}
+
 template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>
 __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned blk) {
     using V4 = typename Vec<R>::V4;
@@ -475,7 +509,14 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             for (int h = 0; h < CPL; ++h) {
                 if (own_lane[h] && frow) {
                     const size_t c2 = size_t(rm2) * nx + j[h];
-                    R hn = quiet ? hT2[h] + R(0) : continuity(hT2[h], qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
+                    // a control structure's transfers join the depth after the fluxes
+                    // (Local_Inertial_Model_D4.m:318-344, :390)
+                    R h_in = hT2[h];
+                    if (INFL && (mt2[h] & kInflowBit)) {
+                        const int ss = a.inflow.cell_struct[(mt2[h] >> 8) & 0x7FFFFFu];
+                        if (ss >= 0) h_in = h_in + a.strct.extra[ss];
+                    }
+                    R hn = quiet ? h_in + R(0) : continuity(h_in, qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
                     R hf3 = R(0);
                     const unsigned ord = outlet_ord(mt2[h]);
                     if (ord) {
@@ -652,6 +693,11 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             sc->stage_vol += __ldcg(&sc->acc_stage) * area;
             sc->acc_stage = 0.0;
         }
+        if (INFL && a.strct.n) {   // the structures' extras this step applied
+            double v = 0.0;
+            for (int q = 0; q < a.strct.n_slots; ++q) v += double(a.strct.extra[q]) * area;
+            sc->struct_vol += v;
+        }
         // the next step's rain: update_spatial_BC over [t_previous, t]
         // (HydroPol2D_Main_While.m:721), then t_previous <- the clock increment on the first
         // step and t after it (:734-738), and the clock advances by the new step (:779)
@@ -685,6 +731,21 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         for (int g = tid; g < a.inflow.n_gauges; g += NT)
             a.inflow.depth[g] = R(inflow_integral(a.inflow, g, ra, rb) / 60000.0);
         for (int g = tid; g < a.inflow.n_stage; g += NT) a.inflow.stage_now[g] = R(stage_at(a.inflow, g, tn));
+    }
+    if constexpr (INFL) {
+        if (a.strct.n) {   // the next step's structure transfers, from its d_tot
+            __syncthreads();
+            __shared__ StepConsts<R> s_Kn;
+            __shared__ int s_skn;
+            __shared__ double s_tsn;
+            if (tid == 0) {
+                s_tsn = a.sc->time_step;
+                s_Kn.make(s_tsn * 60.0, a.res, a.tol_mm, a.thr_mm);
+                s_skn = a.sc->skip_clamp;
+            }
+            __syncthreads();
+            structure_prepare<R, INF, MAP, INFL>(a, s_rsn, s_skn != 0, s_Kn, sout, gout, tid, NT, s_tsn);
+        }
     }
     return cta_ok;
 }
@@ -778,6 +839,26 @@ template <typename R> __global__ void k_inflow_depth(InflowDesc<R> d, const Step
     for (int g = threadIdx.x; g < d.n_gauges; g += blockDim.x)
         d.depth[g] = R(inflow_integral(d, g, ra, rb) / 60000.0);
     for (int g = threadIdx.x; g < d.n_stage; g += blockDim.x) d.stage_now[g] = R(stage_at(d, g, t));
+}
+
+// the structure transfers of the first fused step of a call (one block)
+template <typename R, int INF, bool MAP>
+__global__ void k_struct_prime(const FusedArgs<R> a) {
+    __shared__ RainStep<R> s_r;
+    __shared__ StepConsts<R> s_k;
+    __shared__ int s_skip, s_cur;
+    __shared__ double s_ts;
+    if (threadIdx.x == 0) {
+        const StepScalars* sc = a.sc;
+        s_r.make(a.rain, sc->rain_a, sc->rain_b);
+        s_ts = sc->time_step;
+        s_k.make(s_ts * 60.0, a.res, a.tol_mm, a.thr_mm);
+        s_skip = sc->skip_clamp;
+        s_cur = sc->cur;
+    }
+    __syncthreads();
+    structure_prepare<R, INF, MAP, true>(a, s_r, s_skip != 0, s_k, s_cur ? a.st1 : a.st0, s_cur ? a.gs1 : a.gs0,
+                                         threadIdx.x, blockDim.x, s_ts);
 }
 
 template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>

@@ -130,6 +130,16 @@ __global__ void k_continuity(GridView<R> g, double dt_s, R* h, const R* qx, cons
     }
 }
 
+// control-structure transfers of an unfused step (Local_Inertial_Model_D4.m:318-344), one
+// thread: from the d_tot the fluxes used, the extras join h before the continuity kernel
+template <typename R>
+__global__ void k_struct_unfused(StructDesc<R> s, R* h, double time_step, double area, StepScalars* sc) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = 0; i < s.n; ++i) s.hres[i] = h[s.slot_cell[s.slot[3 * i]]];
+    sc->struct_vol += structure_transfers(s, time_step, area);
+    for (int q = 0; q < s.n_slots; ++q) h[s.slot_cell[q]] = h[s.slot_cell[q]] + s.extra[q];
+}
+
 // outlet sink (LIM_D4.m:417-498), one thread per outlet cell
 template <typename R>
 __global__ void k_outlet(GridView<R> g, double dt_s, R* h, const int32_t* cells, const R* coef, int n_out,

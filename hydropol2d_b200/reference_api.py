@@ -73,7 +73,9 @@ def Local_Inertial_Model_D4(flag_numerical_scheme, reservoir_x, reservoir_y, k1,
     """``[qout_left, qout_right, qout_up, qout_down, outlet_flow, d_t, I_tot_end_cell, outflow,
     Hf, Qc, Qf, Qci, Qfi, C_a] = Local_Inertial_Model_D4(...)`` (Local_Inertial_Model_D4.m:1-5).
 
-    Arguments the non-subgrid, reservoir-free branch never reads (reservoir tables, d_p,
+    With ``flag_reservoir = 1`` the reservoir tables (1-based cells, NaN for no downstream
+    cell) drive the control-structure transfers (Local_Inertial_Model_D4.m:318-344).
+    Arguments the non-subgrid branch never reads (d_p,
     outlet_index, d_tolerance, idx_nan, the subgrid inputs) are accepted and ignored, as in
     the reference (idx_nan only enters Inertial_Solver's schemes 2/3).  ``roughness_squared``
     must equal ``roughness_cell.^2`` and ``cell_area`` must be ``Resolution^2``: the library
@@ -81,10 +83,9 @@ def Local_Inertial_Model_D4(flag_numerical_scheme, reservoir_x, reservoir_y, k1,
     an (ny, nx) map sampled at the outlets (outlet_type 1).  ``precision`` selects the FP64
     (default, the reference's) or FP32 build.
     """
-    if int(flag_subgrid) != 0 or int(flag_reservoir) != 0 or int(flag_numerical_scheme) != 1:
+    if int(flag_subgrid) != 0 or int(flag_reservoir) not in (0, 1) or int(flag_numerical_scheme) != 1:
         # the C ABI rejects these; raise the same error before touching the device
-        raise _abi.HP2DError(2, "flag_subgrid/flag_reservoir = 1 and schemes 2/3 are not "
-                                "implemented by this build")
+        raise _abi.HP2DError(2, "flag_subgrid = 1 and schemes 2/3 are not implemented by this build")
     z = np.asarray(z, dtype=np.float64)
     if z.ndim != 2:
         raise ValueError("z must be an (ny, nx) array")
@@ -107,10 +108,16 @@ def Local_Inertial_Model_D4(flag_numerical_scheme, reservoir_x, reservoir_y, k1,
     else:
         per_outlet = np.broadcast_to(s, (ny, nx))[rows, cols]
     params = _abi.default_params(outlet_type=int(outlet_type), slope_outlet=scalar_slope,
-                                 flag_critical=int(flag_critical))
-    pkey = (int(outlet_type), scalar_slope, int(flag_critical))
+                                 flag_critical=int(flag_critical), flag_reservoir=int(flag_reservoir))
+    pkey = (int(outlet_type), scalar_slope, int(flag_critical), int(flag_reservoir))
     g = _session(ny, nx, res, precision, pkey, params)
     g.upload_static(z, n, rows, cols, per_outlet)
+    if int(flag_reservoir) == 1:   # 1-based (x = column, y = row); NaN: no downstream cell
+        def idx(v):
+            a = np.asarray(v, dtype=np.float64).ravel()
+            return np.where(np.isfinite(a), a - 1, -1).astype(np.int32)
+        g.set_reservoirs(idx(reservoir_y), idx(reservoir_x), k1, h1, k2, idx(yds1), idx(xds1), k3, h2, k4,
+                         idx(yds2), idx(xds2))
     of = np.asarray(outflow, dtype=np.float64)
     if of.shape != (ny, nx, 3) and of.shape != (ny, nx, 2):
         raise ValueError("outflow must be (ny, nx, 3) pages [mm/h]")

@@ -150,6 +150,21 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_stage(self._h, int(d.shape[1]), int(t.size), _dp(t), _dp(d), int(rr.size),
                                            rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
 
+    def set_reservoirs(self, res_row, res_col, k1, h1, k2, ds1_row, ds1_col, k3, h2, k4, ds2_row, ds2_col):
+        """Reservoir / control structures (``flag_reservoir = 1``): the reservoir_x/y, k1, h1, k2,
+        k3, h2, k4, yds1/xds1, yds2/xds2 arguments of Local_Inertial_Model_D4 as arrays over the
+        structures, 0-based cells, -1 rows for the reference's NaN (no downstream cell)."""
+        i32 = [np.ascontiguousarray(a, dtype=np.int32).ravel() for a in (res_row, res_col, ds1_row, ds1_col,
+                                                                          ds2_row, ds2_col)]
+        f64 = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (k1, h1, k2, k3, h2, k4)]
+        n = i32[0].size
+        if any(a.size != n for a in i32 + f64):
+            raise ValueError("every structure argument needs one entry per structure")
+        ip = C.POINTER(C.c_int32)
+        rr, rc, d1r, d1c, d2r, d2c = (a.ctypes.data_as(ip) for a in i32)
+        self._check(self._L.hp2d_set_reservoirs(self._h, int(n), rr, rc, _dp(f64[0]), _dp(f64[1]), _dp(f64[2]), d1r, d1c,
+                                                _dp(f64[3]), _dp(f64[4]), _dp(f64[5]), d2r, d2c))
+
     def set_rain_gauges(self, x_gauge, y_gauge, rates, record_dt: float, x_ul: float = 0.0, y_ul: float = 0.0):
         """Rain from gauges: ``rates`` (n_times, n_gauges) [mm/h] (NaN: no record) over intervals
         of ``record_dt`` minutes, interpolated by inverse-distance weighting to every cell."""

@@ -40,6 +40,7 @@ class Case:
     meta: dict = field(default_factory=dict)
     inflow: dict | None = None              # set_inflow kwargs (t_start, rates, rows, cols, gauge)
     stage: dict | None = None               # set_stage kwargs (t_start, depth_m, rows, cols, gauge)
+    reservoirs: dict | None = None          # set_reservoirs kwargs (flag_reservoir = 1)
 
     @property
     def shape(self):
@@ -59,6 +60,8 @@ class Case:
             sf.set_inflow(**self.inflow)
         if self.stage is not None:
             sf.set_stage(**self.stage)
+        if self.reservoirs is not None:
+            sf.set_reservoirs(**self.reservoirs)
         return sf
 
 
@@ -164,6 +167,44 @@ def inflow_case(ny: int = 96, nx: int = 96, dx: float = 10.0, minutes: float = 4
                   gauge=np.concatenate([np.zeros(g0_r.size, np.int32), np.ones(g1_r.size, np.int32)]))
     return Case(f"inflow_vtilt_{ny}x{nx}", z, np.full((ny, nx), 0.03), dx, rows, ch.astype(np.int32), params,
                 np.zeros((ny, nx)), inflow=inflow)
+
+
+def structures_case(ny: int = 48, nx: int = 48, dx: float = 10.0, minutes: float = 20.0, soil: bool = False,
+                    maps: bool = False) -> Case:
+    """The V-tilted catchment with a 0.6 m pond on the left plane drained by control structures
+    (flag_reservoir = 1, Local_Inertial_Model_D4.m:318-344), rain at 50 mm/h for 10 min:
+    structure 0 drains the pond's centre through two rating curves (crest 0.2 m into a cell
+    down the plane, crest 0.4 m into a cell along it); structure 1 drains structure 0's first
+    downstream cell into the channel (so it sees structure 0's transfer the same step);
+    structure 2 drains a right-plane cell that only rain fills.  ``soil`` adds Green-Ampt
+    classes, ``maps`` replaces the uniform rain by 8 x 8 rate maps."""
+    z, ch = vtilt_domain(ny, nx, dx, 0.005, 0.002)
+    rows = np.zeros(ch.size, dtype=np.int32)
+    params = dict(routing_time=minutes, alfa_min=0.7, alfa_max=0.7, outlet_type=1, slope_outlet=0.002,
+                  min_time_step=0.01, max_time_step=10.0, flag_reservoir=1)
+    pr, pc = ny // 2, nx // 6
+    d0 = np.zeros((ny, nx))
+    d0[pr - 1:pr + 2, pc - 1:pc + 2] = 600.0
+    res = dict(res_row=[pr, pr, ny - 3], res_col=[pc, pc + 6, nx - 5],
+               k1=[3.0, 0.5, 1.0], h1=[0.2, 0.0, 0.001], k2=[1.5, 5.0 / 3.0, 1.0],
+               ds1_row=[pr, ny // 3, ny - 3], ds1_col=[pc + 6, int(ch[0]), nx - 10],
+               k3=[1.0, 0.0, 0.0], h2=[0.4, 0.0, 0.0], k4=[2.5, 0.0, 0.0],
+               ds2_row=[pr + 5, -1, -1], ds2_col=[pc, -1, -1])
+    c = Case(f"structures_vtilt_{ny}x{nx}", z, np.full((ny, nx), 0.03), dx, rows, ch.astype(np.int32), params,
+             d0, rain_uniform=(np.array([0.0, 10.0]), np.array([50.0, 0.0])), reservoirs=res)
+    if soil:
+        cls = voronoi_classes(ny, nx, 12, 3, 5).astype(np.uint8)
+        cls[:, ch] = 255
+        c.soil = dict(soil_class=cls, **green_ampt_soil_tables([1.0, 10.0, 30.0], [50.0, 110.0, 200.0],
+                                                                  [0.2, 0.3, 0.4]))
+        c.I0 = np.full((ny, nx), 5.0)
+        c.params["flag_infiltration"] = 1
+    if maps:
+        rng = np.random.default_rng(4)
+        c.rain_uniform = None
+        c.rain_maps = rng.uniform(0.0, 100.0, size=(3, 8, 8)).astype(np.float32)
+        c.rain_map_dt = 5.0
+    return c
 
 
 def breach_inflow_case(ny: int = 128, nx: int = 512, dx: float = 5.0, seed: int = 11, minutes: float = 30.0,

@@ -37,7 +37,7 @@ extern "C" {
 typedef enum hp2d_status {
     HP2D_OK = 0,
     HP2D_INVALID_ARG = 1,
-    HP2D_UNSUPPORTED_FLAG = 2,   /* flag_subgrid/flag_D8/flag_reservoir=1, scheme 2/3 ... */
+    HP2D_UNSUPPORTED_FLAG = 2,   /* flag_subgrid/flag_D8=1, scheme 2/3 ... */
     HP2D_CUDA_ERROR = 3,
     HP2D_NUMERICAL = 4,          /* NaN/Inf in the state */
     HP2D_DT_FLOOR = 5,           /* dt hit min_time_step (refreshing_timestep.m:357-359) */
@@ -62,7 +62,7 @@ typedef struct hp2d_params {
     int32_t flag_critical;              /* 0/1: critical-velocity clip (LIM_D4.m:272-275) */
     int32_t flag_subgrid;               /* must be 0 */
     int32_t flag_D8;                    /* must be 0 */
-    int32_t flag_reservoir;             /* must be 0 */
+    int32_t flag_reservoir;             /* 0, or 1 with hp2d_set_reservoirs */
     int32_t flag_infiltration;          /* 0 off, 1 Green-Ampt (hp2d_set_soil), 2 van Genuchten (hp2d_set_soil_vg) */
     int32_t flag_timestep;              /* 1: dt = min(dt_adv, dt_wave); 0: dt_wave */
     int32_t flag_adaptive_timestepping; /* 1: wave celerity only; 0: celerity + speed */
@@ -111,6 +111,7 @@ typedef struct hp2d_diag {
     double t_previous;            /* the loop's t_previous [min] */
     double inflow_volume;         /* cumulative inflow-hydrograph volume [m^3] */
     double stage_volume;          /* cumulative volume the stage overwrites added [m^3] */
+    double structure_volume;      /* cumulative volume the control structures added [m^3] */
 } hp2d_diag;
 
 typedef struct hp2d_ctx hp2d_ctx;
@@ -233,6 +234,23 @@ hp2d_status hp2d_download_map_record(hp2d_ctx* ctx, int64_t index, double* depth
 hp2d_status hp2d_set_stage(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, const double* t_start,
                            const double* depth_m, int32_t n_cells, const int32_t* rows, const int32_t* cols,
                            const int32_t* gauge);
+
+/* Reservoir / control structures (flag_reservoir = 1): the reservoir_x, reservoir_y, k1, h1,
+ * k2, k3, h2, k4, yds1, xds1, yds2, xds2 arguments of Local_Inertial_Model_D4
+ * (Local_Inertial_Model_D4.m:2, :318-344; Reservoir_Data of HydroPol2D_preprocessing.m:820-826),
+ * 0-based cells, ds1_row = -1 / ds2_row = -1 for the reference's NaN.  Each step, structure i
+ * takes the depth of its reservoir cell entering the fluxes and moves
+ * dh = min(k1 max(h-h1,0)^k2 / A x 3.6e6, 1000 max(h-h1,0)/dt_h) dt_h [mm] to ds1 (and likewise
+ * through k3, h2, k4 to ds2), in structure order, with the reference's bookkeeping: the
+ * reservoir cell's volume term GAINS the transfer and the first transfer is added to ds1 a
+ * second time when a second structure exists.  The transfers enter each cell after the fluxes
+ * (both hp2d_li_step and the fused step); hp2d_get_diag reports the volume they add.  After
+ * hp2d_upload_static; outlet and NaN-elevation cells cannot take part; ds2 needs ds1;
+ * n = 0 removes them. */
+hp2d_status hp2d_set_reservoirs(hp2d_ctx* ctx, int32_t n, const int32_t* res_row, const int32_t* res_col,
+                                const double* k1, const double* h1, const double* k2, const int32_t* ds1_row,
+                                const int32_t* ds1_col, const double* k3, const double* h2, const double* k4,
+                                const int32_t* ds2_row, const int32_t* ds2_col);
 
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
 /* Hydrological_Model for this path: adds delta_p_agg (the rain of the current rain

@@ -66,6 +66,8 @@ def _load():
             "oracle_set_map_records": ([vp, C.c_int32, dp], C.c_int),
             "oracle_set_stage": ([vp, C.c_int32, C.c_int32, dp, dp, C.c_int32, P(C.c_int32), P(C.c_int32),
                                   P(C.c_int32)], C.c_int),
+            "oracle_set_reservoirs": ([vp, C.c_int32, i32p, i32p, dp, dp, dp, i32p, i32p, dp, dp, dp, i32p, i32p],
+                                      C.c_int),
             "oracle_map_records": ([vp], C.c_int64),
             "oracle_download_map_record": ([vp, C.c_int64, dp, dp], C.c_int),
             "oracle_set_inflow": ([vp, C.c_int32, C.c_int32, dp, dp, C.c_int32, P(C.c_int32), P(C.c_int32),
@@ -168,6 +170,15 @@ class KernelFormOracle:
         ip = C.POINTER(C.c_int32)
         self._L.oracle_set_stage(self._h, int(d.shape[1]), int(t.size), _dp(t), _dp(d), int(rr.size),
                                  rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip))
+
+    def set_reservoirs(self, res_row, res_col, k1, h1, k2, ds1_row, ds1_col, k3, h2, k4, ds2_row, ds2_col):
+        i32 = [np.ascontiguousarray(a, dtype=np.int32).ravel() for a in (res_row, res_col, ds1_row, ds1_col,
+                                                                          ds2_row, ds2_col)]
+        f64 = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (k1, h1, k2, k3, h2, k4)]
+        ip = C.POINTER(C.c_int32)
+        rr, rc, d1r, d1c, d2r, d2c = (a.ctypes.data_as(ip) for a in i32)
+        self._L.oracle_set_reservoirs(self._h, int(i32[0].size), rr, rc, _dp(f64[0]), _dp(f64[1]), _dp(f64[2]),
+                                      d1r, d1c, _dp(f64[3]), _dp(f64[4]), _dp(f64[5]), d2r, d2c)
 
     def set_map_records(self, time_records, n_slots=None):
         t = np.ascontiguousarray(time_records, dtype=np.float64).ravel()

@@ -439,6 +439,72 @@ public:
         stage_vol += v * res * res;
     }
 
+    // ---------------- reservoir / control structures (Local_Inertial_Model_D4.m:318-344) ------
+    // From the depth the fluxes use, in structure order: dtsup = d_tot(res)/1000 (with the
+    // earlier structures' additions to d_tot), dh = min(k1 max(dtsup-h1,0)^k2 / A 1000 3600,
+    // 1000 max(dtsup-h1,0)/dt_h) dt_h mm; the reservoir's Vol_Flux gains dh (the reference's
+    // sign), ds1 gains dh, and with a second structure ds1 gains dh again, then dh2 goes the
+    // same way to ds2.  Each cell's additions (in mm, FP64) join its depth before the
+    // continuity as one extra: hn = (h + extra) + flux term.
+    int st_n = 0;
+    std::vector<double> st_coef;          // [n][6] k1 h1 k2 k3 h2 k4
+    std::vector<int32_t> st_slot;         // [n][3] slot of res, ds1, ds2 (-1: none)
+    std::vector<size_t> st_cell;          // slot -> cell
+    double struct_vol = 0;
+    void set_reservoirs(int n, const int32_t* rr, const int32_t* rc, const double* k1, const double* h1,
+                        const double* k2, const int32_t* d1r, const int32_t* d1c, const double* k3,
+                        const double* h2, const double* k4, const int32_t* d2r, const int32_t* d2c) {
+        st_n = n;
+        st_coef.assign(size_t(n) * 6, 0.0);
+        st_slot.assign(size_t(n) * 3, -1);
+        st_cell.clear();
+        auto slot_of = [&](int r, int c) {
+            const size_t k = at(r, c);
+            for (size_t q = 0; q < st_cell.size(); ++q)
+                if (st_cell[q] == k) return int32_t(q);
+            st_cell.push_back(k);
+            return int32_t(st_cell.size() - 1);
+        };
+        for (int i = 0; i < n; ++i) {
+            const double cf[6] = {k1[i], h1[i], k2[i], k3[i], h2[i], k4[i]};
+            for (int q = 0; q < 6; ++q) st_coef[size_t(i) * 6 + q] = cf[q];
+            st_slot[3 * i] = slot_of(rr[i], rc[i]);
+            if (d1r[i] >= 0) st_slot[3 * i + 1] = slot_of(d1r[i], d1c[i]);
+            if (d2r[i] >= 0) st_slot[3 * i + 2] = slot_of(d2r[i], d2c[i]);
+        }
+    }
+    // extras [m] per slot from the depth h the fluxes use; time_step [min]
+    std::vector<R> structure_extras(double ts_min) const {
+        const size_t m = st_cell.size();
+        std::vector<double> ds(m, 0.0), rv(m, 0.0);
+        const double dt_h = ts_min / 60.0, area = res * res;
+        for (int i = 0; i < st_n; ++i) {
+            const double* c = &st_coef[size_t(i) * 6];
+            const int sr = st_slot[3 * i], s1 = st_slot[3 * i + 1], s2 = st_slot[3 * i + 2];
+            double dh = 0.0, dtsup = 0.0;
+            if (s1 >= 0) {
+                dtsup = (double(h[st_cell[size_t(sr)]]) * 1000.0 + ds[size_t(sr)]) / 1000.0;
+                const double q = std::fmax(dtsup - c[1], 0.0);
+                const double avail = 1000.0 * q / dt_h;
+                dh = std::fmin(c[0] * std::pow(q, c[2]) / area * 1000.0 * 3600.0, avail) * dt_h;
+                rv[size_t(sr)] += dh;
+                dtsup = dtsup - dh / 1000.0;
+                ds[size_t(s1)] += dh;
+            }
+            if (s2 >= 0) {
+                ds[size_t(s1)] += dh;
+                const double q = std::fmax(dtsup - c[4], 0.0);
+                const double avail = 1000.0 * q / dt_h;
+                const double dh2 = std::fmin(c[3] * std::pow(q, c[5]) / area * 1000.0 * 3600.0, avail) * dt_h;
+                rv[size_t(sr)] += dh2;
+                ds[size_t(s2)] += dh2;
+            }
+        }
+        std::vector<R> ex(m);
+        for (size_t q = 0; q < m; ++q) ex[q] = R((ds[q] + rv[q]) / 1000.0);
+        return ex;
+    }
+
     // ---------------- hydrology: rain + Green-Ampt + clamp ----------------
     void hydrology(double dts) {
         Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
@@ -539,7 +605,7 @@ public:
         q = std::fmin(std::fmax(q, -thr), thr);
     }
 
-    void li(double dts) {
+    void li(double dts, double ts_min) {
         Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
         // faces (unlimited)
 #pragma omp parallel for schedule(static)
@@ -589,6 +655,16 @@ public:
                 if (!std::isfinite(q)) q = R(0);
                 qy[c] = q;
             }
+        // control structures: extras from the depth the fluxes used, joining h first
+        if (st_n) {
+            const std::vector<R> ex = structure_extras(ts_min);
+            double v = 0.0;
+            for (size_t q = 0; q < ex.size(); ++q) {
+                h[st_cell[q]] = h[st_cell[q]] + ex[q];
+                v += double(ex[q]) * res * res;
+            }
+            struct_vol += v;
+        }
         // continuity
         hn.resize(h.size());
 #pragma omp parallel for schedule(static)
@@ -723,7 +799,7 @@ public:
     void step() {
         double dts = time_step * 60.0;
         hydrology(dts);
-        li(dts);
+        li(dts, time_step);
         double pos_save = std::ceil((t_min * 60.0) / p.time_step_change);
         double time_save = (pos_save - 1.0) * p.time_step_change / 60.0;
         double delta = time_save - tsp;

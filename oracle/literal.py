@@ -130,11 +130,54 @@ class LIOutputs:
     Hf: np.ndarray               # (3, ny, nx) m
 
 
+def reservoir_transfers(d_tot, vol_flux, rs: dict, time_step: float, cell_area: float):
+    """Local_Inertial_Model_D4.m:318-344 line by line (after the volume flux :313, before
+    d_t :390): structure ii drains (res_row, res_col) through k1 max(dtsup-h1,0)^k2 into
+    ds1 and, when ds2 exists, through (k3, h2, k4) into ds2.  Cells are 0-based; a ds1/ds2
+    row that is negative or NaN is the reference's NaN.  Kept as the reference has it: the
+    reservoir cell's Vol_Flux GAINS each transfer, and the first transfer is added to ds1 a
+    second time in the second structure's branch.  Returns the new (d_tot, vol_flux)."""
+    d_tot = np.array(d_tot, dtype=np.float64)
+    vol_flux = np.array(vol_flux, dtype=np.float64)
+    dt_h = time_step / 60
+
+    def none(v):
+        return not (v >= 0)
+
+    dtsup = None
+    for ii in range(len(rs["res_row"])):
+        r = (int(rs["res_row"][ii]), int(rs["res_col"][ii]))
+        if not none(rs["ds1_row"][ii]):
+            ds1 = (int(rs["ds1_row"][ii]), int(rs["ds1_col"][ii]))
+            dtsup = d_tot[r] / 1000
+            available_volume = 1000 * (np.fmax(dtsup - rs["h1"][ii], 0)) / dt_h
+            dh = np.fmin(rs["k1"][ii] * (np.fmax(dtsup - rs["h1"][ii], 0)) ** rs["k2"][ii] / cell_area * 1000 * 3600,
+                         available_volume) * dt_h
+            vol_flux[r] = vol_flux[r] + dh / 1000 * cell_area
+            dtsup = dtsup - dh / 1000
+            d_tot[ds1] = d_tot[ds1] + dh
+        else:
+            dh = 0
+        if not none(rs["ds2_row"][ii]):
+            if none(rs["ds1_row"][ii]):
+                raise IndexError("yds1 is NaN where yds2 is not (the reference's indexing fails)")
+            ds1 = (int(rs["ds1_row"][ii]), int(rs["ds1_col"][ii]))
+            ds2 = (int(rs["ds2_row"][ii]), int(rs["ds2_col"][ii]))
+            d_tot[ds1] = d_tot[ds1] + dh
+            available_volume = 1000 * (np.fmax(dtsup - rs["h2"][ii], 0)) / dt_h
+            dh = np.fmin(rs["k3"][ii] * (np.fmax(dtsup - rs["h2"][ii], 0)) ** rs["k4"][ii] / cell_area * 1000 * 3600,
+                         available_volume) * dt_h
+            vol_flux[r] = vol_flux[r] + dh / 1000 * cell_area
+            d_tot[ds2] = d_tot[ds2] + dh
+    return d_tot, vol_flux
+
+
 def local_inertial_model_d4(z, d_tot, roughness_cell, roughness_squared, cell_area, time_step,
                             resolution, outlet_rows, outlet_cols, outlet_type, slope_outlet,
                             outflow, flag_numerical_scheme=1, flag_critical=0,
-                            h_min=0.0) -> LIOutputs:
-    """``Local_Inertial_Model_D4`` with ``flag_subgrid=0`` and ``flag_reservoir=0``.
+                            h_min=0.0, reservoirs: dict | None = None) -> LIOutputs:
+    """``Local_Inertial_Model_D4`` with ``flag_subgrid=0``; ``reservoirs`` (``flag_reservoir=1``)
+    is the structure table of ``reservoir_transfers``.
 
     Follows Local_Inertial_Model_D4.m:31-44 (depth, WSE), :89-142 (slopes, face depths,
     closed N/E boundary faces), :184 (Hf>=0), :198-201 (q_prev, dt), :263-264 (solver,
@@ -190,7 +233,10 @@ def local_inertial_model_d4(z, d_tot, roughness_cell, roughness_squared, cell_ar
         qout_right = out[0].copy()
         qout_up = out[1].copy()
         qout_down = -np.concatenate([out[1][1:, :], zr], axis=0)
-        d_t = d_tot + 1000 * vol_flux / (res * res)
+        d_src = d_tot
+        if reservoirs is not None:
+            d_src, vol_flux = reservoir_transfers(d_tot, vol_flux, reservoirs, time_step, cell_area)
+        d_t = d_src + 1000 * vol_flux / (res * res)
         d_t[d_t < 0] = 0
         outlet_flow = np.zeros((ny, nx))
         out[2] = 0
@@ -479,6 +525,8 @@ class RunConfig:
     stage_times_min: np.ndarray | None = None
     stage_depth_m: np.ndarray | None = None
     stage_cells: np.ndarray | None = None
+    # reservoir / control structures (flag_reservoir = 1): the table of reservoir_transfers
+    reservoirs: dict | None = None
     fixed_time_step_s: float | None = None      # bypass refreshing_timestep
 
 
@@ -648,6 +696,7 @@ class RunState:
     outlet_volume: float = 0.0
     inflow_volume: float = 0.0
     stage_volume: float = 0.0
+    structure_volume: float = 0.0
     # rain interval [rain_a, rain_b] of the current step and the loop's t_previous [min]; the
     # first step's comes from the call before the loop (HydroPol2D_Main_While.m:115) with
     # t_previous = 0 (:120)
@@ -697,7 +746,10 @@ def step(cfg: RunConfig, st: RunState) -> None:
     n = cfg.roughness
     out = local_inertial_model_d4(cfg.z, d_tot, n, n * n, A, time_step, res, cfg.outlet_rows,
                                   cfg.outlet_cols, cfg.outlet_type, cfg.slope_outlet, st.outflow,
-                                  cfg.flag_numerical_scheme, cfg.flag_critical)
+                                  cfg.flag_numerical_scheme, cfg.flag_critical, reservoirs=cfg.reservoirs)
+    if cfg.reservoirs is not None:   # what the transfers added: d_t + outlet water - (d_tot + fluxes)
+        d_plain, vf = reservoir_transfers(d_tot, np.zeros_like(d_tot), cfg.reservoirs, time_step, A)
+        st.structure_volume += (float(np.sum(d_plain - d_tot)) + float(np.sum(vf)) * 1000 / A) * A / 1000
     st.outlet_volume += float(np.nansum(out.outlet_flow)) * (time_step / 60) / 1000 * A
     # HydroPol2D_Main_While.m:691-705 (time_save gate) + refreshing_timestep.m
     if cfg.fixed_time_step_s:

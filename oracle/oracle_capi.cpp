@@ -77,6 +77,12 @@ int oracle_set_stage(oracle_model* m, int32_t ng, int32_t nt, const double* t0, 
     return dispatch(m, [&](auto& M) { M.set_stage(ng, nt, t0, d, nc, rows, cols, gauge); return 0; });
 }
 
+int oracle_set_reservoirs(oracle_model* m, int32_t n, const int32_t* rr, const int32_t* rc, const double* k1,
+                          const double* h1, const double* k2, const int32_t* d1r, const int32_t* d1c, const double* k3,
+                          const double* h2, const double* k4, const int32_t* d2r, const int32_t* d2c) {
+    return dispatch(m, [&](auto& M) { M.set_reservoirs(n, rr, rc, k1, h1, k2, d1r, d1c, k3, h2, k4, d2r, d2c); return 0; });
+}
+
 int oracle_set_map_records(oracle_model* m, int32_t n, const double* times) {
     return dispatch(m, [&](auto& M) { M.set_map_records(n, times); return 0; });
 }
@@ -128,7 +134,7 @@ int oracle_hydrology_step(oracle_model* m, double time_step) {
 }
 
 int oracle_li_step(oracle_model* m, double time_step) {
-    return dispatch(m, [&](auto& M) { M.li(time_step * 60.0); return 0; });
+    return dispatch(m, [&](auto& M) { M.li(time_step * 60.0, time_step); return 0; });
 }
 
 int oracle_cfl_dt(oracle_model* m, double time_step_applied, double* ts_out, double* vmax) {
@@ -223,6 +229,7 @@ int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
         o->t_previous = M.t_prev;
         o->inflow_volume = M.inflow_vol;
         o->stage_volume = M.stage_vol;
+        o->structure_volume = M.struct_vol;
         return 0;
     });
 }

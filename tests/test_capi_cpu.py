@@ -35,7 +35,7 @@ def _create(**kw):
     return st, L.hp2d_create_error().decode(), h
 
 
-@pytest.mark.parametrize("flag,value", [("flag_subgrid", 1), ("flag_D8", 1), ("flag_reservoir", 1),
+@pytest.mark.parametrize("flag,value", [("flag_subgrid", 1), ("flag_D8", 1),
                                         ("flag_numerical_scheme", 2), ("flag_numerical_scheme", 3),
                                         ("flag_infiltration", 3)])
 def test_unsupported_flags_rejected(hp2d_lib, flag, value):
@@ -45,7 +45,7 @@ def test_unsupported_flags_rejected(hp2d_lib, flag, value):
 
 
 @pytest.mark.parametrize("kw", [dict(outlet_type=3), dict(min_time_step=0.0), dict(max_time_step=0.001),
-                                dict(flag_critical=2)])
+                                dict(flag_critical=2), dict(flag_reservoir=2)])
 def test_invalid_controls_rejected(hp2d_lib, kw):
     st, msg, _ = _create(**kw)
     assert _abi.STATUS[st] == "HP2D_INVALID_ARG", msg

@@ -41,6 +41,8 @@ def literal_cfg(case):
         for r, c, g in zip(stage["rows"], stage["cols"], stage["gauge"]):
             masks[g, r, c] = 1.0
         kw["stage_times_min"], kw["stage_depth_m"], kw["stage_cells"] = stage["t_start"], d, masks
+    if getattr(case, "reservoirs", None) is not None:
+        kw["reservoirs"] = {k: np.asarray(v, dtype=np.float64) for k, v in case.reservoirs.items()}
     return L.RunConfig(**kw)
 
 

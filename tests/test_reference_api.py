@@ -27,9 +27,9 @@ def test_unsupported_flags_raise_before_device():
     from hydropol2d_b200 import HP2DError, reference_api
     case = random_terrain(8, 8, seed=1)
     args = list(_lim_args(case, case.d0, np.zeros((8, 8, 3)), 0.01))
-    for pos in (0, 13, 31):   # flag_numerical_scheme=2, flag_reservoir=1, flag_subgrid=1
+    for pos, v in ((0, 2), (13, 2), (31, 1)):   # flag_numerical_scheme=2, flag_reservoir=2, flag_subgrid=1
         bad = list(args)
-        bad[pos] = 2 if pos == 0 else 1
+        bad[pos] = v
         with pytest.raises(HP2DError) as e:
             reference_api.Local_Inertial_Model_D4(*bad)
         assert e.value.status_name == "HP2D_UNSUPPORTED_FLAG"
@@ -102,3 +102,44 @@ def test_refreshing_timestep_matches_literal():
     assert math.isclose(vmax, lit.max_velocity, rel_tol=2e-6)
     assert abs(tcr - lit.time_calculation_routing) <= 0.001 + 1e-12
     assert math.isclose(ts, tcr / 60, rel_tol=1e-15)
+
+
+@pytest.mark.gpu
+def test_local_inertial_model_d4_with_reservoirs_matches_literal():
+    """flag_reservoir = 1 through the MATLAB signature: 1-based reservoir tables with NaN for
+    a missing downstream cell, two chained calls, FP64, against the literal restatement."""
+    from hydropol2d_b200 import reference_api
+    from oracle import literal
+    case = random_terrain(30, 36, seed=7)
+    ny, nx = case.z.shape
+    d = case.d0.copy()
+    d[10, 10] = 900.0
+    d[20, 5] = 400.0
+    tab = dict(res_row=np.array([10, 20]), res_col=np.array([10, 5]), k1=np.array([2.0, 0.7]),
+               h1=np.array([0.3, 0.1]), k2=np.array([1.5, 2.0]), ds1_row=np.array([12, 10]),
+               ds1_col=np.array([14, 14]), k3=np.array([1.0, 0.0]), h2=np.array([0.5, 0.0]),
+               k4=np.array([2.5, 0.0]), ds2_row=np.array([8.0, np.nan]), ds2_col=np.array([3.0, np.nan]))
+    outflow = np.zeros((ny, nx, 3))
+    d_lit, of_lit = d.copy(), np.zeros((3, ny, nx))
+    for time_step in (0.02, 0.015):
+        args = list(_lim_args(case, d, outflow, time_step))
+        args[1], args[2] = tab["res_col"] + 1, tab["res_row"] + 1          # reservoir_x, reservoir_y
+        args[3], args[4], args[5] = tab["k1"], tab["h1"], tab["k2"]
+        args[6], args[7], args[8] = tab["k3"], tab["h2"], tab["k4"]
+        args[9], args[10] = tab["ds1_row"] + 1, tab["ds1_col"] + 1         # yds1, xds1
+        args[11], args[12] = tab["ds2_row"] + 1, tab["ds2_col"] + 1        # yds2, xds2 (NaN stays)
+        args[13] = 1
+        got = reference_api.Local_Inertial_Model_D4(*args)
+        ref = literal.local_inertial_model_d4(
+            case.z, d_lit, case.roughness, case.roughness ** 2, case.resolution ** 2, time_step,
+            case.resolution, case.outlet_rows, case.outlet_cols, 1, case.params["slope_outlet"], of_lit,
+            reservoirs=tab)
+        fin = np.isfinite(ref.d_t)
+        np.testing.assert_allclose(got[5][fin], ref.d_t[fin], rtol=1e-9, atol=1e-9)
+        plain = literal.local_inertial_model_d4(
+            case.z, d_lit, case.roughness, case.roughness ** 2, case.resolution ** 2, time_step,
+            case.resolution, case.outlet_rows, case.outlet_cols, 1, case.params["slope_outlet"], of_lit)
+        if time_step == 0.02:   # the first call moves water (the steep cells drain below the crests)
+            assert np.nanmax(np.abs(ref.d_t - plain.d_t)) > 1.0
+        d, outflow = got[5], got[7]
+        d_lit, of_lit = ref.d_t, ref.outflow
