@@ -330,7 +330,7 @@ def main():
     # and filled on the device.  D2H: outlet hydrograph (4 B per outlet) and the clock block
     # every step, then the depth and dmax components (FP32, 8 B/cell) once
     h2d_per_step = 28 * cells / e2e_steps
-    d2h_per_step = n_out * 4 + 2 * 224 + 8 * cells / e2e_steps   # 224 B: the clock block
+    d2h_per_step = n_out * 4 + 2 * 232 + 8 * cells / e2e_steps   # 232 B: the clock block
     e2e = cells * e2e_steps / e2e_s / 1e9
     if dist is not None:
         t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
