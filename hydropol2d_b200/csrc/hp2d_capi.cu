@@ -1022,6 +1022,8 @@ template <typename R> struct Impl : Base {
         a.inflow = inflow;
         a.rec = rec;
         a.strct = strct;
+        a.vmax = hz_on ? vmaxm.p : nullptr;
+        a.hzmax = hz_on ? hzmaxm.p : nullptr;
         a.sc = sc.p;
         return a;
     }
@@ -1071,7 +1073,30 @@ template <typename R> struct Impl : Base {
     }
 
     // the fused kernel variant with boundary-condition cells (inflow, stage, structures)
-    bool bc_kernel() const { return inflow.n_gauges > 0 || inflow.n_stage > 0 || strct.n > 0; }
+    bool bc_kernel() const { return inflow.n_gauges > 0 || inflow.n_stage > 0 || strct.n > 0 || hz_on; }
+
+    // Velocity and hazard maxima (velocities.vmax_final, velocities.hazardmax_final of
+    // save_output_maps.m:588-604) tracked by the fused step; on = 1 (re)starts them at zero.
+    // Every step must refresh the velocities (time_step_change at most half min_time_step).
+    bool hz_on = false;
+    Dev<R> vmaxm, hzmaxm;
+    hp2d_status set_hazard_tracking(int32_t on) {
+        if (on != 0 && on != 1) { ctx->err = "on must be 0 or 1"; return HP2D_INVALID_ARG; }
+        if (on && !(2.0 * ctx->p.time_step_change <= ctx->p.min_time_step)) {
+            ctx->err = "hazard maps need a velocity refresh every step (time_step_change <= min_time_step / 2)";
+            return HP2D_INVALID_ARG;
+        }
+        if (on) {
+            vmaxm.alloc(n);
+            hzmaxm.alloc(n);
+            fill(vmaxm.p, n, R(0));
+            fill(hzmaxm.p, n, R(0));
+        }
+        hz_on = on != 0;
+        invalidate_graph();
+        dirty = true;
+        return HP2D_OK;
+    }
 
     template <int INF> void struct_prime_t(const FusedArgs<R>& a) {
         if (rain.n_maps > 0) k_struct_prime<R, INF, true><<<1, kThreads, 0, st()>>>(a);
@@ -1327,6 +1352,12 @@ template <typename R> struct Impl : Base {
             case HP2D_FIELD_HF_OUTLET: per_outlet_map(hf3, 1.0); break;
             case HP2D_FIELD_DMAX: { auto v = fetch_component(3); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0; break; }
             case HP2D_FIELD_ARRIVAL: { auto v = fetch(arrival.p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) / 60.0; break; }
+            case HP2D_FIELD_VMAX: case HP2D_FIELD_HAZARD_MAX: {
+                if (!hz_on) { ctx->err = "velocity / hazard maxima are off (hp2d_set_hazard_tracking)"; return HP2D_NOT_READY; }
+                auto v = fetch(field == HP2D_FIELD_VMAX ? vmaxm.p : hzmaxm.p, n);
+                for (size_t k = 0; k < n; ++k) out[k] = double(v[k]);
+                break;
+            }
             case HP2D_FIELD_SOIL_STORAGE: {
                 if (!gs2[0].p) { ctx->err = "no soil storage (hp2d_set_soil not called)"; return HP2D_NOT_READY; }
                 pull_sc();
@@ -1815,6 +1846,10 @@ hp2d_status hp2d_set_reservoirs(hp2d_ctx* ctx, int32_t n, const int32_t* res_row
     return with_impl(ctx, [&](auto& m) {
         return m.set_reservoirs(n, res_row, res_col, k1, h1, k2, ds1_row, ds1_col, k3, h2, k4, ds2_row, ds2_col);
     });
+}
+
+hp2d_status hp2d_set_hazard_tracking(hp2d_ctx* ctx, int32_t on) {
+    return with_impl(ctx, [&](auto& m) { return m.set_hazard_tracking(on); });
 }
 
 hp2d_status hp2d_set_stage(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, const double* t_start,

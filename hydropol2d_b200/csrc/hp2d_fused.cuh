@@ -81,6 +81,7 @@ template <typename R> struct FusedArgs {
     InflowDesc<R> inflow;
     RecordDesc<R> rec;
     StructDesc<R> strct;         // reservoir / control structures (n = 0: none)
+    R* vmax; R* hzmax;           // velocity / hazard maxima [m/s], [m^2/s] (null: not tracked)
     StepScalars* sc;
 };
 
@@ -547,11 +548,13 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     const R dm = dm2[h];
                     if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
                     // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
+                    R vras = R(0);   // velocity raster: largest |face velocity| (refreshing_timestep.m:109-111)
                     if (!quiet) {
                         const R big = R(1e9);
                         const R vr = qxl2[h] == R(0) ? qxl2[h] : qdiv(qxl2[h], hfx2[h] < K.tol ? big : hfx2[h]);
                         const R vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
                         const R vb = qyl1[h] == R(0) ? qyl1[h] : qdiv(qyl1[h], hfy1[h] < K.tol ? big : hfy1[h]);
+                        if (INFL) vras = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb));
                         const R rc = j[h] == 0 ? R(0.5) * vr : vr;
                         const R uc = R(0.5) * (vu + vb);
                         const R s2 = rc * rc + uc * uc;
@@ -574,6 +577,17 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     o4.z = qyl2[h];
                     o4.w = hn > dm ? hn : dm;   // save_output_maps.m:598, max(d_t, dmax)
                     sout[c2] = o4;
+                    // running maxima of the velocity raster and of depth x velocity
+                    // (save_output_maps.m:588-604, snisb_velocity_hazard_snapshot :832-848)
+                    if (INFL && a.vmax) {
+                        const R vo = a.vmax[c2];
+                        a.vmax[c2] = vras > vo ? vras : vo;
+                        const R hd = fmax(hn, R(0));
+                        R hz = hd * vras;
+                        if (hd < R(0.01) || !isfinite(hz)) hz = R(0);
+                        const R ho = a.hzmax[c2];
+                        a.hzmax[c2] = isnan(hn) ? hn : (hz > ho ? hz : ho);
+                    }
                 }
             }
             // (G) shift the window down one row

@@ -150,6 +150,11 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_stage(self._h, int(d.shape[1]), int(t.size), _dp(t), _dp(d), int(rr.size),
                                            rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
 
+    def set_hazard_tracking(self, on: bool = True):
+        """Per-cell maxima of the velocity raster and of depth x velocity over the fused steps
+        (velocities.vmax_final / hazardmax_final); read with download("vmax"/"hazard_max")."""
+        self._check(self._L.hp2d_set_hazard_tracking(self._h, 1 if on else 0))
+
     def set_reservoirs(self, res_row, res_col, k1, h1, k2, ds1_row, ds1_col, k3, h2, k4, ds2_row, ds2_col):
         """Reservoir / control structures (``flag_reservoir = 1``): the reservoir_x/y, k1, h1, k2,
         k3, h2, k4, yds1/xds1, yds2/xds2 arguments of Local_Inertial_Model_D4 as arrays over the

@@ -93,7 +93,9 @@ typedef enum hp2d_field {
     HP2D_FIELD_DMAX = 9,         /* depths.dmax_final [mm] */
     HP2D_FIELD_ARRIVAL = 10,     /* first time depth >= arrival_threshold [min]; +Inf never */
     HP2D_FIELD_SOIL_STORAGE = 11,/* Soil_Properties.I_t [mm] */
-    HP2D_FIELD_I_TOT_END_CELL = 12 /* CA_States.I_tot_end_cell [m^3] (LIM_D4.m:512-514) */
+    HP2D_FIELD_I_TOT_END_CELL = 12,/* CA_States.I_tot_end_cell [m^3] (LIM_D4.m:512-514) */
+    HP2D_FIELD_VMAX = 13,        /* velocities.vmax_final [m/s] (hp2d_set_hazard_tracking) */
+    HP2D_FIELD_HAZARD_MAX = 14   /* velocities.hazardmax_final, depth x velocity [m^2/s] */
 } hp2d_field;
 
 typedef struct hp2d_diag {
@@ -251,6 +253,15 @@ hp2d_status hp2d_set_reservoirs(hp2d_ctx* ctx, int32_t n, const int32_t* res_row
                                 const double* k1, const double* h1, const double* k2, const int32_t* ds1_row,
                                 const int32_t* ds1_col, const double* k3, const double* h2, const double* k4,
                                 const int32_t* ds2_row, const int32_t* ds2_col);
+
+/* Velocity and hazard maxima of save_output_maps.m:588-604: each fused step keeps, per cell,
+ * the running maximum of the velocity raster max(|vel_left|, |vel_right|, |vel_up|,
+ * |vel_down|) of refreshing_timestep.m:109-111 and of snisb_velocity_hazard_snapshot's depth x
+ * velocity (0 below 0.01 m, NaN where the depth is NaN).  on = 1 starts both at zero, 0 stops
+ * them; read with HP2D_FIELD_VMAX / HP2D_FIELD_HAZARD_MAX.  The reference keeps the raster of
+ * its last velocity refresh, so the fused step's maps equal it when every step refreshes:
+ * on = 1 needs time_step_change <= min_time_step / 2.  Fused path only. */
+hp2d_status hp2d_set_hazard_tracking(hp2d_ctx* ctx, int32_t on);
 
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
 /* Hydrological_Model for this path: adds delta_p_agg (the rain of the current rain

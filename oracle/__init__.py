@@ -68,6 +68,7 @@ def _load():
                                   P(C.c_int32)], C.c_int),
             "oracle_set_reservoirs": ([vp, C.c_int32, i32p, i32p, dp, dp, dp, i32p, i32p, dp, dp, dp, i32p, i32p],
                                       C.c_int),
+            "oracle_set_hazard_tracking": ([vp, C.c_int32], C.c_int),
             "oracle_map_records": ([vp], C.c_int64),
             "oracle_download_map_record": ([vp, C.c_int64, dp, dp], C.c_int),
             "oracle_set_inflow": ([vp, C.c_int32, C.c_int32, dp, dp, C.c_int32, P(C.c_int32), P(C.c_int32),
@@ -99,7 +100,7 @@ class KernelFormOracle:
     """Same call surface as hydropol2d_b200.SurfaceFlow, computed on the CPU."""
 
     NATIVE = {"h": 0, "qx": 1, "qy": 2, "I": 3, "T": 4, "dmax": 5, "arrival": 6, "hfx": 7,
-              "hfy": 8, "hf3": 9, "qo": 10}
+              "hfy": 8, "hf3": 9, "qo": 10, "vmax": 11, "hazard_max": 12}
 
     def __init__(self, ny, nx, resolution, precision="fp32", params=None, **param_kw):
         from hydropol2d_b200 import _abi
@@ -170,6 +171,9 @@ class KernelFormOracle:
         ip = C.POINTER(C.c_int32)
         self._L.oracle_set_stage(self._h, int(d.shape[1]), int(t.size), _dp(t), _dp(d), int(rr.size),
                                  rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip))
+
+    def set_hazard_tracking(self, on=True):
+        self._L.oracle_set_hazard_tracking(self._h, 1 if on else 0)
 
     def set_reservoirs(self, res_row, res_col, k1, h1, k2, ds1_row, ds1_col, k3, h2, k4, ds2_row, ds2_col):
         i32 = [np.ascontiguousarray(a, dtype=np.int32).ravel() for a in (res_row, res_col, ds1_row, ds1_col,

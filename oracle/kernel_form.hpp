@@ -700,6 +700,30 @@ public:
 
     // ---------------- refreshing_timestep (refresh branch) ----------------
     // returns time_calculation_routing [s]; fills vmax
+    // ---------------- velocity / hazard maxima (save_output_maps.m:588-604) ----------------
+    // the velocity raster max(|vr|, |vu|, |vb|) of the last refresh, and running maxima of it
+    // and of depth x velocity (0 below 0.01 m or non-finite, NaN where the depth is NaN)
+    bool hz_on = false;
+    std::vector<R> vras, vmaxm, hzmaxm;
+    void set_hazard_tracking(bool on) {
+        hz_on = on;
+        if (on) {
+            vras.assign(h.size(), R(0));
+            vmaxm.assign(h.size(), R(0));
+            hzmaxm.assign(h.size(), R(0));
+        }
+    }
+    void track_hazard() {
+        for (size_t c = 0; c < h.size(); ++c) {
+            const R vr = vras[c];
+            vmaxm[c] = vr > vmaxm[c] ? vr : vmaxm[c];
+            const R hd = std::fmax(h[c], R(0));
+            R hz = hd * vr;
+            if (hd < R(0.01) || !std::isfinite(hz)) hz = R(0);
+            hzmaxm[c] = std::isnan(h[c]) ? h[c] : (hz > hzmaxm[c] ? hz : hzmaxm[c]);
+        }
+    }
+
     double cfl(double dts, double* vmax_out) {
         Consts<R> K(dts, res, p.depth_tolerance, p.arrival_threshold);
         std::vector<R> hf3c(h.size(), R(0));
@@ -722,6 +746,7 @@ public:
                     R sb = hfy[cb] < K.tol ? K.big_depth : hfy[cb];
                     vb = qdiv(qy[cb], sb);
                 }
+                if (hz_on) vras[c] = std::fmax(std::fmax(std::fabs(vr), std::fabs(vu)), std::fabs(vb));
                 R rc = (j == 0) ? K.half * vr : vr;
                 R uc = K.half * (vu + vb);
                 R tot = std::sqrt(rc * rc + uc * uc);
@@ -813,6 +838,7 @@ public:
         }
         apply_stage();
         track(t_min * 60.0 + dts);
+        if (hz_on) track_hazard();
         if (!rec_times.empty()) {
             const int idx = last_below(t_min + tcr / 60.0);
             if (idx > rec_last) {

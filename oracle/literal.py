@@ -430,6 +430,7 @@ class CFLResult:
     dt_adv: float
     dt_wave: float
     unstable: bool
+    velocity_raster: np.ndarray | None = None   # max |face velocity| per cell [m/s] (:109-111)
 
 
 def refreshing_timestep(Hf, qout_right, qout_up, resolution, depth_tolerance, alfa_min,
@@ -478,7 +479,7 @@ def refreshing_timestep(Hf, qout_right, qout_up, resolution, depth_tolerance, al
         new = max_time_step
     tcr = max(time_step_increments * math.floor(new / time_step_increments), min_time_step)
     tcr = min(tcr, max_time_step)
-    return CFLResult(tcr, tcr / 60, max_velocity, dt_adv, dt_wave, tcr == min_time_step)
+    return CFLResult(tcr, tcr / 60, max_velocity, dt_adv, dt_wave, tcr == min_time_step, raster)
 
 
 # --------------------------------------------------------------------------------------
@@ -527,6 +528,8 @@ class RunConfig:
     stage_cells: np.ndarray | None = None
     # reservoir / control structures (flag_reservoir = 1): the table of reservoir_transfers
     reservoirs: dict | None = None
+    # velocities.vmax_final / hazardmax_final of save_output_maps.m:588-604
+    hazard_maps: bool = False
     fixed_time_step_s: float | None = None      # bypass refreshing_timestep
 
 
@@ -697,6 +700,9 @@ class RunState:
     inflow_volume: float = 0.0
     stage_volume: float = 0.0
     structure_volume: float = 0.0
+    velocity_raster: np.ndarray | None = None    # of the last velocity refresh
+    vmax_final: np.ndarray | None = None
+    hazardmax_final: np.ndarray | None = None
     # rain interval [rain_a, rain_b] of the current step and the loop's t_previous [min]; the
     # first step's comes from the call before the loop (HydroPol2D_Main_While.m:115) with
     # t_previous = 0 (:120)
@@ -704,6 +710,19 @@ class RunState:
     rain_b: float = 0.0
     t_previous: float = 0.0
     history: list = field(default_factory=list)
+
+
+def velocity_hazard_snapshot(velocity_raster, depth_mm, idx_nan) -> np.ndarray:
+    """snisb_velocity_hazard_snapshot (save_output_maps.m:832-848), the hazard output: depth [m]
+    x velocity [m/s], 0 below 0.01 m and where non-finite, NaN on idx_nan cells."""
+    depth_m = np.fmax(np.asarray(depth_mm, dtype=np.float64) / 1000, 0)
+    v = np.array(velocity_raster, dtype=np.float64) + np.zeros(depth_m.shape)
+    v[~np.isfinite(v)] = 0
+    hazard = depth_m * v
+    hazard[depth_m < 0.01] = 0
+    hazard[~np.isfinite(hazard)] = 0
+    hazard[idx_nan] = np.nan
+    return hazard
 
 
 def init_state(cfg: RunConfig) -> RunState:
@@ -781,6 +800,17 @@ def step(cfg: RunConfig, st: RunState) -> None:
         for i in range(depth.shape[1]):
             out.d_t[np.asarray(cfg.stage_cells[i], dtype=bool)] = 1000.0 * depth[z2, i]
         st.stage_volume += float(np.nansum(out.d_t - before)) * A / 1000
+    if cfg.hazard_maps:   # save_output_maps.m:588-604 with snisb_velocity_hazard_snapshot (:832-848)
+        if cfl is not None:
+            st.velocity_raster = cfl.velocity_raster
+        hazard = velocity_hazard_snapshot(st.velocity_raster, out.d_t, np.isnan(cfg.z))
+        if st.k == 1:
+            st.vmax_final = np.array(st.velocity_raster, dtype=np.float64)
+            st.hazardmax_final = hazard
+        else:
+            st.vmax_final = np.fmax(st.velocity_raster, st.vmax_final)
+            st.hazardmax_final = np.fmax(hazard, st.hazardmax_final)
+            st.hazardmax_final[np.isnan(hazard) & np.isnan(st.hazardmax_final)] = np.nan
     # save_output_maps.m:588-600 (running maximum depth) + arrival-time definition
     t_end_s = st.t * 60 + time_step * 60
     newly = (st.dmax < cfg.arrival_threshold_mm) & (out.d_t >= cfg.arrival_threshold_mm)

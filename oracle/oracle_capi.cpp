@@ -83,6 +83,10 @@ int oracle_set_reservoirs(oracle_model* m, int32_t n, const int32_t* rr, const i
     return dispatch(m, [&](auto& M) { M.set_reservoirs(n, rr, rc, k1, h1, k2, d1r, d1c, k3, h2, k4, d2r, d2c); return 0; });
 }
 
+int oracle_set_hazard_tracking(oracle_model* m, int32_t on) {
+    return dispatch(m, [&](auto& M) { M.set_hazard_tracking(on != 0); return 0; });
+}
+
 int oracle_set_map_records(oracle_model* m, int32_t n, const double* times) {
     return dispatch(m, [&](auto& M) { M.set_map_records(n, times); return 0; });
 }
@@ -170,7 +174,8 @@ int oracle_run(oracle_model* m, int64_t max_steps, int64_t* done) {
 
 // Raw state in the internal units and precision (for bit-exact comparison).
 //   0 h [m], 1 qx [m^2/s], 2 qy, 3 I [m], 4 T [s], 5 dmax [m], 6 arrival [s],
-//   7 Hf_x [m], 8 Hf_y [m], 9 Hf3 per outlet, 10 outlet rate per outlet [m/s]
+//   7 Hf_x [m], 8 Hf_y [m], 9 Hf3 per outlet, 10 outlet rate per outlet [m/s],
+//   11 velocity maximum [m/s], 12 hazard maximum [m^2/s]
 int oracle_download_native(oracle_model* m, int32_t field, void* out, size_t bytes) {
     return dispatch(m, [&](auto& M) {
         using R = typename std::remove_reference<decltype(M.h[0])>::type;
@@ -187,6 +192,8 @@ int oracle_download_native(oracle_model* m, int32_t field, void* out, size_t byt
             case 8: src = &M.hfy; break;
             case 9: src = &M.hf3; break;
             case 10: src = &M.qo; break;
+            case 11: src = &M.vmaxm; break;
+            case 12: src = &M.hzmaxm; break;
             default: return int(HP2D_INVALID_ARG);
         }
         if (bytes != src->size() * sizeof(R)) return int(HP2D_INVALID_ARG);
