@@ -282,6 +282,8 @@ def main():
     sf.fused_steps(args.warmup)
     if dist is not None:
         dist.barrier()
+    d0 = sf.diag()
+    skip0, skipr0 = d0["skipped_cells"], d0["skipped_read_cells"]
     with ClockSampler(local) as clocks:
         ms = sf.fused_steps_timed(args.steps)
     if dist is not None:
@@ -291,6 +293,11 @@ def main():
     ms_per_step = ms / args.steps
     value = cells * args.steps * world / (ms / 1e3) / 1e9
     d = sf.diag()
+    # deep-dry rows whose records the output buffer already held were not stored again
+    skip_frac = (d["skipped_cells"] - skip0) / (cells * args.steps)
+    # ... and whole dry row blocks were neither read nor written
+    skipr_frac = (d["skipped_read_cells"] - skipr0) / (cells * args.steps)
+    req_bpc = BYTES_PER_CELL - 32.0 * skipr_frac - 16.0 * skip_frac
     wet_main = float(np.mean(sf.download_native("h") > 0))
     late = None
     if args.late_steps > 0:
@@ -338,7 +345,8 @@ def main():
         e2e = cells * e2e_steps * world / float(t.item()) / 1e9
 
     peak, peak_kind = load_peaks()
-    achieved = BYTES_PER_CELL * cells / (ms_per_step / 1e3) / 1e9
+    # bytes the step must move: the dense 48 B per cell less the records it skipped
+    achieved = req_bpc * cells / (ms_per_step / 1e3) / 1e9
     traffic_pc = load_traffic()
 
     ens = None
@@ -368,7 +376,9 @@ def main():
                    "wet_fraction": wet_main},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_cell": BYTES_PER_CELL,
+                     "algorithmic_bytes_per_cell": req_bpc,
+                     "dense_bytes_per_cell": BYTES_PER_CELL,
+                     "write_skip_fraction": skip_frac, "read_skip_fraction": skipr_frac,
                      "traffic": None if traffic_pc is None else traffic_pc * cells},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d_per_step,

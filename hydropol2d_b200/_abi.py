@@ -91,7 +91,7 @@ class Diag(C.Structure):
         ("status_bits", C.c_int64),
         ("rain_t0", C.c_double), ("rain_t1", C.c_double), ("t_previous", C.c_double),
         ("inflow_volume", C.c_double), ("stage_volume", C.c_double),
-        ("structure_volume", C.c_double),
+        ("structure_volume", C.c_double), ("skipped_cells", C.c_int64), ("skipped_read_cells", C.c_int64),
     ]
 
 

@@ -1022,6 +1022,8 @@ template <typename R> struct Impl : Base {
         a.inflow = inflow;
         a.rec = rec;
         a.strct = strct;
+        a.dry_rows = dry_rows();
+        a.dryflag = (rpw % 4 == 0 && rpw <= 128) ? dryf.p : nullptr;
         a.vmax = hz_on ? vmaxm.p : nullptr;
         a.hzmax = hz_on ? hzmaxm.p : nullptr;
         a.sc = sc.p;
@@ -1035,7 +1037,7 @@ template <typename R> struct Impl : Base {
         const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
         int dev = 0;
         HP_CK(cudaGetDevice(&dev));
-        if (sm > 48 * 1024 && dev < 8 && !done[dev]) {
+        if (sm > 40 * 1024 && dev < 8 && !done[dev]) {   // the static shared memory counts too
             HP_CK(cudaFuncSetAttribute(k_fused_step<R, kThreads, INF, MAP, CPL, INFL>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
             done[dev] = true;
@@ -1109,8 +1111,27 @@ template <typename R> struct Impl : Base {
         graph_steps = 0;
     }
 
+    // Dry-row flags of the fused step ([2][ny][strips of the narrowest layout]): zero is always
+    // valid ("not known to hold the dry record"); they are cleared whenever something other
+    // than a fused step of the current layout wrote the state buffers.
+    Dev<unsigned char> dryf;
+    int dry_layout = -1;
+    int dry_rows() const { return (ny + 3) & ~3; }
+    void reset_dry() {
+        if (!dryf.p) dryf.alloc(2 * size_t(dry_rows()) * size_t((nx + 27) / 28));
+        HP_CK(cudaMemsetAsync(dryf.p, 0, dryf.n, st()));
+    }
+    void dry_for_layout(int cpl) {
+        if (dry_layout != cpl || !dryf.p) {
+            reset_dry();
+            dry_layout = cpl;
+        }
+    }
+
     void prologue() {
+        dry_for_layout(cells_per_lane);
         if (!dirty) return;
+        reset_dry();
         pull_sc();
         hs.skip_clamp = 0;
         hs.counter = 0;
@@ -1223,6 +1244,7 @@ template <typename R> struct Impl : Base {
         }
         s.scs.alloc(1);
         copy_dev(s.scs.p, sc.p, 1);
+        reset_dry();   // trial layouts may differ from the current one
         HP_CK(cudaStreamSynchronize(st()));
     }
     void put_back(const Snapshot& s) {
@@ -1233,6 +1255,7 @@ template <typename R> struct Impl : Base {
         copy_dev(arrival.p, s.arr.p, n);
         if (n_out) { copy_dev(hf3.p, s.hf3s.p, n_out); copy_dev(qo.p, s.qos.p, n_out); }
         copy_dev(sc.p, s.scs.p, 1);
+        reset_dry();
         HP_CK(cudaStreamSynchronize(st()));
         pull_sc();
     }
@@ -1429,6 +1452,8 @@ template <typename R> struct Impl : Base {
         o->inflow_volume = hs.inflow_vol;
         o->stage_volume = hs.stage_vol;
         o->structure_volume = hs.struct_vol;
+        o->skipped_cells = int64_t(hs.skipped_cells);
+        o->skipped_read_cells = int64_t(hs.skipped_read_cells);
         o->max_velocity = hs.vmax_last;
         o->rain_volume = hs.rain_vol;
         o->infiltration_volume = hs.inf_vol;
@@ -1560,6 +1585,7 @@ struct hp2d_ensemble {
                 im.invalidate_graph();
             }
             im.prologue();
+            im.dry_for_layout(cells_per_lane);   // the ensemble's layout may differ from the member's
             HP_CK(cudaStreamSynchronize(im.st()));
             host[m] = im.fused_args(cells_per_lane);
         }

@@ -155,6 +155,10 @@ struct StepScalars {
     long long rec_count;
     int rec_last, rec_pending;
     double struct_vol;     // cumulative volume the control structures added [m^3]
+    unsigned long long skipped_cells;   // cumulative cell records a fused step found unchanged
+                                        // in its output buffer and did not rewrite
+    unsigned long long skipped_read_cells;   // of those, cells of whole skipped row blocks
+                                             // (their records were not read either)
 };
 
 // ---------------- map records (save_output_maps.m) -----------------------------------

@@ -82,6 +82,12 @@ template <typename R> struct FusedArgs {
     RecordDesc<R> rec;
     StructDesc<R> strct;         // reservoir / control structures (n = 0: none)
     R* vmax; R* hzmax;           // velocity / hazard maxima [m/s], [m^2/s] (null: not tracked)
+    // [2][n_strips][dry_rows]: 1 when a deep-dry row of the strip wrote its records into state
+    // buffer b; the same row deep-dry again two steps later would write identical values
+    // (null: off; dry_rows is ny rounded up to a multiple of 4, rows_per_warp <= 128 and a
+    // multiple of 4, so that a warp reads its rows' flags as one word per lane)
+    unsigned char* dryflag;
+    int dry_rows;
     StepScalars* sc;
 };
 
@@ -224,6 +230,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     __shared__ int s_negn;   // an outlet cell would go below -1e-11 m after the next rain
     __shared__ int s_rec;    // slot that receives this step's input depth (-1: none)
     __shared__ double s_stage;   // depth the stage overwrites of this CTA added [m]
+    __shared__ unsigned s_skipw;  // cells whose unchanged record this CTA did not rewrite
+    __shared__ unsigned s_skipr;  // of those, cells of skipped blocks (not read either)
     __shared__ RainStep<R> s_rs, s_rsn;   // this step's rain and the next one's
     __shared__ R red_s2[NT / 32];
     __shared__ unsigned long long red_c[NT / 32];
@@ -242,6 +250,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         s_skip = sc->skip_clamp;
         s_negn = 0;
         s_stage = 0.0;
+        s_skipw = 0u;
+        s_skipr = 0u;
         s_rec = (sc->rec_pending && a.rec.n_slots > 0) ? int(sc->rec_count % a.rec.n_slots) : -1;
         s_done = !(s_tmin <= a.t_end);
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
@@ -292,6 +302,46 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         }
         const int r0 = rb * a.rows_per_warp;
         const int r_end = min(r0 + a.rows_per_warp, ny);
+        unsigned char* const dfl =
+            a.dryflag ? a.dryflag + (size_t(cur ^ 1) * a.n_strips + strip) * size_t(a.dry_rows) : nullptr;
+        unsigned own_n = 0;   // cells of the strip this warp stores
+#pragma unroll
+        for (int h = 0; h < CPL; ++h) own_n += __popc(__ballot_sync(FULL, own_lane[h]));
+        // the flags of this warp's rows, four per lane (read once: each row's flag changes only
+        // at that row)
+        unsigned dfw = 0u;
+        if (dfl && r0 + 4 * lane < r_end) dfw = *reinterpret_cast<const unsigned*>(dfl + r0 + 4 * lane);
+        // The whole block of rows: when this step adds no water (no rain, infiltration or
+        // boundary cells) and records no map, and the flags show every input row r0-1..r_end+1
+        // of this strip and of its neighbours (the 2-column aprons) deep-dry and every output
+        // row already holding the record the deep-dry path would write, the loop below would
+        // store nothing and contribute nothing: skip it, copies included.
+        bool blk_skip = false;
+        if constexpr (INF == 0 && !MAP && !INFL) {
+            if (dfl && s_rec < 0 && RS.depth == R(0) && K.thr > R(0)) {
+                const int nrow = r_end - r0;
+                const int nb = min(max(nrow - 4 * lane, 0), 4);
+                const unsigned mask = nb == 4 ? 0xffffffffu : (1u << (8 * nb)) - 1u;
+                const unsigned want = 0x01010101u & mask;
+                bool ok = (dfw & mask) == want;
+                const unsigned char* fin = a.dryflag + size_t(cur) * a.n_strips * size_t(a.dry_rows);
+                for (int q = max(strip - 1, 0); q <= min(strip + 1, a.n_strips - 1); ++q) {
+                    const unsigned char* fq = fin + size_t(q) * a.dry_rows;
+                    if (nb > 0) ok = ok && (*reinterpret_cast<const unsigned*>(fq + r0 + 4 * lane) & mask) == want;
+                    if (lane < 3) {
+                        const int rr = lane == 0 ? r0 - 1 : r_end + lane - 1;
+                        if (rr >= 0 && rr < ny) ok = ok && fq[rr] == 1;
+                    }
+                }
+                blk_skip = __all_sync(FULL, ok);
+            }
+        }
+        if (blk_skip) {
+            if (lane == 0) {
+                atomicAdd(&s_skipw, own_n * unsigned(r_end - r0));
+                atomicAdd(&s_skipr, own_n * unsigned(r_end - r0));
+            }
+        } else {
 
         // rolling window (suffix = rows back), one entry per cell of the lane
         R hT1[CPL], hT2[CPL], qxu1[CPL], qyu1[CPL], hfx1[CPL], hfx2[CPL], hfy1[CPL], hfy2[CPL];
@@ -355,6 +405,10 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         for (int k = 0; k <= last_k; ++k) {
             const int r = r0 - 2 + k;
             const int s = k % kStages;
+            // the dry flag of the output row r-2 in the buffer this step writes
+            const bool frow_f = r - 2 >= r0 && r - 2 < r_end;
+            const int fri = frow_f ? r - 2 - r0 : 0;
+            const unsigned flg = frow_f ? (__shfl_sync(FULL, dfw, fri >> 2) >> (8 * (fri & 3))) & 255u : 0u;
             const bool landed = mbar_wait_bounded(bar0 + 8u * s, uint32_t((k / kStages) & 1), 1u << 22);
             if (__any_sync(FULL, !landed)) {   // the whole warp leaves the loop together
                 timed_out = true;
@@ -438,7 +492,11 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 for (int h = 0; h < CPL; ++h) plain = plain && (mt2[h] >> 8) == 0u;
                 if (__all_sync(FULL, plain)) {
                     const int rm2 = r - 2;
-                    if (rm2 >= r0 && rm2 < r_end) {
+                    if (frow_f && flg) {
+                        // this buffer already holds the row as this step would write it (the
+                        // same deep-dry row two steps ago; nothing else wrote the buffer since)
+                        if (lane == 0) atomicAdd(&s_skipw, own_n);
+                    } else if (frow_f) {
 #pragma unroll
                         for (int h = 0; h < CPL; ++h)
                             if (own_lane[h]) {
@@ -449,6 +507,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                                 o4.w = R(0) > dm2[h] ? R(0) : dm2[h];
                                 sout[size_t(rm2) * nx + j[h]] = o4;
                             }
+                        if (dfl && lane == 0) dfl[rm2] = 1;
                     }
 #pragma unroll
                     for (int h = 0; h < CPL; ++h) {
@@ -590,6 +649,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     }
                 }
             }
+            if (flg && lane == 0) dfl[r - 2] = 0;   // rewritten: no longer known dry
             // (G) shift the window down one row
 #pragma unroll
             for (int h = 0; h < CPL; ++h) {
@@ -608,6 +668,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         __syncwarp();
         if (lane == 0 && !timed_out)
             for (int s = 0; s < kStages; ++s) mbar_inval(bar0 + 8u * s);
+        }  // !blk_skip
     }
 
     // ---- CTA reductions ---------------------------------------------------------------
@@ -654,6 +715,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         if (out_acc != 0.0) atomicAdd(&sc->acc_out, out_acc);
         if (negn) atomicOr(&sc->skip_next, 1);
         if (INFL && s_stage != 0.0) atomicAdd(&sc->acc_stage, s_stage);
+        if (s_skipw) atomicAdd(&sc->skipped_cells, (unsigned long long)s_skipw);
+        if (s_skipr) atomicAdd(&sc->skipped_read_cells, (unsigned long long)s_skipr);
         __threadfence();
         const unsigned int ticket = atomicAdd(&sc->counter, 1u);
         s_last = (ticket == a.n_ctas - 1);

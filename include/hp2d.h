@@ -114,6 +114,10 @@ typedef struct hp2d_diag {
     double inflow_volume;         /* cumulative inflow-hydrograph volume [m^3] */
     double stage_volume;          /* cumulative volume the stage overwrites added [m^3] */
     double structure_volume;      /* cumulative volume the control structures added [m^3] */
+    int64_t skipped_cells;        /* cumulative cell records the fused step found already
+                                     written (dry rows) and did not store again */
+    int64_t skipped_read_cells;   /* of those, cells of whole dry row blocks whose records
+                                     were not read either */
 } hp2d_diag;
 
 typedef struct hp2d_ctx hp2d_ctx;

@@ -237,6 +237,8 @@ int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
         o->inflow_volume = M.inflow_vol;
         o->stage_volume = M.stage_vol;
         o->structure_volume = M.struct_vol;
+        o->skipped_cells = 0;
+        o->skipped_read_cells = 0;
         return 0;
     });
 }
