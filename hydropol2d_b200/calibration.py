@@ -1,5 +1,5 @@
-"""Calibration on the batched ensemble: every candidate parameter set of a generation is one
-member of one ``Ensemble`` run.
+"""Calibration and sensitivity analysis on the batched ensemble: every candidate parameter set
+of a generation (or every one-at-a-time variation) is one member of one ``Ensemble`` run.
 
 Automatic_Calibrator_HydroPol2D.m minimises Objective_Function_HydroPol2D.m over the
 parameters with MATLAB's genetic algorithm, one model run per candidate.  Here a generation's
@@ -60,10 +60,13 @@ def discharge_at(times_min: np.ndarray, t_samples: Sequence[float], v_samples: S
     return (vol - vprev) / ((times - prev) * 60.0)
 
 
-def ensemble_hydrographs(cases: Sequence, times_min: np.ndarray, device: int = 0, chunk: int = 32) -> np.ndarray:
-    """Runs ``cases`` (FP32 ``synthetic.Case``s on grids of any size) as one batched ensemble
-    and returns their outlet discharges at the observation times, (members, n_times).  Each
-    member's cumulative outlet volume is sampled after every ``chunk`` launches."""
+def ensemble_runs(cases: Sequence, times_min: np.ndarray, device: int = 0, chunk: int = 32,
+                  flood_depth_m: float | None = None) -> dict:
+    """Runs ``cases`` (FP32 ``synthetic.Case``s on grids of any size) as one batched ensemble.
+    Returns the outlet discharges at the observation times ("q", (members, n_times)) from each
+    member's cumulative outlet volume sampled after every ``chunk`` launches and, with
+    ``flood_depth_m``, the largest flooded area seen at those samples ("flooded_area" [m^2]:
+    cells deeper than it x cell area, the Flooded_Area of save_output_maps.m:451 with 150 mm)."""
     from .ensemble import Ensemble
     from .surface import SurfaceFlow
     ens = Ensemble(device)
@@ -73,16 +76,61 @@ def ensemble_hydrographs(cases: Sequence, times_min: np.ndarray, device: int = 0
             c.apply(m)
             ens.add(m)
         samples = [([], []) for _ in cases]
+        area = np.zeros(len(cases))
         active = len(cases)
         while active:
             active = ens.steps(chunk)
-            for s, m in zip(samples, ens.members):
+            for i, (s, m) in enumerate(zip(samples, ens.members)):
                 d = m.diag()
                 s[0].append(d["t"])
                 s[1].append(d["outlet_volume"])
-        return np.stack([discharge_at(times_min, ts, vs) for ts, vs in samples])
+                if flood_depth_m is not None:
+                    wet = np.count_nonzero(m.download_native("h") > flood_depth_m)
+                    area[i] = max(area[i], wet * m.resolution ** 2)
+        out = {"q": np.stack([discharge_at(times_min, ts, vs) for ts, vs in samples])}
+        if flood_depth_m is not None:
+            out["flooded_area"] = area
+        return out
     finally:
         ens.close()
+
+
+def ensemble_hydrographs(cases: Sequence, times_min: np.ndarray, device: int = 0, chunk: int = 32) -> np.ndarray:
+    """Outlet discharges of ``cases`` at the observation times, (members, n_times)."""
+    return ensemble_runs(cases, times_min, device, chunk)["q"]
+
+
+def hydrograph_metrics(q: np.ndarray, dt_min: float) -> dict:
+    """Sensitivity_Analysis_HydroPol2D.m:152-157 for hydrographs sampled every ``dt_min``:
+    peak flow [m^3/s], volume sum(q dt 60) [m^3] and time to peak (first maximum, samples
+    from 0) [min]; ``q`` is (..., n_times)."""
+    q = np.asarray(q, dtype=np.float64)
+    return {"peak": q.max(axis=-1), "volume": (q * dt_min * 60.0).sum(axis=-1),
+            "time_to_peak": np.argmax(q, axis=-1) * dt_min}
+
+
+def sensitivity_oat(make_case: Callable[[dict], object], base: dict, names: Sequence[str],
+                    factors: Sequence[float], times_min: np.ndarray, device: int = 0, chunk: int = 16,
+                    flood_depth_m: float = 0.15) -> dict:
+    """One-at-a-time sensitivity (Sensitivity_Analysis_HydroPol2D.m:82-171): every parameter in
+    ``names`` is scaled by every factor while the others keep their ``base`` values; the
+    baseline and all variations run as ONE batched ensemble.  Returns, per output, the
+    percentage change against the baseline as (len(names), len(factors)) arrays ("peak",
+    "volume", "time_to_peak", "flooded_area"), plus the baseline outputs."""
+    times_min = np.asarray(times_min, dtype=np.float64)
+    dt = float(times_min[1] - times_min[0])
+    variants = [dict(base)]
+    for n in names:
+        for f in factors:
+            variants.append(dict(base, **{n: base[n] * f}))
+    runs = ensemble_runs([make_case(v) for v in variants], times_min, device, chunk, flood_depth_m)
+    m = hydrograph_metrics(runs["q"], dt)
+    m["flooded_area"] = runs["flooded_area"]
+    out = {"baseline": {k: float(v[0]) for k, v in m.items()}}
+    for k, v in m.items():
+        b = v[0]
+        out[k] = ((v[1:] - b) / b * 100.0).reshape(len(names), len(factors))
+    return out
 
 
 def calibrate(evaluate: Callable[[np.ndarray], np.ndarray], lower: Sequence[float], upper: Sequence[float],

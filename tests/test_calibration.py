@@ -70,3 +70,12 @@ def test_calibrate_finds_box_minimum_and_is_seeded():
     # the best objective never gets worse from one generation to the next (elitism)
     bests = [h[1].min() for h in r["history"]]
     assert all(b1 <= b0 for b0, b1 in zip(bests, bests[1:]))
+
+
+def test_hydrograph_metrics_by_hand():
+    from hydropol2d_b200.calibration import hydrograph_metrics
+    q = np.array([[0.0, 2.0, 5.0, 5.0, 1.0], [1.0, 1.0, 1.0, 1.0, 1.0]])
+    m = hydrograph_metrics(q, 2.0)
+    assert list(m["peak"]) == [5.0, 1.0]
+    assert list(m["volume"]) == [13.0 * 120.0, 5.0 * 120.0]
+    assert list(m["time_to_peak"]) == [4.0, 0.0]      # first maximum, samples counted from 0

@@ -42,3 +42,22 @@ def test_roughness_recovered_from_outlet_hydrograph():
     assert calls == [12, 12, 12]
     assert abs(r["x"][0] - TRUE_N) < 0.1 * TRUE_N
     assert r["objective"] < -0.98
+
+
+def test_one_at_a_time_sensitivity():
+    """Rougher planes delay and flatten the outlet peak; more rain raises peak, volume and the
+    flooded area -- the baseline and the 6 variations run as one ensemble."""
+    from hydropol2d_b200.calibration import sensitivity_oat
+
+    def make(p):
+        base = synthetic.vtilt_case(48, 48, 10.0)
+        rain = (np.array([0.0, 20.0]), np.array([p["rain"], 0.0]))
+        return replace(base, roughness=np.full(base.shape, p["n"]), rain_uniform=rain,
+                       params={**base.params, "routing_time": 30.0})
+
+    r = sensitivity_oat(make, {"n": 0.03, "rain": 100.0}, ["n", "rain"], [0.5, 1.0, 1.5], TIMES[:15])
+    assert r["peak"].shape == (2, 3)
+    assert abs(r["peak"][0, 1]) < 1e-6 and abs(r["volume"][1, 1]) < 1e-6      # factor 1 = baseline
+    assert r["peak"][0, 0] > 0 > r["peak"][0, 2]                              # smoother -> higher peak
+    assert r["peak"][1, 2] > 0 and r["volume"][1, 2] > 30.0                    # more rain
+    assert r["flooded_area"][1, 2] >= 0 and r["baseline"]["flooded_area"] >= 0
