@@ -19,6 +19,7 @@
 #include <limits>
 #include <memory>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -1324,14 +1325,53 @@ template <typename R> struct Impl : Base {
 
     // ---------------- outputs ----------------
     // one component of the current state records (a quarter of the record bytes cross)
-    std::vector<R> fetch_component(int comp) {
+    // Device -> caller's double array, times `scale`, through two 4 MB pinned staging buffers:
+    // the copy of one chunk overlaps the conversion of the previous one, and no pageable
+    // staging or large host allocation sits in the path.
+    // The two staging buffers are shared by every context of the process (portable pinned
+    // memory, one reader at a time); the events are the context's own.
+    struct StageEvents {
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        ~StageEvents() {
+            for (auto e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    };
+    StageEvents stage_ev;
+    static constexpr size_t kStageBytes = size_t(4) << 20;
+    static constexpr size_t kStageElems = kStageBytes / sizeof(R);
+    void fetch_scaled(const R* src, size_t count, double scale, double* out) {
+        static std::mutex mu;
+        static void* buf[2] = {nullptr, nullptr};
+        std::lock_guard<std::mutex> lock(mu);
+        for (int b = 0; b < 2; ++b) {
+            if (!buf[b]) HP_CK(cudaHostAlloc(&buf[b], kStageBytes, cudaHostAllocPortable));
+            if (!stage_ev.ev[b]) HP_CK(cudaEventCreateWithFlags(&stage_ev.ev[b], cudaEventDisableTiming));
+        }
+        const size_t nch = (count + kStageElems - 1) / kStageElems;
+        auto issue = [&](size_t c) {
+            const size_t off = c * kStageElems, m = std::min(kStageElems, count - off);
+            HP_CK(cudaMemcpyAsync(buf[c & 1], src + off, m * sizeof(R), cudaMemcpyDeviceToHost, st()));
+            HP_CK(cudaEventRecord(stage_ev.ev[c & 1], st()));
+        };
+        if (nch) issue(0);
+        for (size_t c = 0; c < nch; ++c) {
+            if (c + 1 < nch) issue(c + 1);   // its buffer held chunk c-1, converted already
+            HP_CK(cudaEventSynchronize(stage_ev.ev[c & 1]));
+            const R* v = static_cast<const R*>(buf[c & 1]);
+            const size_t off = c * kStageElems, m = std::min(kStageElems, count - off);
+            for (size_t k = 0; k < m; ++k) out[off + k] = double(v[k]) * scale;
+        }
+    }
+    void fetch_component_scaled(int comp, double scale, double* out) {
         pull_sc();
         Dev<R> tmp;
         tmp.alloc(n);
         k_state_component<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, comp, tmp.p);
         HP_CK(cudaGetLastError());
-        return fetch(tmp.p, n);
+        fetch_scaled(tmp.p, n, scale, out);
     }
+
     std::vector<V4> fetch_state() {
         pull_sc();
         return fetch(st4[hs.cur].p, n);
@@ -1348,9 +1388,9 @@ template <typename R> struct Impl : Base {
             for (int o = 0; o < n_out; ++o) out[cells[o]] = double(v[o]) * scale_;
         };
         switch (field) {
-            case HP2D_FIELD_DEPTH: { auto v = fetch_component(0); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0; break; }
-            case HP2D_FIELD_QOUT_RIGHT: { auto v = fetch_component(1); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * to_mmh; break; }
-            case HP2D_FIELD_QOUT_UP: { auto v = fetch_component(2); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * to_mmh; break; }
+            case HP2D_FIELD_DEPTH: fetch_component_scaled(0, 1000.0, out); break;
+            case HP2D_FIELD_QOUT_RIGHT: fetch_component_scaled(1, to_mmh, out); break;
+            case HP2D_FIELD_QOUT_UP: fetch_component_scaled(2, to_mmh, out); break;
             case HP2D_FIELD_QOUT_LEFT: {
                 auto v = fetch_state();
                 for (int i = 0; i < ny; ++i)
@@ -1373,12 +1413,11 @@ template <typename R> struct Impl : Base {
                 break;
             }
             case HP2D_FIELD_HF_OUTLET: per_outlet_map(hf3, 1.0); break;
-            case HP2D_FIELD_DMAX: { auto v = fetch_component(3); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) * 1000.0; break; }
+            case HP2D_FIELD_DMAX: fetch_component_scaled(3, 1000.0, out); break;
             case HP2D_FIELD_ARRIVAL: { auto v = fetch(arrival.p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) / 60.0; break; }
             case HP2D_FIELD_VMAX: case HP2D_FIELD_HAZARD_MAX: {
                 if (!hz_on) { ctx->err = "velocity / hazard maxima are off (hp2d_set_hazard_tracking)"; return HP2D_NOT_READY; }
-                auto v = fetch(field == HP2D_FIELD_VMAX ? vmaxm.p : hzmaxm.p, n);
-                for (size_t k = 0; k < n; ++k) out[k] = double(v[k]);
+                fetch_scaled(field == HP2D_FIELD_VMAX ? vmaxm.p : hzmaxm.p, n, 1.0, out);
                 break;
             }
             case HP2D_FIELD_SOIL_STORAGE: {
