@@ -311,13 +311,16 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         // at that row)
         unsigned dfw = 0u;
         if (dfl && r0 + 4 * lane < r_end) dfw = *reinterpret_cast<const unsigned*>(dfl + r0 + 4 * lane);
-        // The whole block of rows: when this step adds no water (no rain, infiltration or
-        // boundary cells) and records no map, and the flags show every input row r0-1..r_end+1
-        // of this strip and of its neighbours (the 2-column aprons) deep-dry and every output
-        // row already holding the record the deep-dry path would write, the loop below would
-        // store nothing and contribute nothing: skip it, copies included.
+        // The whole block of rows: when this step adds no rain and no infiltration and records
+        // no map, and the flags show every input row r0-1..r_end+1 of this strip and of its
+        // neighbours (the 2-column aprons) deep-dry and every output row already holding the
+        // record the deep-dry path would write, the loop below would store nothing and
+        // contribute nothing: skip it, copies included.  (A flag is only ever set on a row
+        // whose 64 columns hold no outlet or boundary cell, so no inflow, stage or structure
+        // water can reach the rows the flags cover, and the deep-dry path updates no velocity
+        // or hazard maximum.)
         bool blk_skip = false;
-        if constexpr (INF == 0 && !MAP && !INFL) {
+        if constexpr (INF == 0 && !MAP) {
             if (dfl && s_rec < 0 && RS.depth == R(0) && K.thr > R(0)) {
                 const int nrow = r_end - r0;
                 const int nb = min(max(nrow - 4 * lane, 0), 4);

@@ -30,6 +30,7 @@ def test_maxima_bit_exact(precision, hp2d_lib, oracle_lib):
         assert same_bits(vg, o.download_native("vmax").astype(np.float64)), chunk
         assert same_bits(hg, o.download_native("hazard_max").astype(np.float64)), chunk
     assert np.nanmax(vg) > 1.0 and np.nanmax(hg) > 1.0
+    assert g.diag()["skipped_read_cells"] > 0     # dry blocks skipped with the maxima on
 
 
 def test_structures_and_hazard_together(hp2d_lib, oracle_lib):
