@@ -1122,10 +1122,17 @@ template <typename R> struct Impl : Base {
         if (!dryf.p) dryf.alloc(2 * size_t(dry_rows()) * size_t((nx + 27) / 28));
         HP_CK(cudaMemsetAsync(dryf.p, 0, dryf.n, st()));
     }
+    // the launches use the flags only with rows per warp a multiple of 4 up to 128; launches
+    // without them do not maintain them, so any change of layout or of flag use clears them
+    int dry_key(int cpl) {
+        const int rpw = rpw_chosen ? rows_per_warp : default_rows(cpl);
+        return (rpw % 4 == 0 && rpw <= 128) ? cpl : -cpl;
+    }
     void dry_for_layout(int cpl) {
-        if (dry_layout != cpl || !dryf.p) {
+        const int key = dry_key(cpl);
+        if (dry_layout != key || !dryf.p) {
             reset_dry();
-            dry_layout = cpl;
+            dry_layout = key;
         }
     }
 

@@ -29,7 +29,8 @@ def test_long_run_bit_exact(precision, hp2d_lib, oracle_lib):
 def test_layout_switches_and_host_writes(hp2d_lib, oracle_lib):
     case = S.dambreak_case(48, 320, 5.0, seed=4, hours=0.2)
     g, o = make_pair(case, "fp32")
-    for step, action in enumerate(["layout1", "layout2", "state", "tuning", "autotune", "layout1"]):
+    for step, action in enumerate(["layout1", "layout2", "state", "tuning16", "tuning5", "tuning40", "autotune",
+                                   "layout1"]):
         g.fused_steps(97)
         o.fused_steps(97)
         assert_same_state(g, o, FIELDS, f"before {action}")
@@ -41,8 +42,8 @@ def test_layout_switches_and_host_writes(hp2d_lib, oracle_lib):
             of = np.stack([g.download("qout_right"), g.download("qout_up")])
             g.set_state(d, of)
             o.set_state(d, of)
-        elif action == "tuning":
-            g.set_tuning(16)
+        elif action.startswith("tuning"):
+            g.set_tuning(int(action[6:]))   # 5 rows per warp: launches without the flags
         else:
             g.autotune(3)
         g.fused_steps(33)
