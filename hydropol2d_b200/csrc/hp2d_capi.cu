@@ -988,6 +988,7 @@ template <typename R> struct Impl : Base {
         HP_CK(cudaGetLastError());
         pack();
         HP_CK(cudaStreamSynchronize(st()));
+        dirty = true;   // the records were rewritten from outside a fused step
         return HP2D_OK;
     }
 
