@@ -299,6 +299,16 @@ def main():
     skipr_frac = (d["skipped_read_cells"] - skipr0) / (cells * args.steps)
     req_bpc = BYTES_PER_CELL - 32.0 * skipr_frac - 16.0 * skip_frac
     wet_main = float(np.mean(sf.download_native("h") > 0))
+    # the same window with the dry skips off, on a second context from the same inputs: every
+    # row read, stepped and written (bit-identical results)
+    dn = SurfaceFlow(ny, nx, DX, "fp32", device=local, **case.params)
+    case.apply(dn)
+    dn.set_dry_skip(False)
+    dn.fused_steps(args.warmup)
+    ms_dense = dn.fused_steps_timed(args.steps)
+    dn.close()
+    dense = {"value": cells * args.steps / (ms_dense / 1e3) / 1e9, "ms_per_step": ms_dense / args.steps,
+             "achieved_gbs": BYTES_PER_CELL * cells / (ms_dense / args.steps / 1e3) / 1e9}
     late = None
     if args.late_steps > 0:
         # the same run later on, once the flood wave has spread over more of the valley
@@ -345,6 +355,7 @@ def main():
         e2e = cells * e2e_steps * world / float(t.item()) / 1e9
 
     peak, peak_kind = load_peaks()
+    dense["hbm_frac"] = dense["achieved_gbs"] / peak   # 48 B/cell streamed, of measured HBM
     # bytes the step must move: the dense 48 B per cell less the records it skipped
     achieved = req_bpc * cells / (ms_per_step / 1e3) / 1e9
     traffic_pc = load_traffic()
@@ -386,6 +397,7 @@ def main():
                 "includes": "input generation excluded; static+state upload, per-step hydrograph "
                             "and clock readback, final depth and dmax readback"},
         "late_window": late,
+        "dense_window": dense,
         "ensemble": ens,
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),

@@ -1025,7 +1025,7 @@ template <typename R> struct Impl : Base {
         a.rec = rec;
         a.strct = strct;
         a.dry_rows = dry_rows();
-        a.dryflag = (rpw % 4 == 0 && rpw <= 128) ? dryf.p : nullptr;
+        a.dryflag = dry_usable(rpw) ? dryf.p : nullptr;
         a.vmax = hz_on ? vmaxm.p : nullptr;
         a.hzmax = hz_on ? hzmaxm.p : nullptr;
         a.sc = sc.p;
@@ -1125,9 +1125,11 @@ template <typename R> struct Impl : Base {
     }
     // the launches use the flags only with rows per warp a multiple of 4 up to 128; launches
     // without them do not maintain them, so any change of layout or of flag use clears them
+    bool dry_enabled = true;   // hp2d_set_dry_skip
+    bool dry_usable(int rpw) const { return dry_enabled && rpw % 4 == 0 && rpw <= 128; }
     int dry_key(int cpl) {
         const int rpw = rpw_chosen ? rows_per_warp : default_rows(cpl);
-        return (rpw % 4 == 0 && rpw <= 128) ? cpl : -cpl;
+        return dry_usable(rpw) ? cpl : -cpl;
     }
     void dry_for_layout(int cpl) {
         const int key = dry_key(cpl);
@@ -1918,6 +1920,15 @@ hp2d_status hp2d_set_reservoirs(hp2d_ctx* ctx, int32_t n, const int32_t* res_row
         return HP2D_INVALID_ARG;
     return with_impl(ctx, [&](auto& m) {
         return m.set_reservoirs(n, res_row, res_col, k1, h1, k2, ds1_row, ds1_col, k3, h2, k4, ds2_row, ds2_col);
+    });
+}
+
+hp2d_status hp2d_set_dry_skip(hp2d_ctx* ctx, int32_t on) {
+    if (on != 0 && on != 1) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) {
+        m.dry_enabled = on != 0;
+        m.invalidate_graph();
+        return HP2D_OK;
     });
 }
 

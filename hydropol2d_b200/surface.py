@@ -150,6 +150,11 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_stage(self._h, int(d.shape[1]), int(t.size), _dp(t), _dp(d), int(rr.size),
                                            rr.ctypes.data_as(ip), cc.ctypes.data_as(ip), gg.ctypes.data_as(ip)))
 
+    def set_dry_skip(self, on: bool = True):
+        """Skipping of provably unchanged dry rows and blocks in the fused step (default on;
+        results are identical either way)."""
+        self._check(self._L.hp2d_set_dry_skip(self._h, 1 if on else 0))
+
     def set_hazard_tracking(self, on: bool = True):
         """Per-cell maxima of the velocity raster and of depth x velocity over the fused steps
         (velocities.vmax_final / hazardmax_final); read with download("vmax"/"hazard_max")."""

@@ -267,6 +267,12 @@ hp2d_status hp2d_set_reservoirs(hp2d_ctx* ctx, int32_t n, const int32_t* res_row
  * on = 1 needs time_step_change <= min_time_step / 2.  Fused path only. */
 hp2d_status hp2d_set_hazard_tracking(hp2d_ctx* ctx, int32_t on);
 
+/* The fused step skips what it can prove unchanged (on by default): a deep-dry row whose output
+ * buffer already holds it is not stored again, and a block of rows whose inputs and outputs are
+ * all dry (no rain or infiltration that step) is neither read nor written.  Results are the
+ * same bit for bit either way; on = 0 runs every row densely (no reference counterpart). */
+hp2d_status hp2d_set_dry_skip(hp2d_ctx* ctx, int32_t on);
+
 /* ---- unfused drop-in entry points (one reference function each) ------------------ */
 /* Hydrological_Model for this path: adds delta_p_agg (the rain of the current rain
  * interval, see hp2d_set_rain_uniform),

@@ -81,3 +81,25 @@ def test_ensemble_members_match_solo_runs(hp2d_lib):
             assert same_bits(m.download_native(f), s.download_native(f)), f
         assert m.diag()["skipped_cells"] > 0
     ens.close()
+
+
+def test_dense_switch_gives_the_same_bits(hp2d_lib):
+    from hydropol2d_b200 import SurfaceFlow
+    case = S.dambreak_case(64, 320, 5.0, seed=9, hours=0.1)
+    a = SurfaceFlow(*case.shape, case.resolution, "fp32", **case.params)
+    b = SurfaceFlow(*case.shape, case.resolution, "fp32", **case.params)
+    case.apply(a)
+    case.apply(b)
+    b.set_dry_skip(False)
+    for chunk in (5, 100, 200):
+        a.fused_steps(chunk)
+        b.fused_steps(chunk)
+        for f in FIELDS:
+            assert same_bits(a.download_native(f), b.download_native(f)), f
+    assert a.diag()["skipped_read_cells"] > 0 and b.diag()["skipped_cells"] == 0
+    b.set_dry_skip(True)                         # back on mid-run
+    a.fused_steps(100)
+    b.fused_steps(100)
+    for f in FIELDS:
+        assert same_bits(a.download_native(f), b.download_native(f)), f
+    assert b.diag()["skipped_cells"] > 0
