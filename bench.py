@@ -1,19 +1,30 @@
 """Benchmark of the fused surface-flow step (one JSON line on rank 0).
 
-Workload: dam-break on a 4096 x 8192 grid (33.5 M cells, dx 5 m, FP32 state with the split
-bed/depth slope), seeded synthetic inputs (hydropol2d_b200.synthetic.dambreak_case).
-A step is one accepted time step of HydroPol2D_Main_While over the whole grid (rain,
-infiltration (off here), local-inertial fluxes, draining limiter, continuity, outlet
-sink, maxima, CFL reduction and timestep refresh) -- one fused kernel launch.
+Workload: the 3-hour dam-break on a 4096 x 8192 grid (33.5 M cells, dx 5 m, FP32 state with the
+split bed/depth slope), seeded synthetic inputs (hydropol2d_b200.synthetic.dambreak_case).  A step
+is one accepted time step of HydroPol2D_Main_While over the whole grid (rain, infiltration (off
+here), local-inertial fluxes, draining limiter, continuity, outlet sink, maxima, CFL reduction and
+timestep refresh) -- one fused kernel launch.
+
+The run goes from t = 0 to the end of the 3 simulated hours, every launch timed with CUDA events
+(`full_run`: cells x steps / device time over the whole simulation, with the time-averaged wet
+fraction).  The headline window (`value`) is taken when the clock first passes 60 min, a third of
+the way through the flood: W untimed warm-up steps, then K timed steps.  The same K steps with the
+dry skips switched off give `dense_window` (every record read, stepped and written; bit-identical
+results).  `roofline.achieved` counts the dense algorithmic bytes of every cell of the grid, 40 B
+per cell-update (h, q_x, q_y, z and n^2 read, 20 B; h, q_x, q_y written, 12 B; the running
+maximum depth read and written, 8 B), over the launch time; `bytes_still_moved` is what the
+kernel's records moved after the dry skips.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --workload wet|dambreak|urban|unet|ensemble [...]   one profiling line
 
 N > 1 runs under torchrun, one rank per GPU, each rank an independent dam-break member
-(different DEM seed): ensemble members share nothing, so there is no collective on the
-data path (weak scaling).  The 256-member ensemble leg is split the same way: each rank
-runs its cost-balanced share (hydropol2d_b200.sharding), members/h is the whole job's.  Timing: CUDA events on the library's stream, barrier +
-synchronize on both sides, max over ranks.  The state (~1.5 GB) is far larger than L2,
-so no flush is needed between steps.
+(different DEM seed): ensemble members share nothing, so there is no collective on the data path
+(weak scaling).  The 256-member ensemble leg is split the same way (hydropol2d_b200.sharding),
+members/h is the whole job's.  Timing: CUDA events on the library's stream, barrier + synchronize
+on both sides, max over ranks.  The state (~1.5 GB) is far larger than L2, so no flush is needed
+between steps.
 """
 from __future__ import annotations
 
@@ -33,12 +44,22 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 NY, NX, DX = 4096, 8192, 5.0
-WORKLOAD = "dambreak_4096x8192_dx5_fp32"
+WORKLOAD = "dambreak_4096x8192_dx5_fp32_3h"
 METRIC = "GCell-updates/s"
-# algorithmic bytes per cell-update of the fused FP32 step without infiltration and rain:
-# read the static record {dz_x, dz_y, n^2, meta} and the state record {h, q_x, q_y, dmax}
-# (2 x 16 B), write the state record (16 B)
-BYTES_PER_CELL = 48.0
+WINDOW_MIN = 60.0          # the headline window starts when the clock first passes this [min]
+# algorithmic HBM bytes per cell-update of the step without rain and infiltration: h, q_x, q_y,
+# z, n^2 read (20 B), h, q_x, q_y written (12 B), the running maximum read and written (8 B)
+ALG_BYTES_PER_CELL = 40.0
+# bytes the fused kernel's records move per cell on a dense step: static record {dz_x, dz_y, n^2,
+# meta} 16 B + state record 16 B read, state record 16 B written
+RECORD_BYTES_PER_CELL = 48.0
+# Green-Ampt step (configuration 2): + soil record {I, T} read and written, 2 x 8 B
+RECORD_BYTES_PER_CELL_GA = 64.0
+ALG_BYTES_PER_CELL_GA = 49.0   # + I read/write 8 B + soil class 1 B
+# DRAM bytes per cell of one launch in the headline window, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of k_fused_step, three launches) on the same
+# dam-break with 2048 rows advanced to the 60-minute mark, scaled per cell
+NCU_DRAM_BYTES_PER_CELL = None
 
 
 def dist_env():
@@ -51,17 +72,6 @@ def load_peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def load_traffic():
-    p = ROOT / "profiles" / "traffic.json"
-    if p.exists():
-        try:
-            d = json.loads(p.read_text())
-            return float(d["dram_bytes_per_cell"])
-        except Exception:
-            return None
-    return None
 
 
 class ClockSampler:
@@ -185,7 +195,8 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "MATLAB/Octave are not installed: the reference's own CPU path cannot run here; "
-                "this is the C++ restatement of its arithmetic (oracle/kernel_form.hpp).",
+                "this is the C++ restatement of its arithmetic (oracle/kernel_form.hpp). It updates "
+                "every cell every step, so its rate does not depend on the window.",
     }
     print(json.dumps(line), flush=True)
 
@@ -214,6 +225,38 @@ def ensemble_leg(device: int, n_members: int = 256) -> dict | None:
                       "member reaches its routing_time; max over ranks"}
 
 
+def urban_leg(device: int, n: int = 2048, peak: float | None = None) -> dict:
+    """Configuration 2: urban rain-on-grid 2048 x 2048 (dx 2 m) with Green-Ampt soils and 64 x 64
+    rain maps changing every 5 minutes, run over its whole 2 simulated hours (every launch timed)."""
+    from hydropol2d_b200 import SurfaceFlow, synthetic as S
+    case = S.urban_case(n, 2.0, seed=7, hours=2.0)
+    sf = SurfaceFlow(n, n, 2.0, "fp32", device=device, **case.params)
+    case.apply(sf)
+    sf.fused_steps(20)
+    ms_win = sf.fused_steps_timed(200)
+    steps, ms = 220, ms_win
+    while True:
+        d = sf.diag()
+        if d["t"] > case.params["routing_time"] + case.params["min_time_step"] / 60:
+            break
+        ms += sf.fused_steps_timed(2000)
+        steps += 2000
+    d = sf.diag()
+    steps_done = d["k"] - 1
+    sf.close()
+    cells = n * n
+    g_win = cells * 200 / (ms_win / 1e3) / 1e9
+    out = {"workload": f"urban_{n}x{n}_dx2_green_ampt_rainmaps_2h", "window_gcups": g_win,
+           "window_ms_per_step": ms_win / 200, "full_run_steps": steps_done,
+           "full_run_gcups": cells * steps_done / (ms / 1e3) / 1e9, "sim_minutes": d["t"],
+           "record_bytes_per_cell": RECORD_BYTES_PER_CELL_GA, "alg_bytes_per_cell": ALG_BYTES_PER_CELL_GA,
+           "window_record_gbs": RECORD_BYTES_PER_CELL_GA * g_win,
+           "window_alg_gbs": ALG_BYTES_PER_CELL_GA * g_win}
+    if peak:
+        out["window_record_hbm_frac"] = out["window_record_gbs"] / peak
+    return out
+
+
 def run_surrogate(args):
     """Learned screening at the configuration's size: 4096 solver runs on 256 x 256 tiles
     train three U-Nets; 1024 held-out members are screened (inference + reruns of members
@@ -231,25 +274,175 @@ def run_surrogate(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- profiling workloads
+def workload_wet(steps: int) -> str:
+    """The V-tilted catchment geometry on 2048 x 2048 cells (dx 10 m) plus a 0.5 m random field,
+    5 cm of water everywhere and 60 mm/h of rain: every cell takes the full local-inertial path
+    of the fused step (no dry-row shortcuts)."""
+    from hydropol2d_b200 import SurfaceFlow, synthetic as S
+    z, ch = S.vtilt_domain(2048, 2048, 10.0, 0.005, 0.002)
+    z = z + 0.5 * S.gaussian_random_field(2048, 2048, -3.0, 5)
+    p = dict(routing_time=600.0, alfa_min=0.7, alfa_max=0.7, outlet_type=1, slope_outlet=0.002,
+             min_time_step=0.01, max_time_step=10.0)
+    case = S.Case("wet2048", z, np.full(z.shape, 0.03), 10.0, np.zeros(ch.size, dtype=np.int32),
+                  ch.astype(np.int32), p, np.full(z.shape, 50.0),
+                  rain_uniform=(np.array([0.0]), np.array([60.0])))
+    g = SurfaceFlow(2048, 2048, 10.0, "fp32", **p)
+    case.apply(g)
+    g.fused_steps(steps)
+    ms = g.fused_steps_timed(200)
+    g.close()
+    return "wet 2048^2: %.4f ms/step, %.1f GCUPS" % (ms / 200, 2048 * 2048 * 200 / ms / 1e6)
+
+
+def workload_dambreak(ny: int, steps: int, advance_min: float, state: str | None, timed: int) -> str:
+    """The bench's dam-break on ny x 8192 cells.  advance_min > 0 runs it to that clock first;
+    --state FILE saves the state reached there (.npz) or, when FILE exists, starts from it."""
+    from hydropol2d_b200 import SurfaceFlow, synthetic as S
+    case = S.dambreak_case(ny, 8192, 5.0, seed=11)
+    g = SurfaceFlow(ny, 8192, 5.0, "fp32", **case.params)
+    case.apply(g)
+    if state and Path(state).exists():
+        z = np.load(state)
+        g.set_state(z["h"].astype(np.float64) * 1000.0,
+                    np.stack([z["qx"], z["qy"]]).astype(np.float64) / 5.0 * 3.6e6)
+        g.set_clock(float(z["t"]), float(z["ts"]), int(z["k"]))
+    elif advance_min > 0:
+        while g.diag()["t"] < advance_min:
+            g.fused_steps(1000)
+        if state:
+            d = g.diag()
+            np.savez(state, h=g.download_native("h"), qx=g.download_native("qx"), qy=g.download_native("qy"),
+                     t=d["t"], ts=d["time_step"], k=d["k"])
+    g.fused_steps(steps)
+    ms = g.fused_steps_timed(timed)
+    t = g.diag()["t"]
+    wet = float(np.mean(g.download_native("h") > 0))
+    g.close()
+    return ("dambreak %dx8192 at t=%.1f min (%.1f%% wet): %.4f ms/step, %.1f GCUPS"
+            % (ny, t, 100 * wet, ms / timed, ny * 8192 * timed / ms / 1e6))
+
+
+def workload_urban(n: int, steps: int, timed: int) -> str:
+    from hydropol2d_b200 import SurfaceFlow, synthetic as S
+    case = S.urban_case(n, 2.0, seed=7, hours=2.0)
+    g = SurfaceFlow(n, n, 2.0, "fp32", **case.params)
+    case.apply(g)
+    g.fused_steps(steps)
+    ms = g.fused_steps_timed(timed)
+    g.close()
+    return "urban %dx%d (Green-Ampt, rain maps): %.4f ms/step, %.1f GCUPS" % (n, n, ms / timed, n * n * timed / ms / 1e6)
+
+
+def workload_unet(batch: int) -> str:
+    import torch
+    from hydropol2d_b200 import nn
+    from hydropol2d_b200.surrogate import UNet, forward_flops
+    net = UNet(seed=0)
+    x = torch.randn(batch, 256, 256, 4, device="cuda").to(torch.bfloat16)
+    for _ in range(3):
+        net.predict(x)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        net.predict(x)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_f = e0.elapsed_time(e1) / 10
+    f = forward_flops(256, 256) * batch
+    t = torch.randn(batch * 256 * 256, 2, device="cuda")
+    w = torch.ones_like(t)
+    for _ in range(3):
+        net.train_step(x, t, w, 1e-4)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(5):
+        net.train_step(x, t, w, 1e-4)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_t = e0.elapsed_time(e1) / 5
+    nn.check()
+    return ("unet B=%d 256^2: forward %.3f ms (%.1f TFLOP/s), training step %.3f ms (%.1f TFLOP/s, 3x forward)"
+            % (batch, ms_f, f / ms_f / 1e9, ms_t, 3 * f / ms_t / 1e9))
+
+
+def workload_ensemble(members: int, launches: int) -> str:
+    from hydropol2d_b200 import SurfaceFlow, synthetic as S
+    from hydropol2d_b200.ensemble import Ensemble
+    ens = Ensemble()
+    for i in range(members):
+        c = S.ensemble_member(i)
+        g = SurfaceFlow(*c.shape, c.resolution, "fp32", **c.params)
+        c.apply(g)
+        ens.add(g)
+    ens.set_tuning(64)
+    ens.steps(4)
+    _, ms = ens.steps_timed(launches)
+    cells = ens.cells()
+    ens.close()
+    return "ensemble %d members: %.4f ms/launch, %.1f GCUPS" % (members, ms / launches, cells * launches / ms / 1e6)
+
+
+def run_workload(args):
+    from hydropol2d_b200 import build
+    build.build()
+    w = args.workload
+    if w == "wet":
+        line = workload_wet(args.steps)
+    elif w == "dambreak":
+        line = workload_dambreak(args.ny, args.steps, args.advance_min, args.state, args.timed)
+    elif w == "urban":
+        line = workload_urban(args.nx if args.nx != NX else 2048, args.steps, args.timed)
+    elif w == "unet":
+        line = workload_unet(args.batch)
+    else:
+        line = workload_ensemble(args.members, args.launches)
+    print(line, flush=True)
+
+
+# ---------------------------------------------------------------- the benchmark
+def pinned(a: np.ndarray) -> np.ndarray:
+    """A copy of `a` in page-locked host memory (the end-to-end leg's inputs and outputs)."""
+    import torch
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-member ensemble leg")
-    ap.add_argument("--late-steps", type=int, default=10000,
-                    help="steps the dam-break advances before the late-window measurement (0: skip)")
+    ap.add_argument("--no-urban", action="store_true", help="skip the urban Green-Ampt leg")
+    ap.add_argument("--window-min", type=float, default=WINDOW_MIN,
+                    help="clock [min] the headline window starts at")
+    ap.add_argument("--hours", type=float, default=3.0, help="simulated hours of the dam-break run")
     ap.add_argument("--surrogate", action="store_true",
                     help="run the learned-screening study instead (4096 training / 1024 held-out members)")
     ap.add_argument("--surrogate-epochs", type=int, default=8)
+    ap.add_argument("--workload", choices=["wet", "dambreak", "urban", "unet", "ensemble"],
+                    help="print one timing line of a profiling workload instead")
+    ap.add_argument("--advance-min", type=float, default=0.0)
+    ap.add_argument("--state", default=None)
+    ap.add_argument("--timed", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--launches", type=int, default=64)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
 
+    if args.workload:
+        run_workload(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -273,93 +466,128 @@ def main():
     ny, nx = args.ny, args.nx
     cells = ny * nx
     t_e2e0 = time.perf_counter()
-    case = S.dambreak_case(ny, nx, DX, seed=11 + rank)
+    case = S.dambreak_case(ny, nx, DX, seed=11 + rank, hours=args.hours)
     t_gen = time.perf_counter() - t_e2e0
+    t_end = case.params["routing_time"] + case.params["min_time_step"] / 60
 
-    # ---- device-resident timing of the fused step ----------------------------------
+    # ---- the whole simulation, every launch timed; the headline window at WINDOW_MIN --------
     sf = SurfaceFlow(ny, nx, DX, "fp32", device=local, **case.params)
     case.apply(sf)
-    sf.fused_steps(args.warmup)
-    if dist is not None:
-        dist.barrier()
-    d0 = sf.diag()
-    skip0, skipr0 = d0["skipped_cells"], d0["skipped_read_cells"]
+    chunk = 1000
+    run_ms, run_steps, wet_samples, trace = 0.0, 0, [], []
+    win = None
     with ClockSampler(local) as clocks:
-        ms = sf.fused_steps_timed(args.steps)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_per_step = ms / args.steps
-    value = cells * args.steps * world / (ms / 1e3) / 1e9
-    d = sf.diag()
-    # deep-dry rows whose records the output buffer already held were not stored again
-    skip_frac = (d["skipped_cells"] - skip0) / (cells * args.steps)
-    # ... and whole dry row blocks were neither read nor written
-    skipr_frac = (d["skipped_read_cells"] - skipr0) / (cells * args.steps)
-    req_bpc = BYTES_PER_CELL - 32.0 * skipr_frac - 16.0 * skip_frac
-    wet_main = float(np.mean(sf.download_native("h") > 0))
-    # the same window with the dry skips off, on a second context from the same inputs: every
-    # row read, stepped and written (bit-identical results)
-    dn = SurfaceFlow(ny, nx, DX, "fp32", device=local, **case.params)
-    case.apply(dn)
-    dn.set_dry_skip(False)
-    dn.fused_steps(args.warmup)
-    ms_dense = dn.fused_steps_timed(args.steps)
-    dn.close()
-    dense = {"value": cells * args.steps / (ms_dense / 1e3) / 1e9, "ms_per_step": ms_dense / args.steps,
-             "achieved_gbs": BYTES_PER_CELL * cells / (ms_dense / args.steps / 1e3) / 1e9}
-    late = None
-    if args.late_steps > 0:
-        # the same run later on, once the flood wave has spread over more of the valley
-        sf.fused_steps(args.late_steps)
-        ms_late = sf.fused_steps_timed(args.steps)
-        h = sf.download_native("h")
-        d_late = sf.diag()
-        late = {"after_steps": args.warmup + args.steps + args.late_steps, "sim_clock_min": d_late["t"],
-                "wet_fraction": float(np.mean(h > 0)), "ms_per_step": ms_late / args.steps,
-                "value": cells * args.steps / (ms_late / 1e3) / 1e9,
-                "wet_fraction_main_window": wet_main}
+        while True:
+            d = sf.diag()
+            if d["t"] > t_end:
+                break
+            if win is None and d["t"] >= args.window_min:
+                # headline window: W warm-up steps, then K timed steps (all part of the run)
+                run_ms += sf.fused_steps_timed(args.warmup)
+                h0_mm = sf.download("depth")
+                of0 = np.stack([sf.download("qout_right"), sf.download("qout_up")])
+                run_steps += args.warmup
+                if dist is not None:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                d0 = sf.diag()
+                ms = sf.fused_steps_timed(args.steps)
+                torch.cuda.synchronize()
+                d1 = sf.diag()
+                run_ms += ms
+                run_steps += args.steps
+                if dist is not None:
+                    t = torch.tensor([ms], device=f"cuda:{local}")
+                    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                    ms = float(t.item())
+                wet_win = float(np.mean(sf.download_native("h") > 0))
+                # the end-to-end leg starts from the state the window started from
+                e2e_in = (d0, pinned(h0_mm), pinned(of0))
+                # the same number of steps with the dry skips off: every record read and written
+                sf.set_dry_skip(False)
+                ms_dense = sf.fused_steps_timed(args.steps)
+                sf.set_dry_skip(True)
+                run_ms += ms_dense
+                run_steps += args.steps
+                win = {"ms": ms, "t0_min": d0["t"], "t1_min": d1["t"], "wet_fraction": wet_win,
+                       "dt_s_last": d1["time_step"] * 60,
+                       "write_skip": (d1["skipped_cells"] - d0["skipped_cells"]) / (cells * args.steps),
+                       "read_skip": (d1["skipped_read_cells"] - d0["skipped_read_cells"]) / (cells * args.steps),
+                       "ms_dense": ms_dense}
+                continue
+            n = chunk
+            ms_c = sf.fused_steps_timed(n)
+            d2 = sf.diag()
+            run_ms += ms_c
+            run_steps += n
+            wet = float(np.mean(sf.download_native("h") > 0))
+            wet_samples.append(wet)
+            trace.append({"t_min": round(d2["t"], 2), "wet": round(wet, 4),
+                          "gcups": round(cells * n / (ms_c / 1e3) / 1e9, 1)})
+    d_end = sf.diag()
+    steps_total = d_end["k"] - 1   # accepted steps of the whole run (launches after the end are no-ops)
     sf.close()
+    if win is None:
+        raise SystemExit(f"the run ended before the clock reached {args.window_min} min")
+    ms_per_step = win["ms"] / args.steps
+    value = cells * args.steps * world / (win["ms"] / 1e3) / 1e9
+    full_run = {"sim_minutes": d_end["t"], "steps": steps_total, "launches": run_steps,
+                "device_s": run_ms / 1e3,
+                "gcups": cells * steps_total / (run_ms / 1e3) / 1e9,
+                "wet_fraction_time_avg": float(np.mean(wet_samples)) if wet_samples else None,
+                "timing": "CUDA events around every launch of the run, t = 0 to the end of the simulated time; "
+                          "launches after the end are no-ops and their time is counted",
+                "trace_every_1000_steps": trace}
+    dense = {"value": cells * args.steps / (win["ms_dense"] / 1e3) / 1e9, "ms_per_step": win["ms_dense"] / args.steps,
+             "record_gbs": RECORD_BYTES_PER_CELL * cells / (win["ms_dense"] / args.steps / 1e3) / 1e9,
+             "alg_gbs": ALG_BYTES_PER_CELL * cells / (win["ms_dense"] / args.steps / 1e3) / 1e9}
 
     # ---- end to end through the C ABI with host buffers ------------------------------
-    # host arrays -> hp2d_upload_static/hp2d_set_state -> K steps, reading the outlet
-    # hydrograph and the clock back every step -> final depth and dmax back to the host
-    e2e_steps = args.steps
+    # The 60-minute state (depth and the two flux pages, as a MATLAB caller holds them) and the
+    # static inputs sit in pinned host memory; timed: context creation, hp2d_upload_static and
+    # hp2d_set_state / hp2d_set_clock from those arrays, K steps reading the outlet hydrograph and
+    # the clock back after every step, then the depth and dmax maps back into pinned host arrays.
+    dw, h_mm, of = e2e_in
+    z_p, n_p = pinned(case.z), pinned(case.roughness)
+    depth_out = pinned(np.empty((ny, nx)))
+    dmax_out = pinned(np.empty((ny, nx)))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sf = SurfaceFlow(ny, nx, DX, "fp32", device=local, **case.params)
-    case.apply(sf)
+    sf.upload_static(z_p, n_p, case.outlet_rows, case.outlet_cols)
+    sf.set_state(h_mm, of)
+    sf.set_clock(dw["t"], dw["time_step"], dw["k"])
     t1 = time.perf_counter()
-    q_hydro = []
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         sf.fused_steps(1)
-        q_hydro.append(sf.download_native("qo"))
+        sf.download_native("qo")
     t2 = time.perf_counter()
-    d_final = sf.download("depth")
-    dmax = sf.download("dmax")
+    sf.download_into("depth", depth_out)
+    sf.download_into("dmax", dmax_out)
     e2e_s = time.perf_counter() - t0
     e2e_split = {"setup_s": t1 - t0, "steps_s": t2 - t1, "readback_s": e2e_s - (t2 - t0)}
     n_out = sf.n_outlets
     sf.close()
-    # H2D per run: the static upload (FP64 elevation and roughness and the 4-byte meta word,
-    # 20 B/cell) and the state upload (FP64 depth, 8 B/cell); the context's records are built
-    # and filled on the device.  D2H: outlet hydrograph (4 B per outlet) and the clock block
-    # every step, then the depth and dmax components (FP32, 8 B/cell) once
-    h2d_per_step = 28 * cells / e2e_steps
-    d2h_per_step = n_out * 4 + 2 * 232 + 8 * cells / e2e_steps   # 232 B: the clock block
-    e2e = cells * e2e_steps / e2e_s / 1e9
+    # H2D per run: elevation and roughness (FP64) + the 4-byte meta word built on the host
+    # (20 B/cell), depth and two flux pages (FP64, 24 B/cell).  D2H: the outlet hydrograph (4 B per
+    # outlet) and the clock block every step, the depth and dmax maps (FP64) once.
+    h2d_per_step = 44 * cells / args.steps
+    d2h_per_step = n_out * 4 + 2 * 296 + 16 * cells / args.steps   # 296 B: the clock block
+    e2e = cells * args.steps / e2e_s / 1e9
     if dist is not None:
         t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = cells * e2e_steps * world / float(t.item()) / 1e9
+        e2e = cells * args.steps * world / float(t.item()) / 1e9
 
     peak, peak_kind = load_peaks()
-    dense["hbm_frac"] = dense["achieved_gbs"] / peak   # 48 B/cell streamed, of measured HBM
-    # bytes the step must move: the dense 48 B per cell less the records it skipped
-    achieved = req_bpc * cells / (ms_per_step / 1e3) / 1e9
-    traffic_pc = load_traffic()
+    dense["record_hbm_frac"] = dense["record_gbs"] / peak
+    dense["alg_hbm_frac"] = dense["alg_gbs"] / peak
+    achieved = ALG_BYTES_PER_CELL * cells / (ms_per_step / 1e3) / 1e9
+    moved_bpc = RECORD_BYTES_PER_CELL - 32.0 * win["read_skip"] - 16.0 * win["write_skip"]
 
+    urban = None
+    if not args.no_urban:
+        urban = urban_leg(local, peak=peak)
     ens = None
     if not args.no_ensemble:
         ens = ensemble_leg(local)   # every rank takes part (its share of the members)
@@ -383,21 +611,30 @@ def main():
         "config": {"workload": WORKLOAD, "ny": ny, "nx": nx, "dx_m": DX, "cells": cells,
                    "parallelism": f"{world} independent members (one per GPU)" if world > 1 else "single grid",
                    "l2": "state 1.5 GB per step > 126 MB L2; no flush needed",
-                   "sim_clock_min_after": d["t"], "dt_s_last": d["time_step"] * 60,
-                   "wet_fraction": wet_main},
+                   "window": f"K steps after the clock first passes {args.window_min:g} min of the "
+                             f"{args.hours:g} h run (W warm-up steps before them)",
+                   "window_clock_min": [win["t0_min"], win["t1_min"]], "dt_s_last": win["dt_s_last"],
+                   "wet_fraction": win["wet_fraction"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_cell": req_bpc,
-                     "dense_bytes_per_cell": BYTES_PER_CELL,
-                     "write_skip_fraction": skip_frac, "read_skip_fraction": skipr_frac,
-                     "traffic": None if traffic_pc is None else traffic_pc * cells},
+                     "algorithmic_bytes_per_cell": ALG_BYTES_PER_CELL,
+                     "bytes_definition": "dense algorithmic bytes of every cell of the grid: state record "
+                                         "read + written (h, q_x, q_y, dmax) and the static slopes and "
+                                         "roughness read, over the launch time",
+                     "traffic": None if NCU_DRAM_BYTES_PER_CELL is None else NCU_DRAM_BYTES_PER_CELL * cells},
+        "bytes_still_moved": {"per_cell": moved_bpc, "gbs": moved_bpc * cells / (ms_per_step / 1e3) / 1e9,
+                              "write_skip_fraction": win["write_skip"], "read_skip_fraction": win["read_skip"],
+                              "note": "records of the fused kernel (48 B dense) less those the dry skips "
+                                      "did not read (32 B) or write (16 B)"},
+        "full_run": full_run,
+        "dense_window": dense,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d_per_step,
-                "d2h_bytes_per_step": d2h_per_step, "steps": e2e_steps, **e2e_split,
-                "includes": "input generation excluded; static+state upload, per-step hydrograph "
-                            "and clock readback, final depth and dmax readback"},
-        "late_window": late,
-        "dense_window": dense,
+                "d2h_bytes_per_step": d2h_per_step, "steps": args.steps, **e2e_split,
+                "includes": "context creation, static + 60-minute state upload from pinned host arrays, "
+                            "per-step hydrograph and clock readback, final depth and dmax readback into "
+                            "pinned host arrays"},
+        "urban_c2": urban,
         "ensemble": ens,
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),

@@ -42,6 +42,7 @@ EXPORTS = [
     "hp2d_set_map_records", "hp2d_map_records", "hp2d_download_map_record", "hp2d_hydrology_step", "hp2d_li_step",
     "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed",
     "hp2d_set_tuning", "hp2d_set_layout", "hp2d_run",
+    "hp2d_set_retry_policy", "hp2d_set_wait_limit", "hp2d_inject_step_fault",
     "hp2d_download",
     "hp2d_download_native", "hp2d_get_diag", "hp2d_stored_volume",
     "hp2d_cfl_dt_noalloc", "hp2d_noalloc_error",
@@ -92,6 +93,7 @@ class Diag(C.Structure):
         ("rain_t0", C.c_double), ("rain_t1", C.c_double), ("t_previous", C.c_double),
         ("inflow_volume", C.c_double), ("stage_volume", C.c_double),
         ("structure_volume", C.c_double), ("skipped_cells", C.c_int64), ("skipped_read_cells", C.c_int64),
+        ("retries", C.c_int64), ("catch_index", C.c_int32), ("pad", C.c_int32), ("max_time_step", C.c_double),
     ]
 
 
@@ -162,6 +164,9 @@ def lib() -> C.CDLL:
         "hp2d_set_tuning": ([vp, C.c_int32], C.c_int),
         "hp2d_set_layout": ([vp, C.c_int32], C.c_int),
         "hp2d_run": ([vp, C.c_int64, P(C.c_int64)], C.c_int),
+        "hp2d_set_retry_policy": ([vp, C.c_int32, C.c_double, C.c_int32], C.c_int),
+        "hp2d_set_wait_limit": ([vp, C.c_int64], C.c_int),
+        "hp2d_inject_step_fault": ([vp, C.c_int64, C.c_int32], C.c_int),
         "hp2d_download": ([vp, C.c_int32, dp, C.c_size_t], C.c_int),
         "hp2d_download_native": ([vp, C.c_int32, vp, C.c_size_t], C.c_int),
         "hp2d_get_diag": ([vp, P(Diag)], C.c_int),

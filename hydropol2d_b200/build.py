@@ -20,8 +20,10 @@ LIB = PKG / "libhp2d.so"
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
+# device code of one translation unit compiled in parallel by nvcc itself
+SPLIT = ["--split-compile=0"]
 
 
 def sources() -> list[Path]:
@@ -41,14 +43,31 @@ def nvcc() -> str:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles every csrc/*.cu to an object in parallel (the build folder is PKG/_build),
+    then links libhp2d.so."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, f"-I{ROOT / 'include'}", f"-I{SRC}",
-           *[str(p) for p in sorted(SRC.glob("*.cu"))], "-o", str(LIB)]
+    from concurrent.futures import ThreadPoolExecutor
+    out_dir = PKG / "_build"
+    out_dir.mkdir(exist_ok=True)
+    inc = [f"-I{ROOT / 'include'}", f"-I{SRC}"]
+    cus = sorted(SRC.glob("*.cu"))
+
+    def compile_one(cu: Path) -> Path:
+        obj = out_dir / (cu.stem + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, *SPLIT, *inc, "-c", str(cu), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(cus)) as ex:
+        objs = list(ex.map(compile_one, cus))
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *[str(o) for o in objs],
+           "-o", str(tmp)]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
-    tmp = LIB.with_suffix(".so.tmp")
-    cmd[-1] = str(tmp)
     subprocess.run(cmd, check=True)
     tmp.replace(LIB)
     return LIB

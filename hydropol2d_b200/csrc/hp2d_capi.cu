@@ -212,6 +212,9 @@ template <typename R> struct Impl : Base {
         hs.rain_a = 0.0;
         hs.rain_b = hs.t_min;
         hs.t_prev = 0.0;
+        hs.catch_index = 1;                      // HydroPol2D_Main_While.m:266
+        hs.max_dt = c->p.max_time_step;
+        hs.fault_k = -1;
         push_sc();
         // closed faces everywhere until hp2d_upload_static, dry state
         const R qn = std::numeric_limits<R>::quiet_NaN();
@@ -331,9 +334,10 @@ template <typename R> struct Impl : Base {
             HP_CK(cudaMemcpyAsync(dz_.p, z, n * sizeof(double), cudaMemcpyHostToDevice, st()));
             HP_CK(cudaMemcpyAsync(dr_.p, rough, n * sizeof(double), cudaMemcpyHostToDevice, st()));
             upload(dm_.p, host_meta);
-            dzx.alloc(n); dzy.alloc(n); n2.alloc(n);
-            k_build_static<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, dz_.p, dr_.p, dm_.p, stat.p, dzx.p,
-                                                                     dzy.p, n2.p);
+            // the unfused entry points' copies are extracted from the records on first use
+            dzx.free(); dzy.free(); n2.free();
+            k_build_static<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, dz_.p, dr_.p, dm_.p, stat.p, nullptr,
+                                                                     nullptr, nullptr);
             HP_CK(cudaGetLastError());
             HP_CK(cudaStreamSynchronize(st()));
         }
@@ -475,6 +479,8 @@ template <typename R> struct Impl : Base {
             upload(gs2[hs.cur].p, g);
         }
         fill(arrival.p, n, std::numeric_limits<R>::infinity());
+        hs.halted = 0;   // a new state starts over after a failed call
+        push_sc();
         dirty = true;
         return HP2D_OK;
     }
@@ -502,6 +508,7 @@ template <typename R> struct Impl : Base {
         hs.t_min = t;
         hs.time_step = time_step;
         hs.k = k;
+        hs.halted = 0;
         push_sc();
         dirty = true;
         return HP2D_OK;
@@ -930,8 +937,13 @@ template <typename R> struct Impl : Base {
         double dts = time_step * 60.0;
         auto gv = view();
         int nb = blocks_for(n);
+        if (!dzx.p) {   // structure-of-arrays copies of the static record, made once
+            dzx.alloc(n); dzy.alloc(n); n2.alloc(n);
+            k_static_soa<R><<<nb, kThreads, 0, st()>>>(n, stat.p, dzx.p, dzy.p, n2.p);
+            HP_CK(cudaGetLastError());
+        }
         k_faces<R><<<nb, kThreads, 0, st()>>>(gv, dts, h.p, dzx.p, dzy.p, n2.p, qx.p, qy.p, hfx.p, hfy.p, qxu.p,
-                                            qyu.p, ctx->p.flag_critical);
+                                            qyu.p, ctx->p.flag_critical, ctx->p.flag_numerical_scheme);
         HP_CK(cudaGetLastError());
         k_scale<R><<<nb, kThreads, 0, st()>>>(gv, dts, h.p, qxu.p, qyu.p, scale.p);
         HP_CK(cudaGetLastError());
@@ -969,7 +981,7 @@ template <typename R> struct Impl : Base {
         const bool is_d = sizeof(R) == 8;
         double vm = from_ord(hs.acc_vmax, is_d), cm = from_ord(hs.acc_cmax, is_d);
         const hp2d_params& p = ctx->p;
-        double tcr = finalize_dt(vm, cm, res, p.alfa_min, p.alfa_max, p.min_time_step, p.max_time_step,
+        double tcr = finalize_dt(vm, cm, res, p.alfa_min, p.alfa_max, p.min_time_step, hs.max_dt,
                                  p.time_step_increments, p.flag_timestep);
         hs.acc_vmax = hs.acc_cmax = 0;
         hs.vmax_last = vm;
@@ -1004,6 +1016,8 @@ template <typename R> struct Impl : Base {
         a.tsc = p.time_step_change; a.alfa_min = p.alfa_min; a.alfa_max = p.alfa_max;
         a.flag_timestep = p.flag_timestep; a.adaptive = p.flag_adaptive_timestepping;
         a.flag_critical = p.flag_critical; a.outlet_type = p.outlet_type; a.ga = ga() ? 1 : 0;
+        a.scheme = p.flag_numerical_scheme;
+        a.wait_polls = wait_polls;
         const int out_cols = 32 * cpl - 4;   // a strip's output columns (2-column apron each side)
         a.n_strips = (nx + out_cols - 1) / out_cols;
         const int rpw = rpw_chosen ? rows_per_warp : default_rows(cpl);
@@ -1033,31 +1047,42 @@ template <typename R> struct Impl : Base {
     }
 
     // kernels whose ring needs more than the default 48 KB of dynamic shared memory opt in
-    // once per instantiation (before any graph capture: fused_steps and autotune call this)
-    template <int INF, bool MAP, int CPL, bool INFL> static void opt_in_smem() {
-        static bool done[8] = {};
+    // once per instantiation and device (before any graph capture: fused_steps and autotune
+    // call this); the per-device flags of an instantiation are guarded by its own mutex, so
+    // host threads sharing a device opt in once
+    template <int INF, bool MAP, int CPL, bool INFL, int SCH = 0> static void opt_in_smem() {
+        static std::mutex mu;
+        static std::vector<char> done;
         const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
+        if (sm <= 40 * 1024) return;   // the static shared memory counts too
         int dev = 0;
         HP_CK(cudaGetDevice(&dev));
-        if (sm > 40 * 1024 && dev < 8 && !done[dev]) {   // the static shared memory counts too
-            HP_CK(cudaFuncSetAttribute(k_fused_step<R, kThreads, INF, MAP, CPL, INFL>,
+        std::lock_guard<std::mutex> lock(mu);
+        if (done.size() <= size_t(dev)) done.resize(size_t(dev) + 1, 0);
+        if (!done[size_t(dev)]) {
+            HP_CK(cudaFuncSetAttribute(k_fused_step<R, kThreads, INF, MAP, CPL, INFL, SCH>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-            done[dev] = true;
+            done[size_t(dev)] = 1;
         }
     }
     template <int INF, int CPL> void opt_in_i() {
         opt_in_smem<INF, false, CPL, false>(); opt_in_smem<INF, true, CPL, false>();
         opt_in_smem<INF, false, CPL, true>(); opt_in_smem<INF, true, CPL, true>();
+        opt_in_smem<INF, false, CPL, true, 1>(); opt_in_smem<INF, true, CPL, true, 1>();
     }
     template <int CPL> void opt_in_t() { opt_in_i<0, CPL>(); opt_in_i<1, CPL>(); opt_in_i<2, CPL>(); }
     void opt_in() { opt_in_t<1>(); opt_in_t<2>(); }
 
-    template <int INF, bool MAP, int CPL, bool INFL> void launch_one(const FusedArgs<R>& a) {
+    template <int INF, bool MAP, int CPL, bool INFL, int SCH = 0> void launch_one(const FusedArgs<R>& a) {
         const size_t sm = fused_smem_bytes<R, CPL>(kThreads);
-        k_fused_step<R, kThreads, INF, MAP, CPL, INFL><<<a.n_ctas, kThreads, sm, st()>>>(a);
+        k_fused_step<R, kThreads, INF, MAP, CPL, INFL, SCH><<<a.n_ctas, kThreads, sm, st()>>>(a);
     }
     template <int INF, int CPL> void launch_i(const FusedArgs<R>& a) {
         const bool map = rain.n_maps > 0, infl = bc_kernel();
+        if (ctx->p.flag_numerical_scheme != 1) {   // schemes 2/3: the general (boundary-cell) variant
+            if (map) launch_one<INF, true, CPL, true, 1>(a); else launch_one<INF, false, CPL, true, 1>(a);
+            return;
+        }
         if (map) {
             if (infl) launch_one<INF, true, CPL, true>(a); else launch_one<INF, true, CPL, false>(a);
         } else {
@@ -1139,6 +1164,8 @@ template <typename R> struct Impl : Base {
         }
     }
 
+    // set by the prologue's scan: a cell of finite elevation holds a non-finite depth
+    bool bad_state = false;
     void prologue() {
         dry_for_layout(cells_per_lane);
         if (!dirty) return;
@@ -1149,6 +1176,9 @@ template <typename R> struct Impl : Base {
         hs.acc_vmax = hs.acc_cmax = 0;
         hs.acc_rain = hs.acc_inf = hs.acc_out = 0;
         hs.n_finite = 0;
+        hs.n_bad0 = 0;
+        hs.acc_bad = 0;
+        hs.bad_domain = 0;
         push_sc();
         k_skip_flag<R><<<blocks_for(n), kThreads, 0, st()>>>(st4[hs.cur].p, stat.p, ny, nx, rain, ga() ? 1 : 0, res,
                                                            ctx->p.depth_tolerance, ctx->p.arrival_threshold, sc.p);
@@ -1167,6 +1197,8 @@ template <typename R> struct Impl : Base {
             HP_CK(cudaGetLastError());
         }
         dirty = false;
+        pull_sc();
+        bad_state = hs.bad_domain != 0;
     }
 
     static constexpr int kGraphChunk = 32;
@@ -1184,13 +1216,9 @@ template <typename R> struct Impl : Base {
         graph_steps = kGraphChunk;
     }
 
-    hp2d_status fused_steps(int32_t nsteps, cudaEvent_t after = nullptr) {
-        if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
-        if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
-        opt_in();
-        prologue();
+    void launch_steps(int64_t count) {
         FusedArgs<R> a = fused_args();
-        int remaining = nsteps;
+        int64_t remaining = count;
         if (remaining >= kGraphChunk) {
             ensure_graph(a);
             while (remaining >= graph_steps) {
@@ -1198,15 +1226,142 @@ template <typename R> struct Impl : Base {
                 remaining -= graph_steps;
             }
         }
-        for (int s = 0; s < remaining; ++s) launch_fused(a);
+        for (int64_t s = 0; s < remaining; ++s) launch_fused(a);
         HP_CK(cudaGetLastError());
-        if (after) HP_CK(cudaEventRecord(after, st()));
-        pull_sc();
+    }
+
+    // `nsteps` accepted steps.  A rejected step halts the remaining launches of the batch; the
+    // host then prepares its retry (handle_halt) and launches the steps still missing, until the
+    // retries of one step run out.
+    hp2d_status fused_steps(int32_t nsteps, cudaEvent_t after = nullptr) {
+        if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
+        if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
+        opt_in();
+        prologue();
+        if (bad_state) return bad_state_error();
+        const int64_t k_target = hs.k + nsteps;
+        int64_t todo = nsteps;
+        hp2d_status status = HP2D_OK;
+        for (;;) {
+            launch_steps(todo);
+            if (after) HP_CK(cudaEventRecord(after, st()));
+            pull_sc();
+            if (!hs.halted) break;
+            status = handle_halt();
+            if (status != HP2D_OK) break;
+            todo = k_target - hs.k;
+            if (todo <= 0) break;
+            prologue();
+            if (bad_state) { status = bad_state_error(); break; }
+        }
         flush_records();
-        if (hs.status & 2u) {
-            ctx->err = "a row copy into shared memory did not complete within its wait limit";
+        return status;
+    }
+
+    // ---------------- failure handling (HydroPol2D_Main_While.m:926-993) ----------------
+    int max_retries = 8;              // attempts of one step rejected before the call fails
+    double factor_reduction = 2.0;    // running_control.factor_reduction (input_data_script.m:486)
+    unsigned int wait_polls = 1u << 22;
+    int64_t rej_k = -1;               // step whose attempts were rejected last, and how often
+    int rej_n = 0;
+
+    hp2d_status bad_state_error() {
+        ctx->err = "the state holds a non-finite depth in a cell of finite elevation (only idx_nan cells, of NaN "
+                   "elevation, may hold NaN); nothing was stepped";
+        return HP2D_NUMERICAL;
+    }
+
+    // The launches halted: a row copy timed out (the step was rejected), the refreshed dt hit
+    // the floor with dt_floor_stop on (the step was kept), or a step was rejected for its
+    // depths.  The last is retried as the reference's catch block does: the attempt's state is
+    // already the rolled-back one (d_t = d_p, I_t = I_p: the buffer the attempt read), the clock
+    // goes back by the attempt's step, catch_index grows, the new step is
+    //   factor * alfa_min * dx / c,  factor = 1 / catch_index / factor_reduction,
+    //   c = sqrt(g max(max(d_tot), max(d_p)))  (+ the last refresh's maximum velocity when
+    //   flag_adaptive_timestepping = 0, for the reference's velocity-raster maximum),
+    // max_time_step drops to min(1.5 x new step, max_time_step), the new step is capped by it
+    // (an infinite one becomes min_time_step), the clock advances by it and the rain interval
+    // becomes [rewound clock, new clock] (update_spatial_BC after the catch).
+    hp2d_status handle_halt() {
+        if (hs.status & kStatusDtFloor) {   // a kept step
+            hs.status &= ~kStatusDtFloor;
+            hs.halted = 0;
+            push_sc();
+            ctx->err = "the refreshed time step reached min_time_step (refreshing_timestep.m:357-359) at step " +
+                       std::to_string(hs.k - 1) + "; that step was kept";
+            return HP2D_DT_FLOOR;
+        }
+        // a rejected step: take back its arrival marks and find max(d_p, d_tot) for the retry
+        hs.retry_dmax = 0ull;
+        push_sc();
+        {
+            const FusedArgs<R> a = fused_args();
+            const R t_arr = R(hs.t_min * 60.0 + hs.time_step * 60.0);
+            k_retry_scan<R><<<blocks_for(n), kThreads, 0, st()>>>(a, inf_mode(), t_arr);
+            HP_CK(cudaGetLastError());
+        }
+        pull_sc();
+        if (hs.status & kStatusTimeout) {
+            hs.status &= ~kStatusTimeout;
+            hs.halted = 0;
+            push_sc();
+            dirty = true;
+            ctx->err = "a row copy into shared memory did not complete within its wait limit; that step was "
+                       "rejected and the state is the last accepted one";
             return HP2D_TIMEOUT;
         }
+        if (hs.k == rej_k) ++rej_n;
+        else { rej_k = hs.k; rej_n = 1; }
+        if (rej_n > max_retries) {
+            hs.halted = 0;
+            push_sc();
+            dirty = true;
+            ctx->err = "step " + std::to_string(hs.k) + " was rejected " + std::to_string(rej_n) +
+                       " times (a depth went non-finite or below -depth_tolerance); the state is the last accepted one";
+            rej_n = 0;
+            return HP2D_NUMERICAL;
+        }
+        const double dmx = from_ord(hs.retry_dmax, sizeof(R) == 8);
+        const double wc = std::sqrt(kG * dmx);
+        const hp2d_params& p = ctx->p;
+        hs.catch_index += 1;
+        const double factor = 1.0 / hs.catch_index / factor_reduction;
+        double nt = p.flag_adaptive_timestepping == 1 ? factor * (p.alfa_min * res / wc)
+                                                      : factor * (p.alfa_min * res / (hs.vmax_last + wc));
+        if (hs.catch_index > 1) hs.max_dt = std::fmin(nt * 1.5, hs.max_dt);
+        nt = std::fmin(nt, hs.max_dt);
+        if (std::isinf(nt)) nt = p.min_time_step;
+        const double t0 = hs.t_min - hs.time_step;
+        hs.t_prev = t0;
+        hs.time_step = nt / 60.0;
+        hs.t_min = t0 + hs.time_step;
+        hs.rain_a = hs.t_prev;
+        hs.rain_b = hs.t_min;
+        hs.halted = 0;
+        hs.retries += 1;
+        push_sc();
+        dirty = true;
+        return HP2D_OK;
+    }
+
+    hp2d_status set_retry_policy(int32_t retries, double factor, int32_t dt_floor_is_error) {
+        if (retries < 0 || !(factor > 0) || (dt_floor_is_error != 0 && dt_floor_is_error != 1)) {
+            ctx->err = "max_retries >= 0, factor_reduction > 0 and dt_floor_is_error 0 or 1";
+            return HP2D_INVALID_ARG;
+        }
+        max_retries = retries;
+        factor_reduction = factor;
+        pull_sc();
+        hs.dt_floor_stop = dt_floor_is_error;
+        push_sc();
+        return HP2D_OK;
+    }
+    hp2d_status inject_fault(int64_t k, int32_t attempts) {
+        if (attempts < 0) { ctx->err = "attempts must be >= 0"; return HP2D_INVALID_ARG; }
+        pull_sc();
+        hs.fault_k = k;
+        hs.fault_n = attempts;
+        push_sc();
         return HP2D_OK;
     }
 
@@ -1306,7 +1461,7 @@ template <typename R> struct Impl : Base {
             HP_CK(cudaEventElapsedTime(&ms, e0, e1));
             if (ms < best_ms) { best_ms = ms; best = c; best_cpl = cpl; }
             pull_sc();
-            timed_out = timed_out || (hs.status & 2u) != 0;
+            timed_out = timed_out || (hs.status & kStatusTimeout) != 0;
             put_back(snap);
         }
         cudaEventDestroy(e0);
@@ -1334,52 +1489,31 @@ template <typename R> struct Impl : Base {
     }
 
     // ---------------- outputs ----------------
-    // one component of the current state records (a quarter of the record bytes cross)
-    // Device -> caller's double array, times `scale`, through two 4 MB pinned staging buffers:
-    // the copy of one chunk overlaps the conversion of the previous one, and no pageable
-    // staging or large host allocation sits in the path.
-    // The two staging buffers are shared by every context of the process (portable pinned
-    // memory, one reader at a time); the events are the context's own.
-    struct StageEvents {
-        cudaEvent_t ev[2] = {nullptr, nullptr};
-        ~StageEvents() {
-            for (auto e : ev)
-                if (e) cudaEventDestroy(e);
-        }
-    };
-    StageEvents stage_ev;
-    static constexpr size_t kStageBytes = size_t(4) << 20;
-    static constexpr size_t kStageElems = kStageBytes / sizeof(R);
-    void fetch_scaled(const R* src, size_t count, double scale, double* out) {
-        static std::mutex mu;
-        static void* buf[2] = {nullptr, nullptr};
-        std::lock_guard<std::mutex> lock(mu);
-        for (int b = 0; b < 2; ++b) {
-            if (!buf[b]) HP_CK(cudaHostAlloc(&buf[b], kStageBytes, cudaHostAllocPortable));
-            if (!stage_ev.ev[b]) HP_CK(cudaEventCreateWithFlags(&stage_ev.ev[b], cudaEventDisableTiming));
-        }
-        const size_t nch = (count + kStageElems - 1) / kStageElems;
-        auto issue = [&](size_t c) {
-            const size_t off = c * kStageElems, m = std::min(kStageElems, count - off);
-            HP_CK(cudaMemcpyAsync(buf[c & 1], src + off, m * sizeof(R), cudaMemcpyDeviceToHost, st()));
-            HP_CK(cudaEventRecord(stage_ev.ev[c & 1], st()));
-        };
-        if (nch) issue(0);
-        for (size_t c = 0; c < nch; ++c) {
-            if (c + 1 < nch) issue(c + 1);   // its buffer held chunk c-1, converted already
-            HP_CK(cudaEventSynchronize(stage_ev.ev[c & 1]));
-            const R* v = static_cast<const R*>(buf[c & 1]);
-            const size_t off = c * kStageElems, m = std::min(kStageElems, count - off);
-            for (size_t k = 0; k < m; ++k) out[off + k] = double(v[k]) * scale;
-        }
+    // A field goes to the caller's FP64 array in one copy: a kernel converts it (one component of
+    // the state records, or a plain array, times `scale`) into this context's FP64 read-back
+    // buffer, allocated on the first read-back and kept, and one cudaMemcpyAsync moves it to the
+    // caller's memory (page-locked memory is read at the full link rate).  Nothing is shared
+    // between contexts.
+    Dev<double> rb;
+    double* readback_buffer() {
+        if (rb.n != n) rb.alloc(n);
+        return rb.p;
+    }
+    void copy_out(const double* dev, double* out) {
+        HP_CK(cudaGetLastError());
+        HP_CK(cudaMemcpyAsync(out, dev, n * sizeof(double), cudaMemcpyDeviceToHost, st()));
+        HP_CK(cudaStreamSynchronize(st()));
+    }
+    void fetch_scaled(const R* src, double scale, double* out) {
+        double* d = readback_buffer();
+        k_scaled_f64<R><<<blocks_for(n), kThreads, 0, st()>>>(n, src, scale, d);
+        copy_out(d, out);
     }
     void fetch_component_scaled(int comp, double scale, double* out) {
         pull_sc();
-        Dev<R> tmp;
-        tmp.alloc(n);
-        k_state_component<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, comp, tmp.p);
-        HP_CK(cudaGetLastError());
-        fetch_scaled(tmp.p, n, scale, out);
+        double* d = readback_buffer();
+        k_state_component_f64<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, comp, scale, d);
+        copy_out(d, out);
     }
 
     std::vector<V4> fetch_state() {
@@ -1427,7 +1561,7 @@ template <typename R> struct Impl : Base {
             case HP2D_FIELD_ARRIVAL: { auto v = fetch(arrival.p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) / 60.0; break; }
             case HP2D_FIELD_VMAX: case HP2D_FIELD_HAZARD_MAX: {
                 if (!hz_on) { ctx->err = "velocity / hazard maxima are off (hp2d_set_hazard_tracking)"; return HP2D_NOT_READY; }
-                fetch_scaled(field == HP2D_FIELD_VMAX ? vmaxm.p : hzmaxm.p, n, 1.0, out);
+                fetch_scaled(field == HP2D_FIELD_VMAX ? vmaxm.p : hzmaxm.p, 1.0, out);
                 break;
             }
             case HP2D_FIELD_SOIL_STORAGE: {
@@ -1510,6 +1644,9 @@ template <typename R> struct Impl : Base {
         o->neg_depth_warnings = hs.neg_warn;
         o->unstable_steps = hs.unstable;
         o->status_bits = hs.status;
+        o->retries = hs.retries;
+        o->catch_index = hs.catch_index;
+        o->max_time_step = hs.max_dt;
         return HP2D_OK;
     }
 
@@ -1564,11 +1701,12 @@ struct hp2d_ensemble {
     int cells_per_lane = 2;   // layout of the streamed strips (as hp2d_set_layout)
     int ga = -1, map = -1;
     bool infl = false;   // some member has inflow hydrographs
-    int grid_for[3][2] = {};
+    int sch = 0;         // members' faces: 0 Bates, 1 schemes 2/3 (members agree on the kind)
+    int grid_for[3][3] = {};
     cudaGraphExec_t graph = nullptr;
     int graph_members = -1, graph_rpw = -1, graph_cpl = -1, graph_kind = -1;
     // the kernel variant a captured graph launches
-    int kind() const { return ga * 4 + map * 2 + (infl ? 1 : 0); }
+    int kind() const { return sch * 16 + ga * 4 + map * 2 + (infl ? 1 : 0); }
 
     Impl<float>& impl(int m) { return *static_cast<Impl<float>*>(members[m]->impl.get()); }
 
@@ -1577,21 +1715,25 @@ struct hp2d_ensemble {
         graph = nullptr;
     }
 
-    template <int INF, bool MAP, int CPL, bool INFL> void launch_t(int nm) {
+    template <int INF, bool MAP, int CPL, bool INFL, int SCH = 0> void launch_t(int nm) {
         const size_t smem = fused_smem_bytes<float, CPL>(kThreads);
-        int& grid = grid_for[CPL][INFL ? 1 : 0];
+        int& grid = grid_for[CPL][INFL ? 1 + SCH : 0];
         if (grid == 0) {
             int per_sm = 0, sms = 0;
             HP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &per_sm, k_ens_step<float, kThreads, INF, MAP, CPL, INFL>, kThreads, smem));
+                &per_sm, k_ens_step<float, kThreads, INF, MAP, CPL, INFL, SCH>, kThreads, smem));
             HP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
             grid = std::max(1, per_sm) * sms;
         }
         k_ens_plan<float><<<1, 1024, 0, stream>>>(args.p, nm, prefix.p, queue.p);
-        k_ens_step<float, kThreads, INF, MAP, CPL, INFL><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p,
-                                                                                        queue.p);
+        k_ens_step<float, kThreads, INF, MAP, CPL, INFL, SCH><<<grid, kThreads, smem, stream>>>(args.p, nm, prefix.p,
+                                                                                             queue.p);
     }
     template <int INF, int CPL> void launch_m(int nm) {
+        if (sch) {
+            if (map) launch_t<INF, true, CPL, true, 1>(nm); else launch_t<INF, false, CPL, true, 1>(nm);
+            return;
+        }
         if (map) {
             if (infl) launch_t<INF, true, CPL, true>(nm); else launch_t<INF, true, CPL, false>(nm);
         } else {
@@ -1621,10 +1763,15 @@ struct hp2d_ensemble {
                 return HP2D_NOT_READY;
             }
             const int mga = im.inf_mode(), mmap = im.rain.n_maps > 0 ? 1 : 0;
-            if (m == 0) { ga = mga; map = mmap; infl = false; }
+            const int msch = members[m]->p.flag_numerical_scheme != 1 ? 1 : 0;
+            if (m == 0) { ga = mga; map = mmap; infl = false; sch = msch; }
             if (im.bc_kernel()) infl = true;
             if (mga != ga || mmap != map) {
                 err = "members must agree on the infiltration model and on the kind of rain forcing";
+                return HP2D_INVALID_ARG;
+            }
+            if (msch != sch) {
+                err = "members must agree on Bates (flag_numerical_scheme 1) against the schemes 2/3";
                 return HP2D_INVALID_ARG;
             }
             HP_CK(cudaSetDevice(device));
@@ -1634,6 +1781,10 @@ struct hp2d_ensemble {
                 im.invalidate_graph();
             }
             im.prologue();
+            if (im.bad_state) {
+                err = "member " + std::to_string(m) + ": " + (im.bad_state_error(), members[m]->err);
+                return HP2D_NUMERICAL;
+            }
             im.dry_for_layout(cells_per_lane);   // the ensemble's layout may differ from the member's
             HP_CK(cudaStreamSynchronize(im.st()));
             host[m] = im.fused_args(cells_per_lane);
@@ -1695,7 +1846,18 @@ struct hp2d_ensemble {
             impl(m).pull_sc();
             impl(m).flush_records();
         }
-        if (n_active) *n_active = int32_t(q.n_active);
+        unsigned retried = 0;
+        for (int m = 0; m < nm; ++m) {   // a rejected member step: its retry, as on its own
+            Impl<float>& im = impl(m);
+            if (!im.hs.halted || (im.hs.status & kStatusTimeout)) continue;
+            const hp2d_status s = im.handle_halt();
+            if (s != HP2D_OK) {
+                err = "member " + std::to_string(m) + ": " + members[m]->err;
+                return s;
+            }
+            ++retried;   // halted members were not counted as running
+        }
+        if (n_active) *n_active = int32_t(q.n_active + retried);
         if (q.stalled) {
             err = std::to_string(q.stalled) + " member(s) stopped: a row copy did not complete within its wait limit";
             return HP2D_TIMEOUT;
@@ -1752,7 +1914,7 @@ struct hp2d_ensemble {
             if (ms < best_ms) { best_ms = ms; best = c; best_cpl = cpl; }
             for (int m = 0; m < nm; ++m) {
                 impl(m).pull_sc();
-                stalled = stalled || (impl(m).hs.status & 2u) != 0;
+                stalled = stalled || (impl(m).hs.status & kStatusTimeout) != 0;
                 impl(m).put_back(*snaps[m]);
             }
         }
@@ -1798,7 +1960,7 @@ hp2d_status hp2d_create(const hp2d_grid* grid, const hp2d_params* params, int32_
     if (p.flag_subgrid != 0) { g_create_error = "flag_subgrid=1 is not supported"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_D8 != 0) { g_create_error = "flag_D8=1 is not supported"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_reservoir != 0 && p.flag_reservoir != 1) { g_create_error = "flag_reservoir must be 0 or 1"; return HP2D_INVALID_ARG; }
-    if (p.flag_numerical_scheme != 1) { g_create_error = "only flag_numerical_scheme=1 (Bates) is supported"; return HP2D_UNSUPPORTED_FLAG; }
+    if (p.flag_numerical_scheme < 1 || p.flag_numerical_scheme > 3) { g_create_error = "flag_numerical_scheme must be 1 (Bates), 2 (s-upwind) or 3 (s-centred)"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_infiltration < 0 || p.flag_infiltration > 2) { g_create_error = "flag_infiltration must be 0, 1 (Green-Ampt) or 2 (van Genuchten)"; return HP2D_UNSUPPORTED_FLAG; }
     if (p.flag_critical != 0 && p.flag_critical != 1) { g_create_error = "flag_critical must be 0 or 1"; return HP2D_INVALID_ARG; }
     if (p.outlet_type != 1 && p.outlet_type != 2) { g_create_error = "outlet_type must be 1 or 2"; return HP2D_INVALID_ARG; }
@@ -2013,6 +2175,24 @@ hp2d_status hp2d_set_tuning(hp2d_ctx* ctx, int32_t rows_per_warp) {
 
 hp2d_status hp2d_run(hp2d_ctx* ctx, int64_t max_steps, int64_t* steps_done) {
     return with_impl(ctx, [&](auto& m) { return m.run(max_steps, steps_done); });
+}
+
+hp2d_status hp2d_set_retry_policy(hp2d_ctx* ctx, int32_t max_retries, double factor_reduction,
+                                  int32_t dt_floor_is_error) {
+    return with_impl(ctx, [&](auto& m) { return m.set_retry_policy(max_retries, factor_reduction, dt_floor_is_error); });
+}
+
+hp2d_status hp2d_set_wait_limit(hp2d_ctx* ctx, int64_t polls) {
+    if (polls < 0 || polls > int64_t(0xffffffffu)) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) {
+        m.wait_polls = unsigned(polls);
+        m.invalidate_graph();
+        return HP2D_OK;
+    });
+}
+
+hp2d_status hp2d_inject_step_fault(hp2d_ctx* ctx, int64_t k, int32_t attempts) {
+    return with_impl(ctx, [&](auto& m) { return m.inject_fault(k, attempts); });
 }
 
 hp2d_status hp2d_download(hp2d_ctx* ctx, int32_t field, double* host, size_t count) {

@@ -134,7 +134,7 @@ struct StepScalars {
     double vmax_last;      // velocities.max_velocity of the last refresh
     double rain_vol, inf_vol, out_vol;   // cumulative [m^3]
     long long neg_warn, unstable;
-    unsigned int status;   // bit 0: non-finite depth seen
+    unsigned int status;   // kStatus* bits
     unsigned int counter;  // CTAs done with the current step
     unsigned long long acc_vmax;   // max speed of the step (ordered bits)
     unsigned long long acc_cmax;   // max wave celerity of non-stagnant cells (ordered bits)
@@ -159,7 +159,30 @@ struct StepScalars {
                                         // in its output buffer and did not rewrite
     unsigned long long skipped_read_cells;   // of those, cells of whole skipped row blocks
                                              // (their records were not read either)
+    // Failure handling (HydroPol2D_Main_While.m:926-993).  A step is rejected when more cells
+    // end it with a depth that is non-finite or below -depth_tolerance than had a non-finite
+    // depth when the run started (idx_nan walls keep theirs), when a row copy timed out, or
+    // when the host's test hook asks for it; a rejected step commits nothing (the state stays
+    // in the buffer it was read from, the clock and counters stay) and halts the launches
+    // until the host has prepared its retry.
+    unsigned long long acc_bad;     // step sum: cells ending non-finite or too negative
+    unsigned long long n_bad0;      // cells with a non-finite depth at the start of the run
+    int halted;                     // 1: launches are no-ops until the host clears it
+    int catch_index;                // the reference's catch_index (1 before any failure)
+    long long fault_k;              // test hook: attempts of step fault_k are rejected ...
+    int fault_n;                    // ... this many times
+    int dt_floor_stop;              // 1: a step whose refreshed dt equals min_time_step halts after it
+    double max_dt;                  // running_control.max_time_step [s], lowered by retries
+    long long retries;              // rejected attempts so far
+    unsigned long long retry_dmax;  // retry scan: max depth of d_p and d_tot [m] (ordered bits)
+    int bad_domain;                 // start-of-run scan: a cell of finite elevation holds a
+                                    // non-finite depth
+    int pad3;
 };
+// StepScalars::status bits
+constexpr unsigned kStatusNumerical = 1u;   // a step was rejected (non-finite / negative depth)
+constexpr unsigned kStatusTimeout = 2u;     // a row copy did not land within the wait limit
+constexpr unsigned kStatusDtFloor = 4u;     // the refreshed dt hit min_time_step (dt_floor_stop)
 
 // ---------------- map records (save_output_maps.m) -----------------------------------
 // After a step whose t_save = t + new dt passes a record time (time_records, 0-based index
@@ -587,6 +610,14 @@ __device__ __forceinline__ R vg_infiltration(R& hh, R& Ic, R zwt, const SoilClas
     return fd;
 }
 
+// momentum term of schemes 2 and 3 for a face with Hf > 0 (see face_flux)
+template <typename R>
+__device__ __forceinline__ R diffused_momentum(R qp, R q_lo, R q_hi, R Hf, const StepConsts<R>& K, int scheme) {
+    const R th = R(1) - K.dt_over_dx * fmin(qdiv(fabs(qp), Hf), sqrt(K.g * Hf));
+    const R qnb = scheme == 2 ? (qp < R(0) ? q_hi : q_lo) : R(0.5) * (q_lo + q_hi);
+    return th * qp + (R(1) - th) * qnb;
+}
+
 // ---------------- one face of the local-inertial momentum update ----------------------
 // x face: (ha, hb) = (left, right) cells, dz = z_right - z_left.
 // y face: (ha, hb) = (upper, lower) cells (row i-1, row i), dz = z_upper - z_lower.
@@ -597,9 +628,22 @@ __device__ __forceinline__ R vg_infiltration(R& hh, R& Ic, R zwt, const SoilClas
 // depth still enters the wave celerity of refreshing_timestep.
 // Faces that carry no water leave early: whole warps of them skip the power and the
 // division, which matters on wet/dry fronts.
-template <typename R, bool IS_X>
+//
+// SCH = 0: Bates (flag_numerical_scheme 1, Inertial_Solver.m:23-26).  SCH = 1: the schemes
+// with numerical diffusion chosen at run time by `scheme` (Inertial_Solver.m:29-121): the
+// momentum term q_p of the numerator becomes theta q_p + (1 - theta) q_nb with
+//   theta = 1 - dt/dx min(|q_p|/Hf, sqrt(g Hf))           (:61, :84; NaN -> 1 at :86 is
+//                                                          never reached for Hf > 0)
+//   q_nb  = q_lo if q_p >= 0, else q_hi                    (scheme 2, s-upwind, :35-58)
+//   q_nb  = (q_lo + q_hi) / 2                              (scheme 3, s-centred, :91-98)
+// where q_lo / q_hi are the previous fluxes of the same direction one face before / after
+// (x: columns j-1, j+1; y: rows i-1, i+1), zero on the first and last column (x) or row
+// (y), as the reference's interior ranges 2:(end-1) leave them.  The friction term keeps
+// |q_p| (total_flux = q_p, :31, :101).
+template <typename R, bool IS_X, int SCH = 0>
 __device__ __forceinline__ void face_flux(R ha, R hb, R dz, R qp, R n2c, const StepConsts<R>& K,
-                                          int flag_critical, R& Hf, R& q) {
+                                          int flag_critical, R& Hf, R& q, int scheme = 1, R q_lo = R(0),
+                                          R q_hi = R(0)) {
     if (!(fabs(dz) <= R(3.0e38))) {
         // NaN dz: MATLAB's max over the two sides skips the NaN one
         Hf = isnan(dz) ? fmax(fmax(ha, hb), R(0)) : R(0);
@@ -617,7 +661,9 @@ __device__ __forceinline__ void face_flux(R ha, R hb, R dz, R qp, R n2c, const S
         S = (dz + (ha - hb)) * K.inv_dx;
     }
     if (!(Hf > R(0))) { q = R(0); return; }
-    R num = fma(-(K.gdt * Hf), S, qp);   // one rounding for qp - (g dt Hf) S
+    R qn = qp;
+    if (SCH) qn = diffused_momentum(qp, q_lo, q_hi, Hf, K, scheme);
+    R num = fma(-(K.gdt * Hf), S, qn);   // one rounding for qn - (g dt Hf) S
     R h73 = pow73_pos(Hf);
     R den = fma(K.gdt * n2c, fabs(qp), h73);
     R qq = qdiv(num * h73, den);
@@ -628,6 +674,49 @@ __device__ __forceinline__ void face_flux(R ha, R hb, R dz, R qp, R n2c, const S
     }
     R thr = Hf * R(10);
     q = fmin(fmax(qq, -thr), thr);
+}
+
+// face_flux split in two for the fused kernel's interleaved faces: face_geom gives the face
+// depth Hf, the slope S and whether the face carries water (open and Hf > 0); face_momentum is
+// the update of a wet face, written without branches so that the independent faces of a row
+// (two directions, CPL cells per lane) can be interleaved.  For a wet face the two together
+// perform the same operations on the same values as face_flux; a face that is not wet is given
+// q = 0 (its momentum is evaluated on harmless operands and discarded).
+template <typename R, bool IS_X>
+__device__ __forceinline__ bool face_geom(R ha, R hb, R dz, R& Hf, R& S, const StepConsts<R>& K) {
+    const bool open = fabs(dz) <= R(3.0e38);
+    const R a = fmax(ha, R(0)), b = fmax(hb, R(0));
+    R Ho;
+    if (IS_X) {
+        Ho = fmax(fmax(a - fmax(dz, R(0)), b + fmin(dz, R(0))), R(0));
+        S = (dz + (b - a)) * K.inv_dx;
+    } else {
+        Ho = fmax(fmax(a + fmin(dz, R(0)), b - fmax(dz, R(0))), R(0));
+        S = (dz + (a - b)) * K.inv_dx;
+    }
+    // closed faces: NaN dz (next to an idx_nan cell) keeps the inside cell's depth, +inf none
+    Hf = open ? Ho : (isnan(dz) ? fmax(fmax(ha, hb), R(0)) : R(0));
+    return open && Ho > R(0);
+}
+template <typename R, int SCH = 0>
+__device__ __forceinline__ R face_momentum(bool wet, R Hf, R S, R qp, R n2c, const StepConsts<R>& K, int flag_critical,
+                                           int scheme = 1, R q_lo = R(0), R q_hi = R(0)) {
+    const R H = wet ? Hf : R(1);
+    const R Sl = wet ? S : R(0);
+    R qn = qp;
+    if (SCH) qn = diffused_momentum(qp, q_lo, q_hi, H, K, scheme);
+    const R num = fma(-(K.gdt * H), Sl, qn);
+    const R h73 = pow73_pos(H);
+    const R den = fma(K.gdt * n2c, fabs(qp), h73);
+    R qq = qdiv(num * h73, den);
+    qq = isfinite(qq) ? qq : R(0);
+    if (flag_critical == 1) {
+        const R crit = H * sqrt(K.g * H);
+        qq = fmin(fmax(qq, -crit), crit);
+    }
+    const R thr = H * R(10);
+    qq = fmin(fmax(qq, -thr), thr);
+    return wet ? qq : R(0);
 }
 
 // outgoing rate of a cell over its four faces and its donor scale factor

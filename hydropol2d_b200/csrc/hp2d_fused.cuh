@@ -50,6 +50,9 @@ constexpr int kStages = HP2D_STAGES;   // shared-memory ring depth of the row pi
 #define HP2D_ROW_UNROLL 1
 #endif
 constexpr int kRowUnroll = HP2D_ROW_UNROLL;   // row-loop unroll (register renaming of the window)
+#ifndef HP2D_FACE_ILP
+#define HP2D_FACE_ILP 0   // 1: the faces of a row as interleaved, branch-free momentum updates
+#endif
 
 // dynamic shared memory of k_fused_step: per warp kStages x (2 records x 32*CPL cells)
 template <typename R, int CPL = 1> constexpr size_t fused_smem_bytes(int nt) {
@@ -66,6 +69,8 @@ template <typename R> struct FusedArgs {
     double t_end;                // routing_time + min_time_step/60 [min]
     double min_dt, max_dt, inc, tsc, alfa_min, alfa_max;
     int flag_timestep, adaptive, flag_critical, outlet_type, ga;   // ga: infiltration on (either model)
+    int scheme;                  // flag_numerical_scheme: 1 Bates, 2 s-upwind, 3 s-centred
+    unsigned int wait_polls;     // polls of a row-copy wait before it gives up (HP2D_TIMEOUT)
     unsigned int n_ctas;
     R stag_s2;
     const V4* stat;
@@ -185,7 +190,9 @@ template <int CPL> struct FusedOcc<double, CPL> { static constexpr int minb = CP
 // shared-memory ring).
 // INF: infiltration model (0 none, 1 Green-Ampt, 2 van Genuchten); MAP: rain from coarse
 // maps (else a uniform rate); INFL: inflow hydrographs present (the grids without them do not
-// carry the lookup)
+// carry the lookup); SCH: 0 Bates faces, 1 the schemes with numerical diffusion
+// (flag_numerical_scheme 2 or 3, a.scheme), whose faces also read the previous fluxes of the
+// neighbouring faces of the same direction
 // The depth d_tot a step hands to its fluxes at each control structure's reservoir cell --
 // phase (A) of that cell restated: rain, infiltration, inflow, clamps, from the state and
 // soil records `st`/`gs` the step starts from -- then the structures' transfers (one thread,
@@ -219,7 +226,7 @@ __device__ __noinline__ void structure_prepare(const FusedArgs<R>& a, const Rain
     if (tid == 0) structure_transfers(a.strct, time_step, a.res * a.res);
 }
 
-template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>
+template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false, int SCH = 0>
 __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned blk) {
     using V4 = typename Vec<R>::V4;
     using V2 = typename Vec<R>::V2;
@@ -237,6 +244,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     __shared__ unsigned long long red_c[NT / 32];
     __shared__ double red_d[3][NT / 32];
     __shared__ int red_to[NT / 32];
+    __shared__ unsigned red_bad[NT / 32];
     __shared__ __align__(8) unsigned long long s_bar[NT / 32][kStages];
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     bool timed_out = false;
@@ -253,7 +261,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         s_skipw = 0u;
         s_skipr = 0u;
         s_rec = (sc->rec_pending && a.rec.n_slots > 0) ? int(sc->rec_count % a.rec.n_slots) : -1;
-        s_done = !(s_tmin <= a.t_end);
+        s_done = !(s_tmin <= a.t_end) || sc->halted;
         s_K.make(s_dts, a.res, a.tol_mm, a.thr_mm);
         s_rs.make(a.rain, sc->rain_a, sc->rain_b);
         // the next step applies the rain of [t_previous, t] (HydroPol2D_Main_While.m:721)
@@ -283,6 +291,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     // per-lane partial sums of the volume ledger in the state precision, Kahan-compensated
     // (the warps' sums and everything after them are FP64)
     Kahan<R> rain_acc_r, inf_acc_r, out_acc_r;
+    unsigned nbad = 0u;                       // own cells ending non-finite or below -tol
     unsigned dry = 0u;                        // bit i: row r-i dry across the strip
     R s2max = R(0);
     R cmaxv = R(-1);   // largest celerity term of a non-stagnant cell (-1: none yet)
@@ -307,10 +316,15 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         unsigned own_n = 0;   // cells of the strip this warp stores
 #pragma unroll
         for (int h = 0; h < CPL; ++h) own_n += __popc(__ballot_sync(FULL, own_lane[h]));
-        // the flags of this warp's rows, four per lane (read once: each row's flag changes only
-        // at that row)
-        unsigned dfw = 0u;
-        if (dfl && r0 + 4 * lane < r_end) dfw = *reinterpret_cast<const unsigned*>(dfl + r0 + 4 * lane);
+        // the flags of this warp's rows in the output buffer and in the input buffer, four per
+        // lane (read once: each row's output flag changes only at that row, the input flags not
+        // at all during the step)
+        unsigned dfw = 0u, dfw_in = 0u;
+        if (dfl && r0 + 4 * lane < r_end) {
+            dfw = *reinterpret_cast<const unsigned*>(dfl + r0 + 4 * lane);
+            dfw_in = *reinterpret_cast<const unsigned*>(a.dryflag + (size_t(cur) * a.n_strips + strip) * size_t(a.dry_rows) +
+                                                        r0 + 4 * lane);
+        }
         // The whole block of rows: when this step adds no rain and no infiltration and records
         // no map, and the flags show every input row r0-1..r_end+1 of this strip and of its
         // neighbours (the 2-column aprons) deep-dry and every output row already holding the
@@ -349,9 +363,11 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         // rolling window (suffix = rows back), one entry per cell of the lane
         R hT1[CPL], hT2[CPL], qxu1[CPL], qyu1[CPL], hfx1[CPL], hfx2[CPL], hfy1[CPL], hfy2[CPL];
         R sc2[CPL], qxl2[CPL], qyl2[CPL], dm1[CPL], dm2[CPL];
+        R qyp1[CPL];   // schemes 2/3: previous q_y of the row before
         unsigned mt1[CPL], mt2[CPL];
 #pragma unroll
         for (int h = 0; h < CPL; ++h) {
+            qyp1[h] = R(0);
             hT1[h] = hT2[h] = qxu1[h] = qyu1[h] = R(0);
             hfx1[h] = hfx2[h] = hfy1[h] = hfy2[h] = R(0);
             sc2[h] = R(1);
@@ -412,11 +428,13 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             const bool frow_f = r - 2 >= r0 && r - 2 < r_end;
             const int fri = frow_f ? r - 2 - r0 : 0;
             const unsigned flg = frow_f ? (__shfl_sync(FULL, dfw, fri >> 2) >> (8 * (fri & 3))) & 255u : 0u;
-            const bool landed = mbar_wait_bounded(bar0 + 8u * s, uint32_t((k / kStages) & 1), 1u << 22);
+            const unsigned flg_in = frow_f ? (__shfl_sync(FULL, dfw_in, fri >> 2) >> (8 * (fri & 3))) & 255u : 0u;
+            const bool landed = mbar_wait_bounded(bar0 + 8u * s, uint32_t((k / kStages) & 1), a.wait_polls);
             if (__any_sync(FULL, !landed)) {   // the whole warp leaves the loop together
                 timed_out = true;
-                // let the copies still in flight land before the CTA leaves
-                for (int kk = k + 1; kk < k + kStages && kk <= last_k; ++kk)
+                // let every copy still in flight (rows k .. k+kStages-1, this one included) land
+                // before the CTA leaves, with the long limit whatever a.wait_polls is
+                for (int kk = k; kk < k + kStages && kk <= last_k; ++kk)
                     mbar_wait_bounded(bar0 + 8u * (kk % kStages), uint32_t((kk / kStages) & 1), 1u << 22);
                 break;
             }
@@ -495,9 +513,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 for (int h = 0; h < CPL; ++h) plain = plain && (mt2[h] >> 8) == 0u;
                 if (__all_sync(FULL, plain)) {
                     const int rm2 = r - 2;
-                    if (frow_f && flg) {
-                        // this buffer already holds the row as this step would write it (the
-                        // same deep-dry row two steps ago; nothing else wrote the buffer since)
+                    if (frow_f && flg && flg_in) {
+                        // this buffer already holds the row as this step would write it: the
+                        // deep-dry record of two steps ago, and the step between wrote the
+                        // deep-dry record into the other buffer (so the running maximum did not
+                        // move; a row that got water in between and lost it again by the next
+                        // step -- rain soaked up by the soil -- is written)
                         if (lane == 0) atomicAdd(&s_skipw, own_n);
                     } else if (frow_f) {
 #pragma unroll
@@ -517,6 +538,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         hT2[h] = hT1[h]; hT1[h] = hT0[h];
                         dm2[h] = dm1[h]; dm1[h] = X[h].w;
                         mt2[h] = mt1[h]; mt1[h] = meta[h];
+                        if (SCH) qyp1[h] = X[h].z;
                     }
                     continue;
                 }
@@ -531,14 +553,72 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 // (B) x face (r, j) between (r, j) and (r, j+1)
                 R hR[CPL];
                 right_of<R, CPL>(hT0, hR, lane);
+                // schemes 2/3: previous q_x of the faces j-1 and j+1 (interior columns only);
+                // lane 0's left neighbour lies outside the strip and is read from memory
+                R qxa[CPL], qxb[CPL];
+                if (SCH) {
+                    R xq[CPL];
+#pragma unroll
+                    for (int h = 0; h < CPL; ++h) xq[h] = X[h].y;
+                    left_of<R, CPL>(xq, qxa, lane);
+                    right_of<R, CPL>(xq, qxb, lane);
+                    if (lane == 0 && rok && j[0] >= 1) qxa[0] = sin[size_t(r) * nx + (j[0] - 1)].y;
+#pragma unroll
+                    for (int h = 0; h < CPL; ++h)
+                        if (!(j[h] >= 1 && j[h] + 1 < nx)) qxa[h] = qxb[h] = R(0);
+                }
+#if HP2D_FACE_ILP
+                // (B) and (C) interleaved: the geometry of the 2 x CPL faces, then -- unless no
+                // lane of the warp has a wet one -- their momentum updates without branches
+                R Sx[CPL], Sy[CPL], ya[CPL], yb[CPL];
+                bool wx[CPL], wy[CPL];
+                bool any_wet = false;
+#pragma unroll
+                for (int h = 0; h < CPL; ++h) {
+                    const bool inx = col_ok[h] && rok;
+                    const bool iny = inx && r >= r0 - 1;
+                    R H;
+                    wx[h] = face_geom<R, true>(hT0[h], hR[h], S[h].x, H, Sx[h], K) && inx;
+                    hfx0[h] = inx ? H : R(0);
+                    wy[h] = face_geom<R, false>(hT1[h], hT0[h], S[h].y, H, Sy[h], K) && iny;
+                    hfy0[h] = iny ? H : R(0);
+                    any_wet = any_wet || wx[h] || wy[h];
+                    ya[h] = yb[h] = R(0);
+                    // schemes 2/3: the previous q_y of rows r-1 (kept from the row before) and r+1
+                    if (SCH && wy[h] && r >= 1 && r + 1 < ny) {
+                        ya[h] = qyp1[h];
+                        yb[h] = sin[size_t(r + 1) * nx + j[h]].z;
+                    }
+                }
+                if (__any_sync(FULL, any_wet)) {
+#pragma unroll
+                    for (int h = 0; h < CPL; ++h) {
+                        qxu0[h] = face_momentum<R, SCH>(wx[h], hfx0[h], Sx[h], X[h].y, S[h].z, K, a.flag_critical,
+                                                         a.scheme, SCH ? qxa[h] : R(0), SCH ? qxb[h] : R(0));
+                        qyu0[h] = face_momentum<R, SCH>(wy[h], hfy0[h], Sy[h], X[h].z, S[h].z, K, a.flag_critical,
+                                                         a.scheme, ya[h], yb[h]);
+                    }
+                }
+#else
 #pragma unroll
                 for (int h = 0; h < CPL; ++h)
-                    if (col_ok[h] && rok) face_flux<R, true>(hT0[h], hR[h], S[h].x, X[h].y, S[h].z, K, a.flag_critical, hfx0[h], qxu0[h]);
-                // (C) y face (r, j) between (r-1, j) and (r, j)
+                    if (col_ok[h] && rok)
+                        face_flux<R, true, SCH>(hT0[h], hR[h], S[h].x, X[h].y, S[h].z, K, a.flag_critical, hfx0[h],
+                                                qxu0[h], a.scheme, SCH ? qxa[h] : R(0), SCH ? qxb[h] : R(0));
+                // (C) y face (r, j) between (r-1, j) and (r, j); schemes 2/3 read the previous
+                // q_y of rows r-1 (kept from the row before) and r+1 (from memory)
 #pragma unroll
                 for (int h = 0; h < CPL; ++h)
-                    if (col_ok[h] && rok && r >= r0 - 1)
-                        face_flux<R, false>(hT1[h], hT0[h], S[h].y, X[h].z, S[h].z, K, a.flag_critical, hfy0[h], qyu0[h]);
+                    if (col_ok[h] && rok && r >= r0 - 1) {
+                        R ya = R(0), yb = R(0);
+                        if (SCH && r >= 1 && r + 1 < ny) {
+                            ya = qyp1[h];
+                            yb = sin[size_t(r + 1) * nx + j[h]].z;
+                        }
+                        face_flux<R, false, SCH>(hT1[h], hT0[h], S[h].y, X[h].z, S[h].z, K, a.flag_critical, hfy0[h],
+                                                 qyu0[h], a.scheme, ya, yb);
+                    }
+#endif
                 // (D) donor scale of (r-1, j)
                 R qxu1_left[CPL];
                 left_of<R, CPL>(qxu1, qxu1_left, lane);
@@ -580,6 +660,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         if (ss >= 0) h_in = h_in + a.strct.extra[ss];
                     }
                     R hn = quiet ? h_in + R(0) : continuity(h_in, qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
+                    const R negtol = -K.tol;
                     R hf3 = R(0);
                     const unsigned ord = outlet_ord(mt2[h]);
                     if (ord) {
@@ -607,6 +688,9 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                             hn = sv;
                         }
                     }
+                    // a non-finite depth (NaN walls included, counted against the run's start)
+                    // or one below -depth_tolerance
+                    nbad += (hn >= negtol) ? 0u : 1u;
                     const R dm = dm2[h];
                     if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
                     // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
@@ -664,6 +748,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                 qxl2[h] = qxl1[h]; qyl2[h] = qyl1[h];
                 dm2[h] = dm1[h]; dm1[h] = X[h].w;
                 mt2[h] = mt1[h]; mt1[h] = meta[h];
+                if (SCH) qyp1[h] = X[h].z;
             }
         }
         // every phase of the ring's barriers has completed: retire them so that the next
@@ -689,7 +774,9 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     inf_acc = warp_sum(inf_acc);
     out_acc = warp_sum(out_acc);
     const int to_any = __any_sync(0xffffffffu, timed_out);
+    nbad = __reduce_add_sync(0xffffffffu, nbad);
     if (lane_ == 0) {
+        red_bad[warp_] = nbad;
         red_s2[warp_] = s2max;
         red_c[warp_] = cenc;
         red_d[0][warp_] = rain_acc;
@@ -702,7 +789,10 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
     if (tid == 0) {
         int to = 0;
         for (int w = 0; w < NT / 32; ++w) to |= red_to[w];
-        if (to) atomicOr(&a.sc->status, 2u);   // a row copy did not arrive in time
+        if (to) atomicOr(&a.sc->status, kStatusTimeout);   // a row copy did not arrive in time
+        unsigned bad = 0u;
+        for (int w = 0; w < NT / 32; ++w) bad += red_bad[w];
+        if (bad) atomicAdd(&a.sc->acc_bad, (unsigned long long)bad);
         for (int w = 1; w < NT / 32; ++w) {
             s2max = fmax(s2max, red_s2[w]);
             cenc = red_c[w] > cenc ? red_c[w] : cenc;
@@ -732,6 +822,38 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
 
     // ---- last CTA: refreshing_timestep + clock (HydroPol2D_Main_While.m:691-705, :779)
     __threadfence();
+    // a rejected step commits nothing: the state stays in buffer cur, the clock, counters and
+    // volumes stay, and the launches halt until the host has prepared the retry
+    // (HydroPol2D_Main_While.m:926-993); s_last doubles as the verdict for the CTA below
+    if (tid == 0) {
+        StepScalars* sc = a.sc;
+        bool reject = (atomicAdd(&sc->status, 0u) & kStatusTimeout) != 0u;
+        if (atomicAdd(&sc->acc_bad, 0ull) > sc->n_bad0) {
+            reject = true;
+            sc->status |= kStatusNumerical;
+        }
+        if (sc->fault_n > 0 && sc->k == sc->fault_k) {   // the host's test hook
+            sc->fault_n -= 1;
+            reject = true;
+            sc->status |= kStatusNumerical;
+        }
+        if (reject) {
+            sc->halted = 1;
+            if (s_skip) sc->neg_warn -= 1;   // the attempt's clamp warning is withdrawn
+            sc->acc_vmax = 0ull;
+            sc->acc_cmax = 0ull;
+            sc->acc_rain = 0.0;
+            sc->acc_inf = 0.0;
+            sc->acc_out = 0.0;
+            sc->acc_stage = 0.0;
+            sc->acc_bad = 0ull;
+            sc->counter = 0u;
+            atomicExch(&sc->skip_next, 0);
+            s_last = 0;
+        }
+    }
+    __syncthreads();
+    if (!s_last) return cta_ok;
     if (tid == 0) {
         StepScalars* sc = a.sc;
         const unsigned long long vbits = atomicAdd(&sc->acc_vmax, 0ull);
@@ -755,10 +877,16 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->tsp = time_save;
         double tcr = sc->time_step * 60.0;   // refreshing_timestep.m:361-365
         if (delta > 0 || sc->k == 1) {
-            tcr = finalize_dt(vm, cm, a.res, a.alfa_min, a.alfa_max, a.min_dt, a.max_dt, a.inc,
+            tcr = finalize_dt(vm, cm, a.res, a.alfa_min, a.alfa_max, a.min_dt, sc->max_dt, a.inc,
                               a.flag_timestep);
             sc->vmax_last = vm;
-            if (tcr == a.min_dt) sc->unstable += 1;
+            if (tcr == a.min_dt) {   // refreshing_timestep.m:357-359 (unstable)
+                sc->unstable += 1;
+                if (sc->dt_floor_stop) {
+                    sc->status |= kStatusDtFloor;
+                    sc->halted = 1;   // this step is kept; the next launches wait for the host
+                }
+            }
         }
         const double area = a.res * a.res;
         sc->rain_vol += rain_s * area;
@@ -802,6 +930,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         sc->acc_rain = 0.0;
         sc->acc_inf = 0.0;
         sc->acc_out = 0.0;
+        sc->acc_bad = 0ull;
         sc->counter = 0u;
         sc->skip_clamp = atomicExch(&sc->skip_next, 0);   // gathered by every CTA's outlets
     }
@@ -861,7 +990,9 @@ static __global__ void k_idw_maps(int ny, int nx, double res, double x_ul, doubl
 
 // ---------------- host boundary on the device: records built from the caller's arrays ----
 // static record {dz_x, dz_y, n^2, meta} and the unfused path's copies, from the elevation and
-// roughness in FP64 (dz formed in FP64 and rounded once; the closed domain edges +inf)
+// roughness in FP64 (dz formed in FP64 and rounded once; the closed domain edges +inf).  A cell
+// of NaN elevation (idx_nan) gets n^2 = NaN: its own faces are closed by their NaN dz before
+// n^2 is read, so the NaN only marks the cell as outside the domain (k_skip_flag reads it).
 template <typename R>
 __global__ void k_build_static(int ny, int nx, const double* z, const double* rough, const uint32_t* meta,
                                typename Vec<R>::V4* stat, R* dzx, R* dzy, R* n2) {
@@ -871,11 +1002,23 @@ __global__ void k_build_static(int ny, int nx, const double* z, const double* ro
         const int i = int(k / nx), j = int(k % nx);
         const R a = R((j + 1 < nx) ? z[k + 1] - z[k] : edge);
         const R b = R((i >= 1) ? z[k - nx] - z[k] : edge);
-        const R c = R(rough[k] * rough[k]);
+        const R c = isnan(z[k]) ? R(__longlong_as_double(0x7ff8000000000000ll)) : R(rough[k] * rough[k]);
         stat[k] = typename Vec<R>::V4{a, b, c, make_meta<R>(meta[k])};
-        dzx[k] = a;
-        dzy[k] = b;
-        n2[k] = c;
+        if (dzx) {
+            dzx[k] = a;
+            dzy[k] = b;
+            n2[k] = c;
+        }
+    }
+}
+// the unfused entry points' structure-of-arrays copies of the static record
+template <typename R>
+__global__ void k_static_soa(size_t n, const typename Vec<R>::V4* stat, R* dzx, R* dzy, R* n2) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const auto v = stat[k];
+        dzx[k] = v.x;
+        dzy[k] = v.y;
+        n2[k] = v.z;
     }
 }
 // state record {h, q_x, q_y, dmax = -inf} from depths.d_t [mm] and outflow_bates pages 1-2
@@ -907,6 +1050,21 @@ __global__ void k_state_component(size_t n, const typename Vec<R>::V4* st, int c
     }
 }
 
+// read-back into FP64: one component of the state records (0..3 = h, q_x, q_y, dmax) or a plain
+// array, times `scale` (the conversion to the caller's units happens on the device)
+template <typename R>
+__global__ void k_state_component_f64(size_t n, const typename Vec<R>::V4* st, int comp, double scale, double* out) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const auto v = st[k];
+        const R x = comp == 0 ? v.x : comp == 1 ? v.y : comp == 2 ? v.z : v.w;
+        out[k] = double(x) * scale;
+    }
+}
+template <typename R> __global__ void k_scaled_f64(size_t n, const R* src, double scale, double* out) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
+        out[k] = double(src[k]) * scale;
+}
+
 // a map record taken by the host when no step follows the one that triggered it
 template <typename R> __global__ void k_record_depth(size_t n, const typename Vec<R>::V4* st, R* dst) {
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x)
@@ -919,6 +1077,47 @@ template <typename R> __global__ void k_inflow_depth(InflowDesc<R> d, const Step
     for (int g = threadIdx.x; g < d.n_gauges; g += blockDim.x)
         d.depth[g] = R(inflow_integral(d, g, ra, rb) / 60000.0);
     for (int g = threadIdx.x; g < d.n_stage; g += blockDim.x) d.stage_now[g] = R(stage_at(d, g, t));
+}
+
+// Retry of a rejected step (HydroPol2D_Main_While.m:928-951): the reference's new step needs
+// the wave celerity sqrt(g max(max(d_tot), max(d_p))) of the attempt.  Over the state the
+// attempt started from (buffer cur, untouched by it) this restates phase (A) per cell -- rain,
+// infiltration, inflow and clamps give d_tot -- and reduces max(d_p, d_tot) (NaN skipped, as
+// MATLAB's max) into sc->retry_dmax.  It also takes back the arrival times the attempt wrote:
+// a cell whose arrival equals the attempt's t_arr and whose start-of-step maximum is below the
+// threshold was marked by it.  inf: 0 none, 1 Green-Ampt, 2 van Genuchten.
+template <typename R>
+__global__ void k_retry_scan(const FusedArgs<R> a, int inf, R t_arr_rejected) {
+    StepScalars* sc = a.sc;
+    RainStep<R> RS;
+    RS.make(a.rain, sc->rain_a, sc->rain_b);
+    StepConsts<R> K;
+    K.make(sc->time_step * 60.0, a.res, a.tol_mm, a.thr_mm);
+    const bool skip = sc->skip_clamp != 0;
+    const typename Vec<R>::V4* st = sc->cur ? a.st1 : a.st0;
+    const typename Vec<R>::V2* gs = sc->cur ? a.gs1 : a.gs0;
+    const size_t n = size_t(a.ny) * a.nx;
+    R m = R(0);
+    for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
+        const int r = int(c / a.nx), j = int(c % a.nx);
+        const auto rec = st[c];
+        R hh = rec.x;
+        m = fmax(m, hh);
+        hh = hh + RS.at(a.rain, r, j, a.ny, a.nx);
+        const unsigned meta = meta_bits(a.stat[c].w);
+        if (inf && (meta & 255u) != 255u) {
+            R Ic = gs[c].x, Tc = gs[c].y;
+            if (inf == 1) green_ampt(hh, Ic, Tc, a.classes[meta & 255u], K);
+            else vg_infiltration(hh, Ic, Tc, a.classes_vg[meta & 255u], a.vg, K);
+        }
+        if (a.inflow.n_gauges) add_inflow(a.inflow, meta, hh);
+        if (!skip && hh < R(1e-9)) hh = R(0);
+        if (hh < R(0)) hh = R(0);
+        m = fmax(m, hh);
+        if (a.arrival[c] == t_arr_rejected && rec.w < K.thr) a.arrival[c] = R(__int_as_float(0x7f800000));
+    }
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0 && m > R(0)) atomicMax(&sc->retry_dmax, ord_bits(m));
 }
 
 // the structure transfers of the first fused step of a call (one block)
@@ -941,9 +1140,9 @@ __global__ void k_struct_prime(const FusedArgs<R> a) {
                                          threadIdx.x, blockDim.x, s_ts);
 }
 
-template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>
+template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false, int SCH = 0>
 __global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb) k_fused_step(const FusedArgs<R> a) {
-    fused_item<R, NT, INF, MAP, CPL, INFL>(a, blockIdx.x);
+    fused_item<R, NT, INF, MAP, CPL, INFL, SCH>(a, blockIdx.x);
 }
 
 // ---- batched ensemble ----------------------------------------------------------------
@@ -973,8 +1172,8 @@ __global__ void k_ens_plan(const FusedArgs<R>* __restrict__ members, int n_membe
         if (m < n_members) {
             const FusedArgs<R>& a = members[m];
             const StepScalars* sc = a.sc;
-            const bool stalled = (sc->status & 2u) != 0u;
-            const bool running = sc->t_min <= a.t_end && !stalled;
+            const bool stalled = (sc->status & kStatusTimeout) != 0u;
+            const bool running = sc->t_min <= a.t_end && !stalled && !sc->halted;
             items = running ? a.n_ctas : 0u;
             if (running) atomicAdd(&s_act, 1u);
             if (stalled) atomicAdd(&s_stall, 1u);
@@ -1002,7 +1201,7 @@ __global__ void k_ens_plan(const FusedArgs<R>* __restrict__ members, int n_membe
     }
 }
 
-template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false>
+template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false, int SCH = 0>
 __global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb)
 k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsigned* __restrict__ prefix,
            EnsQueue* q) {
@@ -1036,12 +1235,14 @@ k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsign
             for (int w = tid; w < int(sizeof(FusedArgs<R>) / 4); w += NT) dst[w] = src[w];
         }
         __syncthreads();
-        if (!fused_item<R, NT, INF, MAP, CPL, INFL>(s_a, s_local)) return;   // ring unusable after a timeout
+        if (!fused_item<R, NT, INF, MAP, CPL, INFL, SCH>(s_a, s_local)) return;   // ring unusable after a timeout
     }
 }
 
 // Clamp-skip flag for the first fused step of a call, over every cell (the state may
-// have been set from the host).  sc->skip_clamp must be zero on entry.
+// have been set from the host).  sc->skip_clamp must be zero on entry.  Also counts the cells
+// with a finite depth (n_finite) and with a non-finite one (n_bad0, the count a healthy step
+// keeps), and flags a non-finite depth in a cell of finite elevation (bad_domain).
 template <typename R>
 __global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>::V4* stat, int ny, int nx,
                             RainDesc rain, int ga, double res, double tol_mm, double thr_mm, StepScalars* sc) {
@@ -1052,8 +1253,13 @@ __global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>
     unsigned long long fin = 0;
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
         const R hc = st[c].x;
+        const auto sr = stat[c];
         if (isfinite(hc)) ++fin;
-        if (ga && (meta_bits(stat[c].w) & 255u) != 255u) continue;
+        else {
+            atomicAdd(&sc->n_bad0, 1ull);
+            if (!isnan(sr.z)) atomicOr(&sc->bad_domain, 1);
+        }
+        if (ga && (meta_bits(sr.w) & 255u) != 255u) continue;
         const int i = int(c / nx), j = int(c % nx);
         if (hc + RS.at(rain, i, j, ny, nx) < R(-1e-11)) neg = 1;
     }

@@ -3,10 +3,10 @@
 //
 // Who needs it: callers that may not allocate GPU memory while they run -- a MEX gateway
 // living inside MATLAB, whose GPU memory pool owns the device and is the only allocator
-// allowed to grow; code running between cudaStreamBeginCapture and EndCapture, where
-// cudaMalloc is not a capturable operation; real-time drivers that forbid allocation
-// after start-up.  They already hold the face fluxes and face depths on the device and
-// only want the next time step.
+// allowed to grow; real-time drivers that forbid allocation after start-up.  They already
+// hold the face fluxes and face depths on the device and only want the next time step.
+// The call ends by copying the two maxima into host memory and synchronising the caller's
+// stream.
 //
 // The reduction scratch (one partial maximum per block of 16 rows, plus the two final
 // maxima) is the file-scope array g_noalloc_scratch below: 64 KB that every GPU which

@@ -68,10 +68,12 @@ __global__ void k_hydro_clamp(size_t n, R* h, const StepScalars* sc) {
     }
 }
 
-// unlimited faces (LIM_D4.m:31-294); face (i,j): x = right face of cell (i,j), y = upper face
+// unlimited faces (LIM_D4.m:31-294); face (i,j): x = right face of cell (i,j), y = upper face.
+// scheme = flag_numerical_scheme (Inertial_Solver.m): 1 Bates, 2 s-upwind, 3 s-centred; the
+// neighbouring previous fluxes of schemes 2/3 exist on interior columns (x) / rows (y) only.
 template <typename R>
 __global__ void k_faces(GridView<R> g, double dt_s, const R* h, const R* dzx, const R* dzy, const R* n2,
-                        const R* qx, const R* qy, R* hfx, R* hfy, R* qxu, R* qyu, int flag_critical) {
+                        const R* qx, const R* qy, R* hfx, R* hfy, R* qxu, R* qyu, int flag_critical, int scheme) {
     StepConsts<R> K;
     K.make(dt_s, g.res, g.tol_mm, g.thr_mm);
     const size_t n = size_t(g.ny) * g.nx;
@@ -79,11 +81,23 @@ __global__ void k_faces(GridView<R> g, double dt_s, const R* h, const R* dzx, co
         const int i = int(c / g.nx), j = int(c % g.nx);
         R Hf, q;
         const R hR = (j + 1 < g.nx) ? h[c + 1] : R(0);
-        face_flux<R, true>(h[c], hR, dzx[c], qx[c], n2[c], K, flag_critical, Hf, q);
+        if (scheme == 1) {
+            face_flux<R, true>(h[c], hR, dzx[c], qx[c], n2[c], K, flag_critical, Hf, q);
+        } else {
+            const bool in = j >= 1 && j + 1 < g.nx;
+            face_flux<R, true, 1>(h[c], hR, dzx[c], qx[c], n2[c], K, flag_critical, Hf, q, scheme,
+                                  in ? qx[c - 1] : R(0), in ? qx[c + 1] : R(0));
+        }
         hfx[c] = Hf;
         qxu[c] = q;
         const R hU = (i >= 1) ? h[c - g.nx] : R(0);
-        face_flux<R, false>(hU, h[c], dzy[c], qy[c], n2[c], K, flag_critical, Hf, q);
+        if (scheme == 1) {
+            face_flux<R, false>(hU, h[c], dzy[c], qy[c], n2[c], K, flag_critical, Hf, q);
+        } else {
+            const bool in = i >= 1 && i + 1 < g.ny;
+            face_flux<R, false, 1>(hU, h[c], dzy[c], qy[c], n2[c], K, flag_critical, Hf, q, scheme,
+                                   in ? qy[c - g.nx] : R(0), in ? qy[c + g.nx] : R(0));
+        }
         hfy[c] = Hf;
         qyu[c] = q;
     }

@@ -6,8 +6,8 @@ MATLAB's layout is kept at this edge: grids are (ny, nx) arrays, page arrays suc
 the reference's (depth mm, flux mm/h, time step min, elevation m).  Every call runs on the
 GPU through ``libhp2d.so``; there is no CPU path, so a missing library or device raises.
 
-* ``Local_Inertial_Model_D4`` -- Local_Inertial_Model_D4.m:1-5, non-subgrid branch, scheme 1
-  (Inertial_Solver.m:19-26).  Stateless: each call uploads z, roughness and the outlets to a
+* ``Local_Inertial_Model_D4`` -- Local_Inertial_Model_D4.m:1-5, non-subgrid branch, schemes 1-3
+  (Inertial_Solver.m:19-121).  Stateless: each call uploads z, roughness and the outlets to a
   cached context of the grid's shape, sets d_tot and outflow, runs ``hp2d_li_step`` and reads
   the outputs back.
 * ``refreshing_timestep`` -- the refresh branch of the refreshing_timestep.m script
@@ -17,8 +17,9 @@ GPU through ``libhp2d.so``; there is no CPU path, so a missing library or device
   caller's workspace between steps; here that workspace is a resident ``SurfaceFlow``
   context, whose ``hydrology_step`` is the script's drop-in.
 
-Flags the build does not implement (``flag_subgrid``, ``flag_reservoir``, schemes 2/3) raise
-``HP2DError`` with ``HP2D_UNSUPPORTED_FLAG``, as the C ABI does.
+Flags the build does not implement (``flag_subgrid = 1``, ``flag_reservoir`` other than 0/1,
+``flag_numerical_scheme`` outside 1-3) raise ``HP2DError`` with ``HP2D_UNSUPPORTED_FLAG``, as the
+C ABI does.
 """
 from __future__ import annotations
 
@@ -77,15 +78,16 @@ def Local_Inertial_Model_D4(flag_numerical_scheme, reservoir_x, reservoir_y, k1,
     cell) drive the control-structure transfers (Local_Inertial_Model_D4.m:318-344).
     Arguments the non-subgrid branch never reads (d_p,
     outlet_index, d_tolerance, idx_nan, the subgrid inputs) are accepted and ignored, as in
-    the reference (idx_nan only enters Inertial_Solver's schemes 2/3).  ``roughness_squared``
+    the reference (idx_nan is an unused argument of Inertial_Solver, in every scheme).  ``roughness_squared``
     must equal ``roughness_cell.^2`` and ``cell_area`` must be ``Resolution^2``: the library
     derives both from ``roughness_cell`` and ``Resolution``.  ``slope_outlet`` is a scalar or
     an (ny, nx) map sampled at the outlets (outlet_type 1).  ``precision`` selects the FP64
     (default, the reference's) or FP32 build.
     """
-    if int(flag_subgrid) != 0 or int(flag_reservoir) not in (0, 1) or int(flag_numerical_scheme) != 1:
+    if int(flag_subgrid) != 0 or int(flag_reservoir) not in (0, 1) or int(flag_numerical_scheme) not in (1, 2, 3):
         # the C ABI rejects these; raise the same error before touching the device
-        raise _abi.HP2DError(2, "flag_subgrid = 1 and schemes 2/3 are not implemented by this build")
+        raise _abi.HP2DError(2, "flag_subgrid = 1, flag_reservoir outside 0/1 and schemes other than 1-3 "
+                                "are not implemented by this build")
     z = np.asarray(z, dtype=np.float64)
     if z.ndim != 2:
         raise ValueError("z must be an (ny, nx) array")
@@ -108,8 +110,9 @@ def Local_Inertial_Model_D4(flag_numerical_scheme, reservoir_x, reservoir_y, k1,
     else:
         per_outlet = np.broadcast_to(s, (ny, nx))[rows, cols]
     params = _abi.default_params(outlet_type=int(outlet_type), slope_outlet=scalar_slope,
-                                 flag_critical=int(flag_critical), flag_reservoir=int(flag_reservoir))
-    pkey = (int(outlet_type), scalar_slope, int(flag_critical), int(flag_reservoir))
+                                 flag_critical=int(flag_critical), flag_reservoir=int(flag_reservoir),
+                                 flag_numerical_scheme=int(flag_numerical_scheme))
+    pkey = (int(outlet_type), scalar_slope, int(flag_critical), int(flag_reservoir), int(flag_numerical_scheme))
     g = _session(ny, nx, res, precision, pkey, params)
     g.upload_static(z, n, rows, cols, per_outlet)
     if int(flag_reservoir) == 1:   # 1-based (x = column, y = row); NaN: no downstream cell

@@ -258,9 +258,32 @@ class SurfaceFlow:
         self._check(self._L.hp2d_run(self._h, int(max_steps), C.byref(done)))
         return done.value
 
+    def set_retry_policy(self, max_retries: int = 8, factor_reduction: float = 2.0,
+                         dt_floor_is_error: bool = False):
+        """Retries of a rejected step (HydroPol2D_Main_While.m:926-993) and whether a step whose
+        refreshed dt hits min_time_step ends the call with HP2D_DT_FLOOR."""
+        self._check(self._L.hp2d_set_retry_policy(self._h, int(max_retries), float(factor_reduction),
+                                                  int(bool(dt_floor_is_error))))
+
+    def set_wait_limit(self, polls: int):
+        """Polls of a row-copy wait before the step gives up with HP2D_TIMEOUT (default 4194304)."""
+        self._check(self._L.hp2d_set_wait_limit(self._h, int(polls)))
+
+    def inject_step_fault(self, k: int, attempts: int = 1):
+        """Test hook: the next ``attempts`` attempts of step ``k`` are rejected."""
+        self._check(self._L.hp2d_inject_step_fault(self._h, int(k), int(attempts)))
+
     # ---------------------------------------------------------------- outputs
     def download(self, field: str) -> np.ndarray:
         out = np.empty((self.ny, self.nx), dtype=np.float64)
+        self._check(self._L.hp2d_download(self._h, _abi.FIELD[field], _dp(out), out.size))
+        return out
+
+    def download_into(self, field: str, out: np.ndarray) -> np.ndarray:
+        """``download`` into a caller-owned C-contiguous float64 (ny, nx) array (for instance one
+        in page-locked memory)."""
+        if out.dtype != np.float64 or out.shape != (self.ny, self.nx) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 (ny, nx) array")
         self._check(self._L.hp2d_download(self._h, _abi.FIELD[field], _dp(out), out.size))
         return out
 

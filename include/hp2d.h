@@ -39,9 +39,12 @@ typedef enum hp2d_status {
     HP2D_INVALID_ARG = 1,
     HP2D_UNSUPPORTED_FLAG = 2,   /* flag_subgrid/flag_D8=1, scheme 2/3 ... */
     HP2D_CUDA_ERROR = 3,
-    HP2D_NUMERICAL = 4,          /* NaN/Inf in the state */
-    HP2D_DT_FLOOR = 5,           /* dt hit min_time_step (refreshing_timestep.m:357-359) */
-    HP2D_TIMEOUT = 6,
+    HP2D_NUMERICAL = 4,          /* a step kept failing (non-finite or negative depth), or the state
+                                    holds a NaN depth in a cell of finite elevation */
+    HP2D_DT_FLOOR = 5,           /* dt hit min_time_step (refreshing_timestep.m:357-359), with
+                                    hp2d_set_retry_policy's dt_floor_is_error = 1 */
+    HP2D_TIMEOUT = 6,            /* a row copy into shared memory did not land within the wait
+                                    limit (hp2d_set_wait_limit); that step was rejected */
     HP2D_NO_DEVICE = 7,
     HP2D_NOT_READY = 8           /* static data or state not uploaded yet */
 } hp2d_status;
@@ -108,7 +111,8 @@ typedef struct hp2d_diag {
     double outlet_volume;         /* cumulative [m^3] */
     int64_t neg_depth_warnings;   /* Hydrological_Model.m:45-47 events */
     int64_t unstable_steps;       /* refreshing_timestep.m:357-359 events */
-    int64_t status_bits;          /* bit 0: non-finite state seen */
+    int64_t status_bits;          /* bit 0: a step was rejected for its depths; bit 1: a row copy
+                                     timed out; bit 2: the refreshed dt hit min_time_step */
     double rain_t0, rain_t1;      /* clock interval whose rain the next step applies [min] */
     double t_previous;            /* the loop's t_previous [min] */
     double inflow_volume;         /* cumulative inflow-hydrograph volume [m^3] */
@@ -118,6 +122,10 @@ typedef struct hp2d_diag {
                                      written (dry rows) and did not store again */
     int64_t skipped_read_cells;   /* of those, cells of whole dry row blocks whose records
                                      were not read either */
+    int64_t retries;              /* rejected step attempts retried so far */
+    int32_t catch_index;          /* the reference's catch_index (1 + failures so far) */
+    int32_t pad;
+    double max_time_step;         /* running_control.max_time_step [s], lowered by retries */
 } hp2d_diag;
 
 typedef struct hp2d_ctx hp2d_ctx;
@@ -313,6 +321,32 @@ hp2d_status hp2d_autotune(hp2d_ctx* ctx, int32_t trial_steps, int32_t* rows_per_
 /* Runs until the clock passes routing_time (or max_steps); returns steps executed. */
 hp2d_status hp2d_run(hp2d_ctx* ctx, int64_t max_steps, int64_t* steps_done);
 
+/* Failure handling of the fused path, the try/catch of HydroPol2D_Main_While.m:926-993.  A fused
+ * step is rejected when a cell of finite elevation ends it with a non-finite depth or one below
+ * -depth_tolerance, or when one of its row copies timed out.  A rejected step commits nothing:
+ * depths, fluxes, soil storage and maxima stay those the step started from (d_t = d_p,
+ * I_t = I_p), and so do the clock, counters and volumes.  A step rejected for its depths is
+ * retried as the reference's catch block does: the clock goes back by the step, catch_index
+ * grows, the new step is alfa_min*dx/sqrt(g*max(d_tot, d_p)) / catch_index / factor_reduction
+ * (the last refresh's maximum velocity joins the celerity when flag_adaptive_timestepping = 0),
+ * max_time_step drops to 1.5 x that step, and the rain interval is recomputed.  After
+ * max_retries rejections of one step the call returns HP2D_NUMERICAL with the last accepted
+ * state (defaults: 8 retries, factor_reduction 2 as input_data_script.m:486).  A timed-out step
+ * is not retried: the call returns HP2D_TIMEOUT with the last accepted state.  With
+ * dt_floor_is_error = 1 a step whose refreshed dt equals min_time_step (refreshing_timestep's
+ * `unstable`, counted in hp2d_diag.unstable_steps either way) is kept and the call returns
+ * HP2D_DT_FLOOR after it.  The velocity and hazard maxima keep what a rejected attempt added. */
+hp2d_status hp2d_set_retry_policy(hp2d_ctx* ctx, int32_t max_retries, double factor_reduction,
+                                  int32_t dt_floor_is_error);
+/* Polls of one row-copy wait of the fused step before it gives up (default 4194304).  A copy
+ * that has not landed then makes the step a rejected one and the call return HP2D_TIMEOUT;
+ * copies still in flight are always waited for with the default limit before a block exits.
+ * 0 makes every wait give up at once (a test of the timeout path). */
+hp2d_status hp2d_set_wait_limit(hp2d_ctx* ctx, int64_t polls);
+/* Test hook (no counterpart in the reference): the next `attempts` attempts of step k are
+ * rejected as if a depth had gone non-finite, so that the retry path runs on demand. */
+hp2d_status hp2d_inject_step_fault(hp2d_ctx* ctx, int64_t k, int32_t attempts);
+
 /* ---- outputs ---------------------------------------------------------------------- */
 hp2d_status hp2d_download(hp2d_ctx* ctx, int32_t field, double* host, size_t count);
 /* Raw copy of an internal array in the context's precision and SI units, for callers
@@ -358,8 +392,8 @@ hp2d_status hp2d_ensemble_run(hp2d_ensemble* ens, int64_t max_steps, int64_t* st
 /* ---- allocation-free timestep (no counterpart in the reference) -------------------- */
 /* refreshing_timestep's refresh branch (as hp2d_cfl_dt) on caller-owned FP32 device
  * arrays, for callers that may not allocate GPU memory while they run: a MEX gateway
- * inside MATLAB whose GPU memory pool owns the device, code inside a CUDA stream capture,
- * real-time drivers that allocate only at start-up.  Nothing is allocated: the reduction
+ * inside MATLAB whose GPU memory pool owns the device, real-time drivers that allocate
+ * only at start-up.  Nothing is allocated: the reduction
  * scratch is a fixed 64 KB array inside the library, resident on every GPU that loads it
  * until the process exits, which limits grids to ny <= 65536 rows (larger grids are
  * rejected with HP2D_INVALID_ARG).  The first call on each device (with that device
@@ -367,7 +401,8 @@ hp2d_status hp2d_ensemble_run(hp2d_ensemble* ens, int64_t max_steps, int64_t* st
  * capture.  Calls that overlap on the GPU share the scratch and race.
  *   q_x, q_y   ny*nx limited face discharge per unit width [m^2/s] (native fields 1, 2)
  *   hf         3*ny*nx face flow depth [m]: pages x, y and outlet, as Hf(:,:,1:3)
- *   stream     cudaStream_t to run on (NULL = default stream); the call synchronises it
+ *   stream     cudaStream_t to run on (NULL = default stream); the call ends by copying
+ *              the two maxima to host memory and synchronising this stream
  *   time_step  [out] new time step [min]; max_velocity [out, nullable] [m/s]
  * On failure hp2d_noalloc_error() gives the message. */
 hp2d_status hp2d_cfl_dt_noalloc(int32_t ny, int32_t nx, double resolution, const hp2d_params* params,

@@ -83,6 +83,8 @@ def _load():
             "oracle_run": ([vp, C.c_int64, P(C.c_int64)], C.c_int),
             "oracle_download_native": ([vp, C.c_int32, vp, C.c_size_t], C.c_int),
             "oracle_get_diag": ([vp, P(_abi.Diag)], C.c_int),
+            "oracle_set_retry_policy": ([vp, C.c_int32, C.c_double, C.c_int32], C.c_int),
+            "oracle_inject_step_fault": ([vp, C.c_int64, C.c_int32], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -228,12 +230,20 @@ class KernelFormOracle:
         self._L.oracle_track_maxima(self._h, float(t_end))
 
     def fused_steps(self, n):
-        self._L.oracle_steps(self._h, int(n))
+        """n accepted steps; returns the hp2d_status code (0, or HP2D_NUMERICAL / HP2D_DT_FLOOR)."""
+        return self._L.oracle_steps(self._h, int(n))
 
     def run(self, max_steps=0):
         done = C.c_int64()
         self._L.oracle_run(self._h, int(max_steps), C.byref(done))
         return done.value
+
+    def set_retry_policy(self, max_retries=8, factor_reduction=2.0, dt_floor_is_error=False):
+        self._L.oracle_set_retry_policy(self._h, int(max_retries), float(factor_reduction),
+                                        int(bool(dt_floor_is_error)))
+
+    def inject_step_fault(self, k, attempts=1):
+        self._L.oracle_inject_step_fault(self._h, int(k), int(attempts))
 
     def download_native(self, field):
         per_outlet = field in ("hf3", "qo")

@@ -198,8 +198,11 @@ public:
 
     size_t at(int i, int j) const { return size_t(i) * nx + j; }
 
+    std::vector<uint8_t> wall;   // NaN elevation (idx_nan): may hold a NaN depth
     void upload_static(const double* z, const double* n, const int32_t* rows, const int32_t* cols,
                        int nout, const double* slopes) {
+        wall.assign(size_t(ny) * nx, 0);
+        for (size_t c = 0; c < wall.size(); ++c) wall[c] = std::isnan(z[c]) ? 1 : 0;
         // domain-edge faces +inf, faces next to a NaN elevation NaN (see face())
         const double edge = std::numeric_limits<double>::infinity();
         for (int i = 0; i < ny; ++i)
@@ -572,7 +575,11 @@ public:
     // ---------------- Local_Inertial_Model_D4 ----------------
     // one face: returns (Hf, q) from neighbour depths; for x faces (a, b) = (L, R);
     // for y faces (a, b) = (U, D) and dz = z_U - z_D, so the roles of max/min swap.
-    inline void face(R ha, R hb, R dz, R qp, R n2c, bool is_x, const Consts<R>& K, R& Hf, R& q) const {
+    // q_lo / q_hi: previous fluxes of the same direction one face before / after, used by
+    // flag_numerical_scheme 2 (s-upwind) and 3 (s-centred), Inertial_Solver.m:29-121 (zero
+    // outside the interior columns / rows)
+    inline void face(R ha, R hb, R dz, R qp, R n2c, bool is_x, const Consts<R>& K, R& Hf, R& q, R q_lo = R(0),
+                     R q_hi = R(0)) const {
         // non-finite dz: +inf on the domain edge (Hf = 0, Local_Inertial_Model_D4.m:139-140),
         // NaN next to an idx_nan cell: MATLAB's max skips the NaN, so Hf is the inside
         // cell's depth (:133-134) and the NaN slope sends q to 0 (:264)
@@ -592,7 +599,15 @@ public:
             S = (dz + (ha - hb)) * K.inv_dx;
         }
         if (!(Hf > R(0))) { q = R(0); return; }
-        R num = std::fma(-(K.gdt * Hf), S, qp);
+        R qn = qp;
+        if (p.flag_numerical_scheme != 1) {
+            // theta = 1 - dt/dx min(|q_p|/Hf, sqrt(g Hf)); the momentum term mixes q_p with the
+            // upwind (scheme 2) or centred (scheme 3) neighbour flux
+            const R th = R(1) - K.dt_over_dx * std::fmin(qdiv(std::fabs(qp), Hf), std::sqrt(K.g * Hf));
+            const R qnb = p.flag_numerical_scheme == 2 ? (qp < R(0) ? q_hi : q_lo) : R(0.5) * (q_lo + q_hi);
+            qn = th * qp + (R(1) - th) * qnb;
+        }
+        R num = std::fma(-(K.gdt * Hf), S, qn);
         R h73 = pow73(Hf);
         R den = std::fma(K.gdt * n2c, std::fabs(qp), h73);
         q = qdiv(num * h73, den);
@@ -614,10 +629,12 @@ public:
                 size_t c = at(i, j);
                 R Hf, q;
                 R hR = (j + 1 < nx) ? h[at(i, j + 1)] : R(0);
-                face(h[c], hR, dzx[c], qx[c], n2[c], true, K, Hf, q);
+                const bool inx = j >= 1 && j + 1 < nx, iny = i >= 1 && i + 1 < ny;
+                face(h[c], hR, dzx[c], qx[c], n2[c], true, K, Hf, q, inx ? qx[c - 1] : R(0), inx ? qx[c + 1] : R(0));
                 hfx[c] = Hf; qx_unl[c] = q;
                 R hU = (i >= 1) ? h[at(i - 1, j)] : R(0);
-                face(hU, h[c], dzy[c], qy[c], n2[c], false, K, Hf, q);
+                face(hU, h[c], dzy[c], qy[c], n2[c], false, K, Hf, q, iny ? qy[at(i - 1, j)] : R(0),
+                     iny ? qy[at(i + 1, j)] : R(0));
                 hfy[c] = Hf; qy_unl[c] = q;
             }
         // donor scale
@@ -776,16 +793,16 @@ public:
         if (vmax > 0) {
             dt_adv = 1.0 * res / std::max(vmax, 1e-10);
             double tsf = std::max(p.alfa_max - 2.0 * std::max(vmax - 5.0, 0.0), p.alfa_min);
-            dt_adv = std::min(dt_adv * tsf, p.max_time_step);
+            dt_adv = std::min(dt_adv * tsf, max_dt());
         } else {
-            dt_adv = p.max_time_step;
+            dt_adv = max_dt();
         }
-        double dt_wave = cmax > 0 ? (p.alfa_min * res) / cmax : p.max_time_step;
+        double dt_wave = cmax > 0 ? (p.alfa_min * res) / cmax : max_dt();
         double nw = p.flag_timestep == 1 ? std::min(dt_adv, dt_wave) : dt_wave;
-        if (std::isnan(nw) || std::isinf(nw)) nw = p.max_time_step;
+        if (std::isnan(nw) || std::isinf(nw)) nw = max_dt();
         double tcr = std::max(p.time_step_increments * std::floor(nw / p.time_step_increments),
                               p.min_time_step);
-        return std::min(tcr, p.max_time_step);
+        return std::min(tcr, max_dt());
     }
 
     void track(double t_end_s) {
@@ -818,27 +835,103 @@ public:
         return idx;
     }
 
+    // ---------------- failure handling (HydroPol2D_Main_While.m:926-993) ----------------
+    // A step is rejected when more cells end it with a depth that is non-finite or below
+    // -depth_tolerance than had a non-finite depth when the call began (idx_nan walls), or when
+    // the test hook asks for it.  The rejected attempt is undone (d_t = d_p, I_t = I_p, and the
+    // clock, counters and volumes it touched) and retried as the catch block does: clock back
+    // by the step, catch_index + 1, new step factor * alfa_min * dx / celerity with
+    // factor = 1/catch_index/factor_reduction and celerity sqrt(g max(max(d_tot), max(d_p)))
+    // (+ the last refresh's maximum velocity when flag_adaptive_timestepping = 0), max_time_step
+    // lowered to 1.5 x the new step, the new step capped by it (infinite -> min_time_step), the
+    // rain interval [rewound clock, new clock].  The velocity and hazard maxima keep the
+    // attempt's contribution (as the library's in-place maps do).
+    int64_t fault_k = -1;
+    int fault_n = 0;
+    int catch_index = 1;
+    double max_dt_eff = -1.0;       // running_control.max_time_step as lowered by retries [s]
+    int max_retries = 8;
+    double factor_reduction = 2.0;
+    int dt_floor_stop = 0;
+    int64_t retries = 0, rej_k = -1;
+    int rej_n = 0;
+    uint64_t n_bad0 = 0;
+    double max_dt() const { return max_dt_eff > 0 ? max_dt_eff : p.max_time_step; }
+    enum StepResult { kAccepted = 0, kRetried = 1, kDtFloor = 2, kFailed = 3 };
+
+    // cells whose depth is non-finite (counted at the start of a call) / bad after a step
+    uint64_t count_bad(bool after_step) const {
+        uint64_t nb = 0;
+        const R negtol = -R(p.depth_tolerance / 1000.0);
+        for (size_t c = 0; c < h.size(); ++c)
+            nb += after_step ? !(h[c] >= negtol) : !std::isfinite(double(h[c]));
+        return nb;
+    }
+    // a non-finite depth in a cell of finite elevation: the state is unusable
+    bool bad_domain() const {
+        for (size_t c = 0; c < h.size(); ++c)
+            if (!std::isfinite(double(h[c])) && !(c < wall.size() && wall[c])) return true;
+        return false;
+    }
+
     // ---------------- one accepted step (HydroPol2D_Main_While.m:403-782) ----------------
     // The step is carried in minutes, as the reference does (time_step, min), and the
     // seconds of the step are time_step*60 (Local_Inertial_Model_D4.m:201).
-    void step() {
+    int step() {
+        // what a rejected attempt restores
+        const std::vector<R> h0 = h, qx0 = qx, qy0 = qy, I0 = I, T0 = T, dmax0 = dmax, arr0 = arrival;
+        const double sv[] = {rain_vol, inf_vol, out_vol, inflow_vol, stage_vol, struct_vol, tsp, vmax_last};
+        const int64_t neg0 = neg_warn, uns0 = unstable;
+        const size_t nrec0 = rec_maps.size();
+        const int rec_last0 = rec_last;
         double dts = time_step * 60.0;
         hydrology(dts);
+        R dmx = R(0);   // max(d_p, d_tot), NaN skipped
+        for (size_t c = 0; c < h.size(); ++c) dmx = std::fmax(std::fmax(dmx, h0[c]), h[c]);
         li(dts, time_step);
         double pos_save = std::ceil((t_min * 60.0) / p.time_step_change);
         double time_save = (pos_save - 1.0) * p.time_step_change / 60.0;
         double delta = time_save - tsp;
         tsp = time_save;
         double tcr = time_step * 60.0;
+        bool floor_hit = false;
         if (delta > 0 || k == 1) {
             double vm;
             tcr = cfl(dts, &vm);
             vmax_last = vm;
-            if (tcr == p.min_time_step) ++unstable;
+            if (tcr == p.min_time_step) { ++unstable; floor_hit = true; }
         }
         apply_stage();
         track(t_min * 60.0 + dts);
         if (hz_on) track_hazard();
+        bool reject = count_bad(true) > n_bad0;
+        if (fault_n > 0 && k == fault_k) { --fault_n; reject = true; }
+        if (reject) {
+            h = h0; qx = qx0; qy = qy0; I = I0; T = T0; dmax = dmax0; arrival = arr0;
+            rain_vol = sv[0]; inf_vol = sv[1]; out_vol = sv[2]; inflow_vol = sv[3]; stage_vol = sv[4];
+            struct_vol = sv[5]; tsp = sv[6]; vmax_last = sv[7];
+            neg_warn = neg0; unstable = uns0;
+            rec_maps.resize(nrec0); rec_t.resize(nrec0); rec_last = rec_last0;
+            if (k == rej_k) ++rej_n;
+            else { rej_k = k; rej_n = 1; }
+            if (rej_n > max_retries) { rej_n = 0; return kFailed; }
+            const double wc = std::sqrt(kG * double(dmx));
+            ++catch_index;
+            const double factor = 1.0 / catch_index / factor_reduction;
+            double nt = p.flag_adaptive_timestepping == 1 ? factor * (p.alfa_min * res / wc)
+                                                          : factor * (p.alfa_min * res / (vmax_last + wc));
+            if (catch_index > 1) max_dt_eff = std::fmin(nt * 1.5, max_dt());
+            nt = std::fmin(nt, max_dt());
+            if (std::isinf(nt)) nt = p.min_time_step;
+            const double t0 = t_min - time_step;
+            t_prev = t0;
+            time_step = nt / 60.0;
+            t_min = t0 + time_step;
+            rain_a = t_prev;
+            rain_b = t_min;
+            ++retries;
+            return kRetried;
+        }
         if (!rec_times.empty()) {
             const int idx = last_below(t_min + tcr / 60.0);
             if (idx > rec_last) {
@@ -855,6 +948,7 @@ public:
         time_step = tcr / 60.0;
         t_min = tcr / 60.0 + t_min;
         ++k;
+        return floor_hit && dt_floor_stop ? kDtFloor : kAccepted;
     }
 
     bool finished() const { return !(t_min <= p.routing_time + p.min_time_step / 60.0); }

@@ -153,21 +153,51 @@ int oracle_track_maxima(oracle_model* m, double t_end) {
     return dispatch(m, [&](auto& M) { M.track(t_end * 60.0); return 0; });
 }
 
+}  // extern "C"
+
+// nsteps accepted steps (as hp2d_fused_steps): a rejected attempt is retried in place; the
+// call returns HP2D_NUMERICAL when one step's retries run out or the state holds a NaN depth
+// in a cell of finite elevation, HP2D_DT_FLOOR after a step that hit min_time_step with the
+// dt-floor stop on
+template <typename M_> static int accepted_steps(M_& M, int64_t nsteps, int64_t* done) {
+    if (M.bad_domain()) return int(HP2D_NUMERICAL);
+    M.n_bad0 = M.count_bad(false);
+    const int64_t k0 = M.k;
+    int st = 0;
+    while (M.k - k0 < nsteps && !M.finished()) {
+        const int r = M.step();
+        if (r == M_::kFailed) { st = int(HP2D_NUMERICAL); break; }
+        if (r == M_::kDtFloor) { st = int(HP2D_DT_FLOOR); break; }
+    }
+    if (done) *done = M.k - k0;
+    return st;
+}
+
+extern "C" {
+
 int oracle_steps(oracle_model* m, int32_t nsteps) {
-    return dispatch(m, [&](auto& M) {
-        for (int s = 0; s < nsteps; ++s) {
-            if (M.finished()) break;
-            M.step();
-        }
-        return 0;
-    });
+    return dispatch(m, [&](auto& M) { return accepted_steps(M, nsteps, nullptr); });
 }
 
 int oracle_run(oracle_model* m, int64_t max_steps, int64_t* done) {
     return dispatch(m, [&](auto& M) {
-        int64_t s = 0;
-        while (!M.finished() && (max_steps <= 0 || s < max_steps)) { M.step(); ++s; }
-        *done = s;
+        return accepted_steps(M, max_steps > 0 ? max_steps : (int64_t(1) << 40), done);
+    });
+}
+
+int oracle_set_retry_policy(oracle_model* m, int32_t max_retries, double factor_reduction, int32_t dt_floor_is_error) {
+    return dispatch(m, [&](auto& M) {
+        M.max_retries = max_retries;
+        M.factor_reduction = factor_reduction;
+        M.dt_floor_stop = dt_floor_is_error;
+        return 0;
+    });
+}
+
+int oracle_inject_step_fault(oracle_model* m, int64_t k, int32_t attempts) {
+    return dispatch(m, [&](auto& M) {
+        M.fault_k = k;
+        M.fault_n = attempts;
         return 0;
     });
 }
@@ -239,6 +269,9 @@ int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
         o->structure_volume = M.struct_vol;
         o->skipped_cells = 0;
         o->skipped_read_cells = 0;
+        o->retries = M.retries;
+        o->catch_index = M.catch_index;
+        o->max_time_step = M.max_dt();
         return 0;
     });
 }

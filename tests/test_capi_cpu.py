@@ -36,7 +36,7 @@ def _create(**kw):
 
 
 @pytest.mark.parametrize("flag,value", [("flag_subgrid", 1), ("flag_D8", 1),
-                                        ("flag_numerical_scheme", 2), ("flag_numerical_scheme", 3),
+                                        ("flag_numerical_scheme", 0), ("flag_numerical_scheme", 4),
                                         ("flag_infiltration", 3)])
 def test_unsupported_flags_rejected(hp2d_lib, flag, value):
     st, msg, h = _create(**{flag: value})

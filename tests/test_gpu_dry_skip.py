@@ -103,3 +103,34 @@ def test_dense_switch_gives_the_same_bits(hp2d_lib):
     for f in FIELDS:
         assert same_bits(a.download_native(f), b.download_native(f)), f
     assert b.diag()["skipped_cells"] > 0
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_row_wet_for_one_step_between_deep_dry_steps(precision, hp2d_lib, oracle_lib):
+    """Rain on every other one-second step, a little faster than the soil takes it: every row gets
+    a thin film in the rainy steps and is dry again (all of it soaked up) in the next, so a row
+    is deep-dry at steps s-2 and s and wet at s-1.  The record a deep-dry step would write then
+    differs from the one written at s-2 (the running maximum moved at s-1): it must be written."""
+    n = 72
+    z = 0.05 * S.gaussian_random_field(n, n, -3.0, 2)
+    steps = 40
+    t_start = np.arange(steps + 2) / 60.0           # [min], one interval per one-second step
+    rate = np.where(np.arange(steps + 2) % 2 == 0, 40.0, 0.0)
+    tabs = S.green_ampt_soil_tables([30.0], [50.0], [0.3])
+    params = dict(routing_time=30.0, alfa_min=0.5, alfa_max=0.7, outlet_type=1, slope_outlet=0.01,
+                  min_time_step=1.0, max_time_step=1.0, flag_infiltration=1)
+    case = S.Case("film", z, np.full((n, n), 0.03), 5.0, np.zeros(0, np.int32), np.zeros(0, np.int32), params,
+                  np.zeros((n, n)), rain_uniform=(t_start, rate),
+                  soil=dict(soil_class=np.zeros((n, n), np.uint8), **tabs), I0=np.full((n, n), 500.0))
+    g, o = make_pair(case, precision)
+    seen_wet = seen_dry = 0
+    for _ in range(steps):
+        g.fused_steps(1)
+        o.fused_steps(1)
+        h = g.download_native("h")
+        seen_wet += int((h > 0).all())
+        seen_dry += int((h == 0).all())
+    assert seen_wet >= 5 and seen_dry >= 5   # the rows did alternate
+    assert_same_state(g, o, FIELDS + ["I", "T"])
+    assert_same_clock(g, o)
+    assert g.download_native("dmax").max() > 0

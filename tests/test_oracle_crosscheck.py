@@ -173,3 +173,96 @@ def test_qdiv_within_one_ulp(oracle_lib):
     err = np.abs(q[fin].astype(np.float64) - exact[fin]) / ulp
     assert err.max() <= 1.0, err.max()
     assert q[0] == 0.0 and q[1] == 0.0   # a zero numerator gives a zero (its sign is not kept)
+
+
+def _prior_state(case, seed, scale_mmh):
+    rng = np.random.default_rng(seed)
+    ny, nx = case.shape
+    outflow = np.zeros((3, ny, nx))
+    outflow[0] = rng.normal(0, scale_mmh, (ny, nx))
+    outflow[1] = rng.normal(0, scale_mmh, (ny, nx))
+    outflow[0][:, -1] = 0
+    outflow[1][0, :] = 0
+    d = np.where(rng.random((ny, nx)) < 0.7, rng.uniform(0, 500, (ny, nx)), 0.0)
+    d[np.isnan(case.z)] = np.nan
+    return d, outflow
+
+
+@pytest.mark.parametrize("scheme", [2, 3])
+@pytest.mark.parametrize("seed,walls", [(6, False), (7, True)])
+def test_li_step_schemes_2_3_agree(oracle_lib, scheme, seed, walls):
+    """Inertial_Solver's s-upwind (2) and s-centred (3) schemes (Inertial_Solver.m:29-121) in the
+    kernel form against the literal restatement: one Local_Inertial_Model_D4 call on a random
+    wet state with random prior fluxes, which the schemes mix with their neighbours'."""
+    case = random_terrain(23, 37, seed=seed, walls=walls)
+    d, outflow = _prior_state(case, seed, 2e4)
+    ts = 0.5 / 60
+    lit = L.local_inertial_model_d4(case.z, d, case.roughness, case.roughness ** 2, case.resolution ** 2, ts,
+                                    case.resolution, case.outlet_rows, case.outlet_cols, 1,
+                                    case.params["slope_outlet"], outflow, flag_numerical_scheme=scheme)
+    bates = L.local_inertial_model_d4(case.z, d, case.roughness, case.roughness ** 2, case.resolution ** 2, ts,
+                                      case.resolution, case.outlet_rows, case.outlet_cols, 1,
+                                      case.params["slope_outlet"], outflow, flag_numerical_scheme=1)
+    assert np.abs(lit.qout_right - bates.qout_right).max() > 1.0   # the scheme changes the fluxes
+    import oracle
+    o = oracle.KernelFormOracle(*case.shape, case.resolution, "fp64",
+                                **dict(case.params, flag_numerical_scheme=scheme))
+    case.apply(o)
+    o.set_state(d, outflow)
+    o.li_step(ts)
+    assert np.allclose(o.download_native("h") * 1000, lit.d_t, rtol=1e-11, atol=1e-10, equal_nan=True)
+    qr = o.download_native("qx") * 3.6e6 / case.resolution
+    qu = o.download_native("qy") * 3.6e6 / case.resolution
+    assert np.allclose(qr, lit.qout_right, rtol=1e-10, atol=1e-8)
+    assert np.allclose(qu, lit.qout_up, rtol=1e-10, atol=1e-8)
+
+
+@pytest.mark.parametrize("scheme", [1, 2])
+def test_li_step_critical_clip_agrees(oracle_lib, scheme):
+    """flag_critical = 1 (Local_Inertial_Model_D4.m:272-275): |q| <= Hf sqrt(g Hf) after the
+    solver; a steep random state with large prior fluxes makes the clip bind on many faces."""
+    case = random_terrain(31, 29, seed=8)
+    case.z = case.z * 6.0   # steep: supercritical faces within one step
+    d, outflow = _prior_state(case, 8, 2e6)
+    ts = 2.0 / 60
+    kw = dict(flag_numerical_scheme=scheme)
+    args = (case.z, d, case.roughness, case.roughness ** 2, case.resolution ** 2, ts, case.resolution,
+            case.outlet_rows, case.outlet_cols, 1, case.params["slope_outlet"], outflow)
+    lit = L.local_inertial_model_d4(*args, flag_critical=1, **kw)
+    free = L.local_inertial_model_d4(*args, flag_critical=0, **kw)
+    clipped = np.abs(lit.qout_right - free.qout_right) > 1e-6
+    assert clipped.sum() > 20   # the clip binds
+    import oracle
+    o = oracle.KernelFormOracle(*case.shape, case.resolution, "fp64",
+                                **dict(case.params, flag_critical=1, **kw))
+    case.apply(o)
+    o.set_state(d, outflow)
+    o.li_step(ts)
+    assert np.allclose(o.download_native("h") * 1000, lit.d_t, rtol=1e-11, atol=1e-10)
+    qr = o.download_native("qx") * 3.6e6 / case.resolution
+    qu = o.download_native("qy") * 3.6e6 / case.resolution
+    assert np.allclose(qr, lit.qout_right, rtol=1e-10, atol=1e-8)
+    assert np.allclose(qu, lit.qout_up, rtol=1e-10, atol=1e-8)
+
+
+@pytest.mark.parametrize("scheme,critical", [(2, 0), (3, 0), (1, 1), (3, 1)])
+def test_full_loop_dambreak_schemes_agree(oracle_lib, scheme, critical):
+    """The whole loop (rain-free dam-break, adaptive dt) with the diffusive schemes and the
+    critical clip: kernel form against literal for 120 steps, to round-off relative to the
+    reservoir depth (the dam-break amplifies the two forms' different roundings to ~1e-11 of
+    the depth scale over these steps)."""
+    from tests.cases import small_dambreak
+    case = small_dambreak(24, 96, seed=9)
+    case.params = dict(case.params, flag_numerical_scheme=scheme, flag_critical=critical)
+    cfg = literal_cfg(case)
+    cfg.flag_numerical_scheme = scheme
+    cfg.flag_critical = critical
+    st = L.init_state(cfg)
+    o = kernel_form(case)
+    for k in range(120):
+        L.step(cfg, st)
+        o.fused_steps(1)
+        d = o.diag()
+        assert d["time_step"] == pytest.approx(st.time_step, rel=1e-12), k
+        h = o.download_native("h") * 1000
+        assert np.abs(h - st.d).max() <= 1e-9 * np.abs(st.d).max(), k

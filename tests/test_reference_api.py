@@ -27,7 +27,7 @@ def test_unsupported_flags_raise_before_device():
     from hydropol2d_b200 import HP2DError, reference_api
     case = random_terrain(8, 8, seed=1)
     args = list(_lim_args(case, case.d0, np.zeros((8, 8, 3)), 0.01))
-    for pos, v in ((0, 2), (13, 2), (31, 1)):   # flag_numerical_scheme=2, flag_reservoir=2, flag_subgrid=1
+    for pos, v in ((0, 4), (13, 2), (31, 1)):   # flag_numerical_scheme=4, flag_reservoir=2, flag_subgrid=1
         bad = list(args)
         bad[pos] = v
         with pytest.raises(HP2DError) as e:

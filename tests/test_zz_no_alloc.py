@@ -1,7 +1,13 @@
 """hp2d_cfl_dt_noalloc: the allocation-free timestep for callers that may not allocate GPU
-memory while they run (a MEX gateway inside MATLAB's GPU memory pool, code inside a stream
-capture).  Its scratch is a fixed array inside the library, so these checks compare it with
-hp2d_cfl_dt on a context, bit for bit, over two calls in a row on different states.
+memory while they run (a MEX gateway inside MATLAB, whose GPU memory pool owns the device).
+Its scratch is a fixed array inside the library, so these checks compare it with
+hp2d_cfl_dt on a context, bit for bit, over two calls in a row on different states:
+
+* an 80-row urban grid (five 16-row blocks of partial maxima);
+* a 8200 x 24 V-tilt (513 blocks, the last one 8 rows), so the final kernel's strided loop
+  over more than 256 partials runs, with flag_adaptive_timestepping 1 and 0 (the wave-only
+  and the speed-plus-celerity terms);
+* a 65536-row V-tilt, the largest grid the scratch holds (4096 blocks).
 
 This file is named to be collected last, and passes alone in a fresh process as well.
 """
@@ -42,14 +48,15 @@ def _noalloc_dt(L, case, sf, qx, qy, hf):
     return ts.value, vm.value
 
 
-def test_noalloc_timestep_matches_context_timestep_twice():
-    from hydropol2d_b200 import SurfaceFlow, _abi, build, synthetic as S
+def _two_calls(case, steps_before=40, steps_between=25, **param_overrides):
+    """Two consecutive calls, each against hp2d_cfl_dt on the same face fluxes and depths."""
+    from hydropol2d_b200 import SurfaceFlow, _abi, build
     build.build()
     L = _abi.lib()
-    case = S.urban_case(80, 2.0, seed=21, hours=0.5)   # 80 rows: five 16-row blocks
-    sf = SurfaceFlow(*case.shape, case.resolution, "fp32", **case.params)
+    params = dict(case.params, **param_overrides)
+    sf = SurfaceFlow(*case.shape, case.resolution, "fp32", **params)
     case.apply(sf)
-    sf.fused_steps(40)
+    sf.fused_steps(steps_before)
     results = []
     for call in range(2):
         d = sf.diag()
@@ -63,10 +70,34 @@ def test_noalloc_timestep_matches_context_timestep_twice():
         assert got_vm == ref_vm, (call, got_vm, ref_vm)
         results.append((got_ts, got_vm))
         sf.set_clock(d["t"] + ref_ts, ref_ts, d["k"] + 1)
-        sf.fused_steps(25)   # a different state for the second call
+        sf.fused_steps(steps_between)   # a different state for the second call
+    sf.close()
+    return results
+
+
+def test_noalloc_timestep_matches_context_timestep_twice():
+    from hydropol2d_b200 import synthetic as S
+    results = _two_calls(S.urban_case(80, 2.0, seed=21, hours=0.5))   # 80 rows: five 16-row blocks
     assert results[0] != results[1]
     assert results[0][1] > 0
-    sf.close()
+
+
+@pytest.mark.parametrize("adaptive", [1, 0])
+def test_noalloc_many_blocks_ragged_last_block(adaptive):
+    from hydropol2d_b200 import synthetic as S
+    case = S.vtilt_case(8200, 24, 10.0)   # 513 blocks of 16 rows, the last one 8 rows
+    case.d0 = np.full(case.shape, 40.0)   # 40 mm everywhere: flowing, non-stagnant cells at once
+    results = _two_calls(case, steps_before=60, steps_between=40, flag_adaptive_timestepping=adaptive)
+    assert results[0] != results[1]
+    assert results[1][1] > 0
+
+
+def test_noalloc_largest_grid_it_holds():
+    from hydropol2d_b200 import synthetic as S
+    case = S.vtilt_case(65536, 8, 10.0)   # 4096 blocks: every partial slot of the scratch
+    case.d0 = np.full(case.shape, 40.0)
+    results = _two_calls(case, steps_before=30, steps_between=20)
+    assert results[1][1] > 0
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
