@@ -39,10 +39,10 @@ EXPORTS = [
     "hp2d_upload_static", "hp2d_set_soil", "hp2d_set_soil_vg", "hp2d_set_state", "hp2d_set_clock", "hp2d_set_rain_clock",
     "hp2d_set_rain_uniform", "hp2d_set_rain_maps", "hp2d_set_rain_gauges", "hp2d_set_inflow", "hp2d_set_stage",
     "hp2d_set_reservoirs", "hp2d_set_hazard_tracking", "hp2d_set_dry_skip",
-    "hp2d_set_map_records", "hp2d_map_records", "hp2d_download_map_record", "hp2d_hydrology_step", "hp2d_li_step",
+    "hp2d_set_map_records", "hp2d_set_map_records_host", "hp2d_map_records", "hp2d_download_map_record", "hp2d_hydrology_step", "hp2d_li_step",
     "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed",
     "hp2d_set_tuning", "hp2d_set_layout", "hp2d_run",
-    "hp2d_set_retry_policy", "hp2d_set_wait_limit", "hp2d_inject_step_fault",
+    "hp2d_set_retry_policy", "hp2d_set_wait_limit", "hp2d_inject_step_fault", "hp2d_set_temporal_blocking",
     "hp2d_download",
     "hp2d_download_native", "hp2d_get_diag", "hp2d_stored_volume",
     "hp2d_cfl_dt_noalloc", "hp2d_noalloc_error",
@@ -93,7 +93,7 @@ class Diag(C.Structure):
         ("rain_t0", C.c_double), ("rain_t1", C.c_double), ("t_previous", C.c_double),
         ("inflow_volume", C.c_double), ("stage_volume", C.c_double),
         ("structure_volume", C.c_double), ("skipped_cells", C.c_int64), ("skipped_read_cells", C.c_int64),
-        ("retries", C.c_int64), ("catch_index", C.c_int32), ("pad", C.c_int32), ("max_time_step", C.c_double),
+        ("retries", C.c_int64), ("catch_index", C.c_int32), ("steps_per_block", C.c_int32), ("max_time_step", C.c_double),
     ]
 
 
@@ -140,6 +140,7 @@ def lib() -> C.CDLL:
         "hp2d_set_clock": ([vp, C.c_double, C.c_double, C.c_int64], C.c_int),
         "hp2d_set_rain_clock": ([vp, C.c_double, C.c_double, C.c_double], C.c_int),
         "hp2d_set_map_records": ([vp, C.c_int32, P(C.c_double), C.c_int32], C.c_int),
+        "hp2d_set_map_records_host": ([vp, C.c_int32, P(C.c_double), C.c_int32], C.c_int),
         "hp2d_set_stage": ([vp, C.c_int32, C.c_int32, P(C.c_double), P(C.c_double), C.c_int32,
                             P(C.c_int32), P(C.c_int32), P(C.c_int32)], C.c_int),
         "hp2d_set_hazard_tracking": ([vp, C.c_int32], C.c_int),
@@ -167,6 +168,7 @@ def lib() -> C.CDLL:
         "hp2d_set_retry_policy": ([vp, C.c_int32, C.c_double, C.c_int32], C.c_int),
         "hp2d_set_wait_limit": ([vp, C.c_int64], C.c_int),
         "hp2d_inject_step_fault": ([vp, C.c_int64, C.c_int32], C.c_int),
+        "hp2d_set_temporal_blocking": ([vp, C.c_int32], C.c_int),
         "hp2d_download": ([vp, C.c_int32, dp, C.c_size_t], C.c_int),
         "hp2d_download_native": ([vp, C.c_int32, vp, C.c_size_t], C.c_int),
         "hp2d_get_diag": ([vp, P(Diag)], C.c_int),

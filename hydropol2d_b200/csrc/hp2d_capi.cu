@@ -20,14 +20,17 @@
 #include <memory>
 #include <string>
 #include <mutex>
+#include <stdexcept>
 #include <vector>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "hp2d.h"
 #include "hp2d_device.cuh"
 #include "hp2d_fused.cuh"
 #include "hp2d_unfused.cuh"
+#include "hp2d_tb.cuh"
 
 using namespace hp2d;
 
@@ -96,6 +99,38 @@ __global__ void k_volume4(size_t n, const typename Vec<R>::V4* st, double* out) 
     if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(out, acc);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+typedef CUresult (*TensorMapEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                      const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+TensorMapEncodeFn tensor_map_encoder() {
+    static TensorMapEncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<TensorMapEncodeFn>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+// an array of ny x nx float4 records as a [ny][nx][4] float tensor, boxes of ex x ey records
+// (coordinates outside the array read as zeros)
+bool record_map(CUtensorMap* m, const void* base, int ny, int nx, int ex, int ey) {
+    TensorMapEncodeFn fn = tensor_map_encoder();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {4, cuuint64_t(nx), cuuint64_t(ny)};
+    cuuint64_t strides[2] = {16, cuuint64_t(nx) * 16};
+    cuuint32_t box[3] = {4, cuuint32_t(ex), cuuint32_t(ey)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 struct hp2d_ctx {
@@ -143,6 +178,17 @@ template <typename R> struct Impl : Base {
     // map records
     Dev<double> rec_times, rec_t;
     Dev<R> rec_snap;
+    // records kept in page-locked host memory mapped into the device's address space
+    // (hp2d_set_record_target(ctx, 1)): the step that takes a record writes it across the host
+    // link itself, overlapped with its other work, and reading it back is a host-side read
+    R* rec_host = nullptr;
+    size_t rec_host_n = 0;
+    int rec_target = 0;
+    void free_rec_host() {
+        if (rec_host) cudaFreeHost(rec_host);
+        rec_host = nullptr;
+        rec_host_n = 0;
+    }
     RecordDesc<R> rec{};
     Dev<float> maps;
     RainDesc rain{};
@@ -226,6 +272,7 @@ template <typename R> struct Impl : Base {
     }
     ~Impl() override {
         if (graph) cudaGraphExecDestroy(graph);
+        free_rec_host();
     }
 
     cudaStream_t st() const { return ctx->stream; }
@@ -817,12 +864,23 @@ template <typename R> struct Impl : Base {
         for (int q = 1; q < nt; ++q)
             if (!(times[q] > times[q - 1])) { ctx->err = "record times must increase"; return HP2D_INVALID_ARG; }
         rec = RecordDesc<R>{};
+        rec_snap.free();
+        free_rec_host();
         if (nt > 0) {
             rec_times.alloc(size_t(nt));
             upload(rec_times.p, std::vector<double>(times, times + nt));
-            rec_snap.alloc(size_t(nslots) * n);
+            R* snap = nullptr;
+            if (rec_target == 1) {
+                HP_CK(cudaHostAlloc(reinterpret_cast<void**>(&rec_host), size_t(nslots) * n * sizeof(R),
+                                    cudaHostAllocMapped | cudaHostAllocPortable));
+                rec_host_n = size_t(nslots) * n;
+                HP_CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&snap), rec_host, 0));
+            } else {
+                rec_snap.alloc(size_t(nslots) * n);
+                snap = rec_snap.p;
+            }
             rec_t.alloc(size_t(nslots));
-            rec = RecordDesc<R>{nt, nslots, rec_times.p, rec_snap.p, rec_t.p};
+            rec = RecordDesc<R>{nt, nslots, rec_times.p, snap, rec_t.p};
         }
         pull_sc();
         hs.rec_count = 0;
@@ -843,6 +901,11 @@ template <typename R> struct Impl : Base {
         hs.rec_pending = 0;
         push_sc();
     }
+    hp2d_status set_record_target(int32_t target, int32_t n_times, const double* times, int32_t n_slots) {
+        if (target != 0 && target != 1) { ctx->err = "record target must be 0 (device) or 1 (mapped host memory)"; return HP2D_INVALID_ARG; }
+        rec_target = target;
+        return set_map_records(n_times, times, n_slots);
+    }
     hp2d_status map_records(int64_t* count) {
         pull_sc();
         flush_records();
@@ -857,8 +920,15 @@ template <typename R> struct Impl : Base {
             return HP2D_INVALID_ARG;
         }
         const size_t slot = size_t(index % rec.n_slots);
-        auto v = fetch(rec.snap + slot * n, n);
-        for (size_t k = 0; k < n; ++k) depth_mm[k] = double(v[k]) * 1000.0;
+        if (rec_host) {   // already in host memory: the steps wrote it there
+            HP_CK(cudaStreamSynchronize(st()));
+            const R* v = rec_host + slot * n;
+            for (size_t k = 0; k < n; ++k) depth_mm[k] = double(v[k]) * 1000.0;
+        } else {
+            double* d = readback_buffer();
+            k_scaled_f64<R><<<blocks_for(n), kThreads, 0, st()>>>(n, rec.snap + slot * n, 1000.0, d);
+            copy_out(d, depth_mm);
+        }
         if (t_min) {
             double t = 0;
             HP_CK(cudaMemcpyAsync(&t, rec.snap_t + slot, sizeof(double), cudaMemcpyDeviceToHost, st()));
@@ -1039,7 +1109,7 @@ template <typename R> struct Impl : Base {
         a.rec = rec;
         a.strct = strct;
         a.dry_rows = dry_rows();
-        a.dryflag = dry_usable(rpw) ? dryf.p : nullptr;
+        a.dryflag = dry_usable(rpw) && tb_chosen <= 1 ? dryf.p : nullptr;
         a.vmax = hz_on ? vmaxm.p : nullptr;
         a.hzmax = hz_on ? hzmaxm.p : nullptr;
         a.sc = sc.p;
@@ -1236,6 +1306,7 @@ template <typename R> struct Impl : Base {
     hp2d_status fused_steps(int32_t nsteps, cudaEvent_t after = nullptr) {
         if (!static_ready) { ctx->err = "hp2d_upload_static not called"; return HP2D_NOT_READY; }
         if (soil_missing()) { ctx->err = "flag_infiltration=1 needs hp2d_set_soil, =2 hp2d_set_soil_vg"; return HP2D_NOT_READY; }
+        if (tb_chosen > 1) return blocked_steps(nsteps, after);
         opt_in();
         prologue();
         if (bad_state) return bad_state_error();
@@ -1251,6 +1322,109 @@ template <typename R> struct Impl : Base {
             if (status != HP2D_OK) break;
             todo = k_target - hs.k;
             if (todo <= 0) break;
+            prologue();
+            if (bad_state) { status = bad_state_error(); break; }
+        }
+        flush_records();
+        return status;
+    }
+
+    // ---------------- temporal blocking (hp2d_set_temporal_blocking) ----------------
+    int tb_k = 1;                 // requested: 1 off, 2..4 steps per block, 0 chosen by hp2d_autotune
+    int tb_chosen = 1;            // steps per block in use
+    int64_t tb_replay_until = 0;  // steps before this one run one per launch (a replayed block)
+    CUtensorMap tb_map[3];        // state buffers 0 and 1, static records
+    int tb_map_k = 0;             // K the maps' boxes were made for
+    int tb_ntx = 0, tb_nty = 0;
+
+    const char* tb_unsupported() const {
+        if (sizeof(R) != 4) return "temporal blocking is built for FP32 contexts";
+        if (inf_mode() != 0) return "temporal blocking does not support infiltration";
+        if (rain.n_uniform || rain.n_maps) return "temporal blocking does not support rain";
+        if (bc_kernel()) return "temporal blocking does not support inflow, stage, control structures or hazard maps";
+        if (rec.n_times > 0) return "temporal blocking does not support map records";
+        if (ctx->p.flag_numerical_scheme != 1) return "temporal blocking supports flag_numerical_scheme 1";
+        return nullptr;
+    }
+    hp2d_status set_temporal_blocking(int32_t k) {
+        if (k < 0 || k > 4) { ctx->err = "steps per block must be 0 (chosen by hp2d_autotune) or 1..4"; return HP2D_INVALID_ARG; }
+        if (k != 1 && sizeof(R) != 4) { ctx->err = "temporal blocking is built for FP32 contexts"; return HP2D_UNSUPPORTED_FLAG; }
+        tb_k = k;
+        use_block_depth(k == 0 ? 1 : k);
+        return HP2D_OK;
+    }
+    void use_block_depth(int k) {
+        tb_chosen = k;
+        pull_sc();
+        hs.refresh_every = k;
+        push_sc();
+        invalidate_graph();
+        dirty = true;   // the dry flags are not kept while blocks run
+    }
+    template <int K> void tb_launch_k(const FusedArgs<R>& a0) {
+        if constexpr (sizeof(R) == 4) {
+            using G = TbGeom<K>;
+            static std::mutex mu;
+            static std::vector<char> done;
+            {
+                int dev = 0;
+                HP_CK(cudaGetDevice(&dev));
+                std::lock_guard<std::mutex> lock(mu);
+                if (done.size() <= size_t(dev)) done.resize(size_t(dev) + 1, 0);
+                if (!done[size_t(dev)]) {
+                    HP_CK(cudaFuncSetAttribute(k_tb_block<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(G::smem)));
+                    done[size_t(dev)] = 1;
+                }
+            }
+            if (tb_map_k != K) {
+                if (!record_map(&tb_map[0], st4[0].p, ny, nx, G::EX, G::EY) ||
+                    !record_map(&tb_map[1], st4[1].p, ny, nx, G::EX, G::EY) ||
+                    !record_map(&tb_map[2], stat.p, ny, nx, G::EX, G::EY))
+                    throw std::runtime_error("cuTensorMapEncodeTiled rejected the record arrays");
+                tb_map_k = K;
+            }
+            FusedArgs<float> a = a0;
+            tb_ntx = (nx + kTbTX - 1) / kTbTX;
+            tb_nty = (ny + kTbTY - 1) / kTbTY;
+            a.n_ctas = unsigned(tb_ntx * tb_nty);
+            k_tb_block<K><<<a.n_ctas, kTbThreads, G::smem, st()>>>(a, tb_map[0], tb_map[1], tb_map[2], tb_ntx);
+        }
+    }
+    void tb_launch(const FusedArgs<R>& a, int k) {
+        if (k == 2) tb_launch_k<2>(a);
+        else if (k == 3) tb_launch_k<3>(a);
+        else tb_launch_k<4>(a);
+    }
+    // nsteps accepted steps with blocks of tb_chosen steps where the step counter is aligned
+    // (a block starts at a step k with (k - 2) % K == 0, so that its last step is a refresh step)
+    // and single launches elsewhere; a block that cannot be committed is replayed step by step
+    hp2d_status blocked_steps(int32_t nsteps, cudaEvent_t after) {
+        if (const char* why = tb_unsupported()) { ctx->err = why; return HP2D_UNSUPPORTED_FLAG; }
+        opt_in();
+        prologue();
+        if (bad_state) return bad_state_error();
+        const int K = tb_chosen;
+        const int64_t k_target = hs.k + nsteps;
+        hp2d_status status = HP2D_OK;
+        for (;;) {
+            const FusedArgs<R> a = fused_args();
+            int64_t k = hs.k;
+            while (k < k_target) {
+                if (k >= tb_replay_until && k >= 2 && (k - 2) % K == 0 && k_target - k >= K) {
+                    tb_launch(a, K);
+                    k += K;
+                } else {
+                    launch_fused(a);
+                    k += 1;
+                }
+            }
+            HP_CK(cudaGetLastError());
+            if (after) HP_CK(cudaEventRecord(after, st()));
+            pull_sc();
+            if (!hs.halted) break;
+            status = handle_halt();
+            if (status != HP2D_OK) break;
+            if (k_target - hs.k <= 0) break;
             prologue();
             if (bad_state) { status = bad_state_error(); break; }
         }
@@ -1295,12 +1469,25 @@ template <typename R> struct Impl : Base {
         hs.retry_dmax = 0ull;
         push_sc();
         {
+            // the launch marked arrivals with the times of at most tb_chosen steps from the clock
             const FusedArgs<R> a = fused_args();
-            const R t_arr = R(hs.t_min * 60.0 + hs.time_step * 60.0);
-            k_retry_scan<R><<<blocks_for(n), kThreads, 0, st()>>>(a, inf_mode(), t_arr);
+            const double dts = hs.time_step * 60.0;
+            double t = hs.t_min;
+            const R lo = R(t * 60.0 + dts);
+            for (int q = 1; q < std::max(tb_chosen, 1); ++q) t = dts / 60.0 + t;
+            const R hi = R(t * 60.0 + dts);
+            k_retry_scan<R><<<blocks_for(n), kThreads, 0, st()>>>(a, inf_mode(), lo, hi);
             HP_CK(cudaGetLastError());
         }
         pull_sc();
+        if (hs.status & kStatusTbReplay) {   // a block of temporal blocking: its steps one by one
+            hs.status &= ~kStatusTbReplay;
+            hs.halted = 0;
+            tb_replay_until = hs.k + tb_chosen;
+            push_sc();
+            dirty = true;
+            return HP2D_OK;
+        }
         if (hs.status & kStatusTimeout) {
             hs.status &= ~kStatusTimeout;
             hs.halted = 0;
@@ -1464,10 +1651,35 @@ template <typename R> struct Impl : Base {
             timed_out = timed_out || (hs.status & kStatusTimeout) != 0;
             put_back(snap);
         }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
         rows_per_warp = best;
         cells_per_lane = best_cpl;
+        // temporal blocking left to the tuner: blocks of 2, 3 and 4 steps against single steps,
+        // per step (the state is put back after each trial; the blocks' results differ from the
+        // single steps' by the frozen time step, which the caller accepted with steps_per_block 0)
+        if (tb_k == 0 && !tb_unsupported() && !timed_out) {
+            int best_k = 1;
+            float best_step = best_ms / float(std::max(trial, 1));
+            const FusedArgs<R> a = fused_args(best_cpl);
+            for (int kb = 2; kb <= 4; ++kb) {
+                tb_chosen = kb;
+                tb_launch(a, kb);   // warm-up
+                HP_CK(cudaEventRecord(e0, st()));
+                for (int s = 0; s < trial; ++s) tb_launch(a, kb);
+                HP_CK(cudaEventRecord(e1, st()));
+                HP_CK(cudaGetLastError());
+                HP_CK(cudaEventSynchronize(e1));
+                float ms = 0;
+                HP_CK(cudaEventElapsedTime(&ms, e0, e1));
+                pull_sc();
+                timed_out = timed_out || (hs.status & kStatusTimeout) != 0;
+                put_back(snap);
+                const float per = ms / float(std::max(trial, 1) * kb);
+                if (per < best_step) { best_step = per; best_k = kb; }
+            }
+            use_block_depth(best_k);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
         invalidate_graph();
         if (timed_out) { ctx->err = "a row copy did not complete within its wait limit"; return HP2D_TIMEOUT; }
         if (chosen) *chosen = best;
@@ -1516,10 +1728,6 @@ template <typename R> struct Impl : Base {
         copy_out(d, out);
     }
 
-    std::vector<V4> fetch_state() {
-        pull_sc();
-        return fetch(st4[hs.cur].p, n);
-    }
 
     hp2d_status download(int32_t field, double* out, size_t count) {
         if (count != n) { ctx->err = "count must be ny*nx"; return HP2D_INVALID_ARG; }
@@ -1535,30 +1743,28 @@ template <typename R> struct Impl : Base {
             case HP2D_FIELD_DEPTH: fetch_component_scaled(0, 1000.0, out); break;
             case HP2D_FIELD_QOUT_RIGHT: fetch_component_scaled(1, to_mmh, out); break;
             case HP2D_FIELD_QOUT_UP: fetch_component_scaled(2, to_mmh, out); break;
-            case HP2D_FIELD_QOUT_LEFT: {
-                auto v = fetch_state();
-                for (int i = 0; i < ny; ++i)
-                    for (int j = 0; j < nx; ++j)
-                        out[size_t(i) * nx + j] = j == 0 ? -0.0 : -double(v[size_t(i) * nx + j - 1].y) * to_mmh;
-                break;
-            }
-            case HP2D_FIELD_QOUT_DOWN: {
-                auto v = fetch_state();
-                for (int i = 0; i < ny; ++i)
-                    for (int j = 0; j < nx; ++j)
-                        out[size_t(i) * nx + j] = i + 1 == ny ? -0.0 : -double(v[size_t(i + 1) * nx + j].z) * to_mmh;
+            case HP2D_FIELD_QOUT_LEFT: case HP2D_FIELD_QOUT_DOWN: {
+                pull_sc();
+                double* d = readback_buffer();
+                k_shifted_flux_f64<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, st4[hs.cur].p,
+                                                                            field == HP2D_FIELD_QOUT_DOWN, to_mmh, d);
+                copy_out(d, out);
                 break;
             }
             case HP2D_FIELD_OUTLET_FLOW: per_outlet_map(qo, 3.6e6); break;
             case HP2D_FIELD_HF_X: case HP2D_FIELD_HF_Y: {
                 if (!(last_dt_s > 0)) { ctx->err = "Hf is materialised by hp2d_li_step only"; return HP2D_NOT_READY; }
-                auto v = fetch(field == HP2D_FIELD_HF_X ? hfx.p : hfy.p, n);
-                for (size_t k = 0; k < n; ++k) out[k] = double(v[k]);
+                fetch_scaled(field == HP2D_FIELD_HF_X ? hfx.p : hfy.p, 1.0, out);
                 break;
             }
             case HP2D_FIELD_HF_OUTLET: per_outlet_map(hf3, 1.0); break;
             case HP2D_FIELD_DMAX: fetch_component_scaled(3, 1000.0, out); break;
-            case HP2D_FIELD_ARRIVAL: { auto v = fetch(arrival.p, n); for (size_t k = 0; k < n; ++k) out[k] = double(v[k]) / 60.0; break; }
+            case HP2D_FIELD_ARRIVAL: {
+                double* d = readback_buffer();
+                k_divided_f64<R><<<blocks_for(n), kThreads, 0, st()>>>(n, arrival.p, 60.0, d);
+                copy_out(d, out);
+                break;
+            }
             case HP2D_FIELD_VMAX: case HP2D_FIELD_HAZARD_MAX: {
                 if (!hz_on) { ctx->err = "velocity / hazard maxima are off (hp2d_set_hazard_tracking)"; return HP2D_NOT_READY; }
                 fetch_scaled(field == HP2D_FIELD_VMAX ? vmaxm.p : hzmaxm.p, 1.0, out);
@@ -1567,21 +1773,17 @@ template <typename R> struct Impl : Base {
             case HP2D_FIELD_SOIL_STORAGE: {
                 if (!gs2[0].p) { ctx->err = "no soil storage (hp2d_set_soil not called)"; return HP2D_NOT_READY; }
                 pull_sc();
-                auto v = fetch(gs2[hs.cur].p, n);
-                for (size_t k = 0; k < n; ++k) out[k] = double(v[k].x) * 1000.0;
+                double* d = readback_buffer();
+                k_soil_component_f64<R><<<blocks_for(n), kThreads, 0, st()>>>(n, gs2[hs.cur].p, 1000.0, d);
+                copy_out(d, out);
                 break;
             }
             case HP2D_FIELD_I_TOT_END_CELL: {
-                auto v = fetch_state();
-                std::vector<double> of(n, 0.0);
-                if (n_out) {
-                    auto cells = fetch(outlet_cells.p, size_t(n_out));
-                    auto q = fetch(qo.p, size_t(n_out));
-                    for (int o = 0; o < n_out; ++o) of[cells[o]] = double(q[o]) * 3.6e6;
-                }
-                double dts = last_dt_s > 0 ? last_dt_s : hs.time_step * 60.0;
-                for (size_t k = 0; k < n; ++k)
-                    out[k] = std::fabs(double(v[k].y) * to_mmh + double(v[k].z) * to_mmh + of[k]) * dts / 1000.0 / 3600.0 * res * res;
+                pull_sc();
+                const double dts = last_dt_s > 0 ? last_dt_s : hs.time_step * 60.0;
+                double* d = readback_buffer();
+                k_itot_f64<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, stat.p, qo.p, to_mmh, dts, res, d);
+                copy_out(d, out);
                 break;
             }
             default: ctx->err = "unknown field"; return HP2D_INVALID_ARG;
@@ -1594,10 +1796,13 @@ template <typename R> struct Impl : Base {
         if (bytes != cnt * sizeof(R)) { ctx->err = "byte count mismatch"; return HP2D_INVALID_ARG; }
         R* o = static_cast<R*>(out);
         switch (field) {
-            case 0: case 1: case 2: case 5: {
-                auto v = fetch_state();
-                for (size_t k = 0; k < n; ++k)
-                    o[k] = field == 0 ? v[k].x : field == 1 ? v[k].y : field == 2 ? v[k].z : v[k].w;
+            case 0: case 1: case 2: case 5: {   // one component, gathered on the device
+                pull_sc();
+                R* d = reinterpret_cast<R*>(readback_buffer());
+                k_state_component<R><<<blocks_for(n), kThreads, 0, st()>>>(n, st4[hs.cur].p, field == 5 ? 3 : field, d);
+                HP_CK(cudaGetLastError());
+                HP_CK(cudaMemcpyAsync(o, d, n * sizeof(R), cudaMemcpyDeviceToHost, st()));
+                HP_CK(cudaStreamSynchronize(st()));
                 break;
             }
             case 3: case 4: {
@@ -1646,6 +1851,7 @@ template <typename R> struct Impl : Base {
         o->status_bits = hs.status;
         o->retries = hs.retries;
         o->catch_index = hs.catch_index;
+        o->steps_per_block = tb_chosen;
         o->max_time_step = hs.max_dt;
         return HP2D_OK;
     }
@@ -2060,7 +2266,11 @@ hp2d_status hp2d_set_inflow(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, co
 }
 
 hp2d_status hp2d_set_map_records(hp2d_ctx* ctx, int32_t n_times, const double* time_records, int32_t n_slots) {
-    return with_impl(ctx, [&](auto& m) { return m.set_map_records(n_times, time_records, n_slots); });
+    return with_impl(ctx, [&](auto& m) { return m.set_record_target(0, n_times, time_records, n_slots); });
+}
+
+hp2d_status hp2d_set_map_records_host(hp2d_ctx* ctx, int32_t n_times, const double* time_records, int32_t n_slots) {
+    return with_impl(ctx, [&](auto& m) { return m.set_record_target(1, n_times, time_records, n_slots); });
 }
 
 hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count) {
@@ -2193,6 +2403,10 @@ hp2d_status hp2d_set_wait_limit(hp2d_ctx* ctx, int64_t polls) {
 
 hp2d_status hp2d_inject_step_fault(hp2d_ctx* ctx, int64_t k, int32_t attempts) {
     return with_impl(ctx, [&](auto& m) { return m.inject_fault(k, attempts); });
+}
+
+hp2d_status hp2d_set_temporal_blocking(hp2d_ctx* ctx, int32_t steps_per_block) {
+    return with_impl(ctx, [&](auto& m) { return m.set_temporal_blocking(steps_per_block); });
 }
 
 hp2d_status hp2d_download(hp2d_ctx* ctx, int32_t field, double* host, size_t count) {

@@ -177,7 +177,8 @@ struct StepScalars {
     unsigned long long retry_dmax;  // retry scan: max depth of d_p and d_tot [m] (ordered bits)
     int bad_domain;                 // start-of-run scan: a cell of finite elevation holds a
                                     // non-finite depth
-    int pad3;
+    int refresh_every;              // temporal blocking K: the time step is refreshed only on step
+                                    // 1 and on the steps k with (k - 1) % K == 0 (<= 1: every step)
 };
 // StepScalars::status bits
 constexpr unsigned kStatusNumerical = 1u;   // a step was rejected (non-finite / negative depth)

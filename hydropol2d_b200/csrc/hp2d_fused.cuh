@@ -876,7 +876,8 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         const double delta = time_save - sc->tsp;
         sc->tsp = time_save;
         double tcr = sc->time_step * 60.0;   // refreshing_timestep.m:361-365
-        if (delta > 0 || sc->k == 1) {
+        if ((delta > 0 || sc->k == 1) &&
+            (sc->refresh_every <= 1 || sc->k == 1 || (sc->k - 1) % sc->refresh_every == 0)) {
             tcr = finalize_dt(vm, cm, a.res, a.alfa_min, a.alfa_max, a.min_dt, sc->max_dt, a.inc,
                               a.flag_timestep);
             sc->vmax_last = vm;
@@ -1064,6 +1065,39 @@ template <typename R> __global__ void k_scaled_f64(size_t n, const R* src, doubl
     for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
         out[k] = double(src[k]) * scale;
 }
+template <typename R> __global__ void k_divided_f64(size_t n, const R* src, double div, double* out) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
+        out[k] = double(src[k]) / div;
+}
+// the soil storage I of the soil records, times `scale`
+template <typename R>
+__global__ void k_soil_component_f64(size_t n, const typename Vec<R>::V2* gs, double scale, double* out) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
+        out[k] = double(gs[k].x) * scale;
+}
+// qout_left (-q_x of the cell to the left, -0 on the first column) or qout_down (-q_y of the
+// cell below, -0 on the last row) [mm/h] (Local_Inertial_Model_D4.m:347-350)
+template <typename R>
+__global__ void k_shifted_flux_f64(int ny, int nx, const typename Vec<R>::V4* st, int down, double scale, double* out) {
+    const size_t n = size_t(ny) * nx;
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(k / nx), j = int(k % nx);
+        if (down) out[k] = i + 1 == ny ? -0.0 : -double(st[k + nx].z) * scale;
+        else out[k] = j == 0 ? -0.0 : -double(st[k - 1].y) * scale;
+    }
+}
+// CA_States.I_tot_end_cell [m^3] (Local_Inertial_Model_D4.m:512-514): |right + up + outlet flux|
+// [mm/h] x dt over the cell area, from the state records and each outlet cell's sink rate
+template <typename R>
+__global__ void k_itot_f64(size_t n, const typename Vec<R>::V4* st, const typename Vec<R>::V4* stat, const R* qo,
+                           double to_mmh, double dts, double res, double* out) {
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const auto v = st[k];
+        const unsigned ord = outlet_ord(meta_bits(stat[k].w));
+        const double of = ord ? double(qo[ord - 1]) * 3.6e6 : 0.0;
+        out[k] = fabs(double(v.y) * to_mmh + double(v.z) * to_mmh + of) * dts / 1000.0 / 3600.0 * res * res;
+    }
+}
 
 // a map record taken by the host when no step follows the one that triggered it
 template <typename R> __global__ void k_record_depth(size_t n, const typename Vec<R>::V4* st, R* dst) {
@@ -1085,9 +1119,10 @@ template <typename R> __global__ void k_inflow_depth(InflowDesc<R> d, const Step
 // infiltration, inflow and clamps give d_tot -- and reduces max(d_p, d_tot) (NaN skipped, as
 // MATLAB's max) into sc->retry_dmax.  It also takes back the arrival times the attempt wrote:
 // a cell whose arrival equals the attempt's t_arr and whose start-of-step maximum is below the
-// threshold was marked by it.  inf: 0 none, 1 Green-Ampt, 2 van Genuchten.
+// threshold was marked by it (a block of temporal blocking marks with the times of its
+// sub-steps, the range [t_arr_lo, t_arr_hi]).  inf: 0 none, 1 Green-Ampt, 2 van Genuchten.
 template <typename R>
-__global__ void k_retry_scan(const FusedArgs<R> a, int inf, R t_arr_rejected) {
+__global__ void k_retry_scan(const FusedArgs<R> a, int inf, R t_arr_lo, R t_arr_hi) {
     StepScalars* sc = a.sc;
     RainStep<R> RS;
     RS.make(a.rain, sc->rain_a, sc->rain_b);
@@ -1114,7 +1149,8 @@ __global__ void k_retry_scan(const FusedArgs<R> a, int inf, R t_arr_rejected) {
         if (!skip && hh < R(1e-9)) hh = R(0);
         if (hh < R(0)) hh = R(0);
         m = fmax(m, hh);
-        if (a.arrival[c] == t_arr_rejected && rec.w < K.thr) a.arrival[c] = R(__int_as_float(0x7f800000));
+        const R ar = a.arrival[c];
+        if (ar >= t_arr_lo && ar <= t_arr_hi && rec.w < K.thr) a.arrival[c] = R(__int_as_float(0x7f800000));
     }
     m = warp_max(m);
     if ((threadIdx.x & 31) == 0 && m > R(0)) atomicMax(&sc->retry_dmax, ord_bits(m));

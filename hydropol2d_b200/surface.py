@@ -184,11 +184,13 @@ class SurfaceFlow:
         self._check(self._L.hp2d_set_rain_gauges(self._h, int(x.size), _dp(x), _dp(y), int(r.shape[0]),
                                                  float(record_dt), _dp(r), float(x_ul), float(y_ul)))
 
-    def set_map_records(self, time_records, n_slots: int):
+    def set_map_records(self, time_records, n_slots: int, host: bool = False):
         """Keep the depth map after each step that passes a record time [min]
-        (save_output_maps); ``n_slots`` maps are held on the device."""
+        (save_output_maps); ``n_slots`` maps are held on the device, or with ``host`` in
+        page-locked host memory that the steps write across the host link themselves."""
         t = _f64(time_records).ravel()
-        self._check(self._L.hp2d_set_map_records(self._h, int(t.size), _dp(t), int(n_slots)))
+        fn = self._L.hp2d_set_map_records_host if host else self._L.hp2d_set_map_records
+        self._check(fn(self._h, int(t.size), _dp(t), int(n_slots)))
 
     def map_records(self) -> int:
         c = C.c_int64()
@@ -268,6 +270,11 @@ class SurfaceFlow:
     def set_wait_limit(self, polls: int):
         """Polls of a row-copy wait before the step gives up with HP2D_TIMEOUT (default 4194304)."""
         self._check(self._L.hp2d_set_wait_limit(self._h, int(polls)))
+
+    def set_temporal_blocking(self, steps_per_block: int):
+        """K steps per launch at the frozen time step of the last refresh (2..4), 1 off, 0 chosen
+        by ``autotune`` (see hp2d_set_temporal_blocking)."""
+        self._check(self._L.hp2d_set_temporal_blocking(self._h, int(steps_per_block)))
 
     def inject_step_fault(self, k: int, attempts: int = 1):
         """Test hook: the next ``attempts`` attempts of step ``k`` are rejected."""

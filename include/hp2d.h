@@ -124,7 +124,7 @@ typedef struct hp2d_diag {
                                      were not read either */
     int64_t retries;              /* rejected step attempts retried so far */
     int32_t catch_index;          /* the reference's catch_index (1 + failures so far) */
-    int32_t pad;
+    int32_t steps_per_block;      /* temporal blocking in use (1: off; hp2d_set_temporal_blocking) */
     double max_time_step;         /* running_control.max_time_step [s], lowered by retries */
 } hp2d_diag;
 
@@ -232,6 +232,12 @@ hp2d_status hp2d_set_inflow(hp2d_ctx* ctx, int32_t n_gauges, int32_t n_times, co
  * The first-step map the reference writes before any record event is overwritten by the first
  * event there and is not kept here.  n_times = 0 switches the records off. */
 hp2d_status hp2d_set_map_records(hp2d_ctx* ctx, int32_t n_times, const double* time_records, int32_t n_slots);
+/* hp2d_set_map_records with the n_slots maps kept in page-locked host memory mapped into the
+ * device's address space (no counterpart in the reference; save_output_maps.m:565-580 moves the
+ * maps to the host in chunks): the step that takes a record writes the map across the host link
+ * itself, overlapped with the rest of its work, so no copy runs at read-back time and nothing of
+ * the record ring occupies GPU memory.  Read with hp2d_download_map_record as usual. */
+hp2d_status hp2d_set_map_records_host(hp2d_ctx* ctx, int32_t n_times, const double* time_records, int32_t n_slots);
 /* Records taken so far. */
 hp2d_status hp2d_map_records(hp2d_ctx* ctx, int64_t* count);
 /* Record `index` (0-based, one of the last n_slots taken): depth [mm] (ny*nx) and clock [min]. */
@@ -346,6 +352,19 @@ hp2d_status hp2d_set_wait_limit(hp2d_ctx* ctx, int64_t polls);
 /* Test hook (no counterpart in the reference): the next `attempts` attempts of step k are
  * rejected as if a depth had gone non-finite, so that the retry path runs on demand. */
 hp2d_status hp2d_inject_step_fault(hp2d_ctx* ctx, int64_t k, int32_t attempts);
+
+/* Temporal blocking (no counterpart in the reference; opt-in): steps_per_block = K in 2..4 makes
+ * hp2d_fused_steps advance K steps per launch at the time step of the last refresh, which then
+ * runs only on step 1 and on the steps k with (k - 1) % K == 0 (refreshing_timestep.m:17-368
+ * runs every step in the reference, so results follow the frozen-step schedule, not the per-step
+ * one).  Each block stages 64 x 32 output cells with a 2K-cell halo in shared memory by TMA and
+ * writes them back once.  Steps that do not fill an aligned block, and blocks in which an outlet
+ * cell asked for the clamp skip of Hydrological_Model.m:45-50 or a step was rejected, run one
+ * per launch under the same schedule.  FP32 only; no rain, infiltration, inflow, stage, control
+ * structures, map records or hazard maps (HP2D_UNSUPPORTED_FLAG at the next fused call); the
+ * dry-row skips are off while it is on.  steps_per_block = 1 switches it off; 0 lets
+ * hp2d_autotune choose K among 1..4 by measured time per step. */
+hp2d_status hp2d_set_temporal_blocking(hp2d_ctx* ctx, int32_t steps_per_block);
 
 /* ---- outputs ---------------------------------------------------------------------- */
 hp2d_status hp2d_download(hp2d_ctx* ctx, int32_t field, double* host, size_t count);

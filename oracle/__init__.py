@@ -85,6 +85,7 @@ def _load():
             "oracle_get_diag": ([vp, P(_abi.Diag)], C.c_int),
             "oracle_set_retry_policy": ([vp, C.c_int32, C.c_double, C.c_int32], C.c_int),
             "oracle_inject_step_fault": ([vp, C.c_int64, C.c_int32], C.c_int),
+            "oracle_set_refresh_every": ([vp, C.c_int32], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -241,6 +242,11 @@ class KernelFormOracle:
     def set_retry_policy(self, max_retries=8, factor_reduction=2.0, dt_floor_is_error=False):
         self._L.oracle_set_retry_policy(self._h, int(max_retries), float(factor_reduction),
                                         int(bool(dt_floor_is_error)))
+
+    def set_temporal_blocking(self, steps_per_block):
+        """The refresh schedule of temporal blocking: the time step is refreshed on step 1 and on
+        the steps k with (k - 1) % K == 0 (K <= 1: every step)."""
+        self._L.oracle_set_refresh_every(self._h, int(steps_per_block))
 
     def inject_step_fault(self, k, attempts=1):
         self._L.oracle_inject_step_fault(self._h, int(k), int(attempts))

@@ -846,6 +846,7 @@ public:
     // lowered to 1.5 x the new step, the new step capped by it (infinite -> min_time_step), the
     // rain interval [rewound clock, new clock].  The velocity and hazard maxima keep the
     // attempt's contribution (as the library's in-place maps do).
+    int refresh_every = 1;          // temporal blocking K: refresh on step 1 and when (k-1) % K == 0
     int64_t fault_k = -1;
     int fault_n = 0;
     int catch_index = 1;
@@ -895,7 +896,7 @@ public:
         tsp = time_save;
         double tcr = time_step * 60.0;
         bool floor_hit = false;
-        if (delta > 0 || k == 1) {
+        if ((delta > 0 || k == 1) && (refresh_every <= 1 || k == 1 || (k - 1) % refresh_every == 0)) {
             double vm;
             tcr = cfl(dts, &vm);
             vmax_last = vm;

@@ -194,6 +194,13 @@ int oracle_set_retry_policy(oracle_model* m, int32_t max_retries, double factor_
     });
 }
 
+int oracle_set_refresh_every(oracle_model* m, int32_t k) {
+    return dispatch(m, [&](auto& M) {
+        M.refresh_every = k;
+        return 0;
+    });
+}
+
 int oracle_inject_step_fault(oracle_model* m, int64_t k, int32_t attempts) {
     return dispatch(m, [&](auto& M) {
         M.fault_k = k;
@@ -271,6 +278,7 @@ int oracle_get_diag(oracle_model* m, hp2d_diag* o) {
         o->skipped_read_cells = 0;
         o->retries = M.retries;
         o->catch_index = M.catch_index;
+        o->steps_per_block = M.refresh_every;
         o->max_time_step = M.max_dt();
         return 0;
     });

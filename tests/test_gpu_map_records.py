@@ -11,13 +11,14 @@ from tests.test_gpu_parity import make_pair
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_records_bit_exact(precision, hp2d_lib, oracle_lib):
+@pytest.mark.parametrize("precision,host", [("fp32", False), ("fp64", False), ("fp32", True), ("fp64", True)])
+def test_records_bit_exact(precision, host, hp2d_lib, oracle_lib):
+    """host: the record ring in page-locked host memory, written by the steps themselves."""
     case = small_vtilt(32, 40)
     case.params = dict(case.params, routing_time=8.0)
     times = np.arange(0.0, 8.01, 0.25)
     g, o = make_pair(case, precision)
-    g.set_map_records(times, 64)
+    g.set_map_records(times, 64, host=host)
     o.set_map_records(times)
     for chunk in (1, 7, 33, 64, 100000):     # calls end between and right after record events
         g.fused_steps(chunk)

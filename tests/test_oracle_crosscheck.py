@@ -266,3 +266,30 @@ def test_full_loop_dambreak_schemes_agree(oracle_lib, scheme, critical):
         assert d["time_step"] == pytest.approx(st.time_step, rel=1e-12), k
         h = o.download_native("h") * 1000
         assert np.abs(h - st.d).max() <= 1e-9 * np.abs(st.d).max(), k
+
+
+def test_block_refresh_schedule(oracle_lib):
+    """The temporal-blocking schedule of the kernel-form oracle: with K = 3 the time step is
+    refreshed on step 1 and on the steps k with (k - 1) % 3 == 0 only, and K = 1 is the per-step
+    path."""
+    from tests.cases import small_dambreak
+    case = small_dambreak(24, 96, seed=9)
+    o = kernel_form(case)
+    o.set_temporal_blocking(3)
+    per = kernel_form(case)
+    prev = o.diag()["time_step"]
+    changed = []
+    for _ in range(30):
+        k = o.diag()["k"]
+        o.fused_steps(1)
+        per.fused_steps(1)
+        ts = o.diag()["time_step"]
+        if ts != prev:
+            changed.append(k)
+        prev = ts
+    assert changed and all(k == 1 or (k - 1) % 3 == 0 for k in changed), changed
+    assert o.diag()["t"] != per.diag()["t"]
+    one = kernel_form(case)
+    one.set_temporal_blocking(1)
+    one.fused_steps(30)
+    assert one.diag()["t"] == per.diag()["t"]
