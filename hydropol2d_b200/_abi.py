@@ -43,6 +43,7 @@ EXPORTS = [
     "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed",
     "hp2d_set_tuning", "hp2d_set_layout", "hp2d_run",
     "hp2d_set_retry_policy", "hp2d_set_wait_limit", "hp2d_inject_step_fault", "hp2d_set_temporal_blocking",
+    "hp2d_set_owned_rows", "hp2d_step_maxima", "hp2d_apply_refresh", "hp2d_copy_rows",
     "hp2d_download",
     "hp2d_download_native", "hp2d_get_diag", "hp2d_stored_volume",
     "hp2d_cfl_dt_noalloc", "hp2d_noalloc_error",
@@ -169,6 +170,10 @@ def lib() -> C.CDLL:
         "hp2d_set_wait_limit": ([vp, C.c_int64], C.c_int),
         "hp2d_inject_step_fault": ([vp, C.c_int64, C.c_int32], C.c_int),
         "hp2d_set_temporal_blocking": ([vp, C.c_int32], C.c_int),
+        "hp2d_set_owned_rows": ([vp, C.c_int32, C.c_int32], C.c_int),
+        "hp2d_step_maxima": ([vp, P(C.c_uint64), P(C.c_uint64), P(C.c_int32)], C.c_int),
+        "hp2d_apply_refresh": ([vp, C.c_uint64, C.c_uint64, C.c_int32], C.c_int),
+        "hp2d_copy_rows": ([vp, C.c_int32, C.c_int32, vp, C.c_int32], C.c_int),
         "hp2d_download": ([vp, C.c_int32, dp, C.c_size_t], C.c_int),
         "hp2d_download_native": ([vp, C.c_int32, vp, C.c_size_t], C.c_int),
         "hp2d_get_diag": ([vp, P(Diag)], C.c_int),

@@ -204,7 +204,12 @@ template <typename R> struct Impl : Base {
     int n_classes_vg = 0;
     VGGlobals<R> vgg{};
     std::vector<R> host_zwt;
-    std::vector<double> host_z;
+    std::vector<double> host_z;   // host copy of the DEM, fetched from z_keep when a setter needs it
+    Dev<double> z_keep;           // the caller's DEM (FP64) as uploaded
+    const std::vector<double>& hz() {
+        if (host_z.size() != n) host_z = fetch(z_keep.p, n);
+        return host_z;
+    }
     bool static_ready = false, dirty = true;
     double last_dt_s = 0;
     int rows_per_warp = 64;
@@ -337,7 +342,7 @@ template <typename R> struct Impl : Base {
 
     hp2d_status upload_static(const double* z, const double* rough, const int32_t* rows, const int32_t* cols,
                               int32_t nout, const double* slopes) {
-        host_z.assign(z, z + n);
+        host_z.clear();
         const double edge = std::numeric_limits<double>::infinity();   // closed domain-edge face
         std::vector<std::pair<int32_t, R>> outs;
         for (int o = 0; o < nout; ++o) {
@@ -375,15 +380,16 @@ template <typename R> struct Impl : Base {
         // the records (and the unfused entry points' structure-of-arrays copies) are built
         // on the device from the caller's FP64 arrays
         {
-            Dev<double> dz_, dr_;
+            Dev<double> dr_;
             Dev<uint32_t> dm_;
-            dz_.alloc(n); dr_.alloc(n); dm_.alloc(n);
-            HP_CK(cudaMemcpyAsync(dz_.p, z, n * sizeof(double), cudaMemcpyHostToDevice, st()));
+            if (z_keep.n != n) z_keep.alloc(n);   // kept: setters that need the DEM fetch it
+            dr_.alloc(n); dm_.alloc(n);
+            HP_CK(cudaMemcpyAsync(z_keep.p, z, n * sizeof(double), cudaMemcpyHostToDevice, st()));
             HP_CK(cudaMemcpyAsync(dr_.p, rough, n * sizeof(double), cudaMemcpyHostToDevice, st()));
             upload(dm_.p, host_meta);
             // the unfused entry points' copies are extracted from the records on first use
             dzx.free(); dzy.free(); n2.free();
-            k_build_static<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, dz_.p, dr_.p, dm_.p, stat.p, nullptr,
+            k_build_static<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, z_keep.p, dr_.p, dm_.p, stat.p, nullptr,
                                                                      nullptr, nullptr);
             HP_CK(cudaGetLastError());
             HP_CK(cudaStreamSynchronize(st()));
@@ -477,10 +483,11 @@ template <typename R> struct Impl : Base {
         // water-table depth (Infiltration_Module.m:192-199): GW_Depth = h_t - (z - Soil_Depth),
         // zwt = max(Soil_Depth - GW_Depth, 0); no head given = water table at the soil bottom
         host_zwt.assign(n, R(0));
+        const std::vector<double>& zz = hz();
         for (size_t k = 0; k < n; ++k) {
             const double sd = soil_depth[k];
-            const double ht = gw_head ? gw_head[k] : host_z[k] - sd;
-            const double gwd = ht - (host_z[k] - sd);
+            const double ht = gw_head ? gw_head[k] : zz[k] - sd;
+            const double gwd = ht - (zz[k] - sd);
             host_zwt[k] = R(std::max(sd - gwd, 0.0));
         }
         host_soil.assign(cls, cls + n);
@@ -686,7 +693,7 @@ template <typename R> struct Impl : Base {
             std::sort(v.begin(), v.end());   // a cell listed twice for a gauge gets it twice
             for (int32_t g : v) {
                 gl.push_back(g);
-                if (std::isfinite(host_z[k])) host_gcells[size_t(g)] += 1.0;
+                if (std::isfinite(hz()[k])) host_gcells[size_t(g)] += 1.0;
             }
             off.push_back(int32_t(gl.size()));
             st.push_back(stg[k]);
@@ -756,7 +763,7 @@ template <typename R> struct Impl : Base {
         hp2d_status s = check_bc_cells(ng, nc, rows, cols, gauge, cells, "stage");
         if (s != HP2D_OK) return s;
         for (size_t k : cells.cell)
-            if (!std::isfinite(host_z[k])) { ctx->err = "a stage cell needs a finite elevation"; return HP2D_INVALID_ARG; }
+            if (!std::isfinite(hz()[k])) { ctx->err = "a stage cell needs a finite elevation"; return HP2D_INVALID_ARG; }
         if (inflow_cells_h.cell.size() + stage_cells_h.cell.size() + cells.cell.size() >= (1u << 23)) {
             ctx->err = "too many stage cells";
             return HP2D_INVALID_ARG;
@@ -804,7 +811,7 @@ template <typename R> struct Impl : Base {
                 ctx->err = "an outlet cell cannot also be a structure cell";
                 return HP2D_INVALID_ARG;
             }
-            if (!std::isfinite(host_z[k])) { ctx->err = "a structure cell needs a finite elevation"; return HP2D_INVALID_ARG; }
+            if (!std::isfinite(hz()[k])) { ctx->err = "a structure cell needs a finite elevation"; return HP2D_INVALID_ARG; }
             auto it = std::find(cells.begin(), cells.end(), k);
             out = int32_t(it - cells.begin());
             if (it == cells.end()) cells.push_back(k);
@@ -1088,6 +1095,8 @@ template <typename R> struct Impl : Base {
         a.flag_critical = p.flag_critical; a.outlet_type = p.outlet_type; a.ga = ga() ? 1 : 0;
         a.scheme = p.flag_numerical_scheme;
         a.wait_polls = wait_polls;
+        a.own_r0 = own_r0;
+        a.own_r1 = own_r1 < 0 ? ny : own_r1;
         const int out_cols = 32 * cpl - 4;   // a strip's output columns (2-column apron each side)
         a.n_strips = (nx + out_cols - 1) / out_cols;
         const int rpw = rpw_chosen ? rows_per_warp : default_rows(cpl);
@@ -1109,7 +1118,7 @@ template <typename R> struct Impl : Base {
         a.rec = rec;
         a.strct = strct;
         a.dry_rows = dry_rows();
-        a.dryflag = dry_usable(rpw) && tb_chosen <= 1 ? dryf.p : nullptr;
+        a.dryflag = dry_usable(rpw) && tb_chosen <= 1 && !slab() ? dryf.p : nullptr;
         a.vmax = hz_on ? vmaxm.p : nullptr;
         a.hzmax = hz_on ? hzmaxm.p : nullptr;
         a.sc = sc.p;
@@ -1251,7 +1260,8 @@ template <typename R> struct Impl : Base {
         hs.bad_domain = 0;
         push_sc();
         k_skip_flag<R><<<blocks_for(n), kThreads, 0, st()>>>(st4[hs.cur].p, stat.p, ny, nx, rain, ga() ? 1 : 0, res,
-                                                           ctx->p.depth_tolerance, ctx->p.arrival_threshold, sc.p);
+                                                           ctx->p.depth_tolerance, ctx->p.arrival_threshold, sc.p,
+                                                           own_r0, own_r1 < 0 ? ny : own_r1);
         HP_CK(cudaGetLastError());
         if (inflow.n_gauges || inflow.n_stage) {
             k_inflow_depth<R><<<1, kThreads, 0, st()>>>(inflow, sc.p);
@@ -1327,6 +1337,74 @@ template <typename R> struct Impl : Base {
         }
         flush_records();
         return status;
+    }
+
+    // ---------------- row slabs of one grid (hp2d_set_owned_rows) ----------------
+    // A context that holds one slab of rows of a larger grid plus halo rows that other slabs own:
+    // its steps reduce the CFL maxima, ledgers and checks over its own rows only; the caller
+    // combines the slabs' maxima (hp2d_step_maxima, hp2d_apply_refresh) and refreshes the halo
+    // rows from their owners (hp2d_copy_rows) after every step.
+    int own_r0 = 0, own_r1 = -1;   // -1: every row
+    bool slab() const { return own_r0 != 0 || (own_r1 >= 0 && own_r1 != ny); }
+    hp2d_status set_owned_rows(int32_t r0, int32_t r1) {
+        if (r0 < 0 || r1 > ny || r0 >= r1) { ctx->err = "owned rows must satisfy 0 <= row0 < row1 <= ny"; return HP2D_INVALID_ARG; }
+        own_r0 = r0;
+        own_r1 = r1;
+        invalidate_graph();
+        dirty = true;
+        return HP2D_OK;
+    }
+    hp2d_status step_maxima(uint64_t* vbits, uint64_t* cbits, int32_t* skip) {
+        pull_sc();
+        *vbits = hs.last_vbits;
+        *cbits = hs.last_cbits;
+        if (skip) *skip = hs.skip_clamp;
+        return HP2D_OK;
+    }
+    // the last step's refresh redone with the maxima of every slab (the same arithmetic as the
+    // step's own finalize), and the clamp skip of the next step set to every slab's verdict
+    hp2d_status apply_refresh(uint64_t vbits, uint64_t cbits, int32_t skip) {
+        pull_sc();
+        if (hs.last_refreshed) {
+            const hp2d_params& p = ctx->p;
+            const bool is_d = sizeof(R) == 8;
+            const R vR = std::sqrt(R(from_ord(vbits, is_d)));
+            const double vm = double(vR);
+            double cm = 0.0;
+            if (cbits) {
+                const R v = R(from_ord(cbits - 1ull, is_d));
+                cm = p.flag_adaptive_timestepping == 1 ? double(std::fmax(std::sqrt(v), R(1e-10))) : double(v);
+            }
+            const double tcr = finalize_dt(vm, cm, res, p.alfa_min, p.alfa_max, p.min_time_step, hs.max_dt,
+                                           p.time_step_increments, p.flag_timestep);
+            const double t_old = hs.rain_b;   // the clock the step started from
+            const int uns = tcr == p.min_time_step;
+            hs.unstable += uns - hs.last_unstable;
+            hs.last_unstable = uns;
+            hs.vmax_last = vm;
+            hs.time_step = tcr / 60.0;
+            hs.t_min = tcr / 60.0 + t_old;
+            hs.t_prev = hs.k - 1 == 1 ? tcr / 60.0 : t_old;
+            hs.last_vbits = vbits;
+            hs.last_cbits = cbits;
+        }
+        hs.skip_clamp = skip;
+        push_sc();
+        return HP2D_OK;
+    }
+    hp2d_status copy_rows(int32_t row0, int32_t nrows, void* buf, int32_t into_state) {
+        if (row0 < 0 || nrows < 0 || row0 + nrows > ny || (nrows > 0 && !buf)) {
+            ctx->err = "rows outside the grid";
+            return HP2D_INVALID_ARG;
+        }
+        if (gs2[0].p && inf_mode()) { ctx->err = "row copies carry the state records only (no infiltration)"; return HP2D_UNSUPPORTED_FLAG; }
+        pull_sc();
+        V4* rows = st4[hs.cur].p + size_t(row0) * nx;
+        const size_t bytes = size_t(nrows) * nx * sizeof(V4);
+        if (into_state) HP_CK(cudaMemcpyAsync(rows, buf, bytes, cudaMemcpyDefault, st()));
+        else HP_CK(cudaMemcpyAsync(buf, rows, bytes, cudaMemcpyDefault, st()));
+        HP_CK(cudaStreamSynchronize(st()));
+        return HP2D_OK;
     }
 
     // ---------------- temporal blocking (hp2d_set_temporal_blocking) ----------------
@@ -2403,6 +2481,23 @@ hp2d_status hp2d_set_wait_limit(hp2d_ctx* ctx, int64_t polls) {
 
 hp2d_status hp2d_inject_step_fault(hp2d_ctx* ctx, int64_t k, int32_t attempts) {
     return with_impl(ctx, [&](auto& m) { return m.inject_fault(k, attempts); });
+}
+
+hp2d_status hp2d_set_owned_rows(hp2d_ctx* ctx, int32_t row0, int32_t row1) {
+    return with_impl(ctx, [&](auto& m) { return m.set_owned_rows(row0, row1); });
+}
+
+hp2d_status hp2d_step_maxima(hp2d_ctx* ctx, uint64_t* speed2_bits, uint64_t* celerity_bits, int32_t* clamp_skip) {
+    if (!speed2_bits || !celerity_bits) return HP2D_INVALID_ARG;
+    return with_impl(ctx, [&](auto& m) { return m.step_maxima(speed2_bits, celerity_bits, clamp_skip); });
+}
+
+hp2d_status hp2d_apply_refresh(hp2d_ctx* ctx, uint64_t speed2_bits, uint64_t celerity_bits, int32_t clamp_skip) {
+    return with_impl(ctx, [&](auto& m) { return m.apply_refresh(speed2_bits, celerity_bits, clamp_skip); });
+}
+
+hp2d_status hp2d_copy_rows(hp2d_ctx* ctx, int32_t row0, int32_t nrows, void* buffer, int32_t into_state) {
+    return with_impl(ctx, [&](auto& m) { return m.copy_rows(row0, nrows, buffer, into_state); });
 }
 
 hp2d_status hp2d_set_temporal_blocking(hp2d_ctx* ctx, int32_t steps_per_block) {

@@ -179,6 +179,11 @@ struct StepScalars {
                                     // non-finite depth
     int refresh_every;              // temporal blocking K: the time step is refreshed only on step
                                     // 1 and on the steps k with (k - 1) % K == 0 (<= 1: every step)
+    // the last step's reduced CFL maxima (ordered bits as acc_vmax / acc_cmax), whether it
+    // refreshed the time step and whether that refresh hit min_time_step: a grid split into row
+    // slabs redoes the refresh with the maxima of all slabs (hp2d_apply_refresh)
+    unsigned long long last_vbits, last_cbits;
+    int last_refreshed, last_unstable;
 };
 // StepScalars::status bits
 constexpr unsigned kStatusNumerical = 1u;   // a step was rejected (non-finite / negative depth)

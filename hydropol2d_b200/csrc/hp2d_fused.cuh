@@ -71,6 +71,8 @@ template <typename R> struct FusedArgs {
     int flag_timestep, adaptive, flag_critical, outlet_type, ga;   // ga: infiltration on (either model)
     int scheme;                  // flag_numerical_scheme: 1 Bates, 2 s-upwind, 3 s-centred
     unsigned int wait_polls;     // polls of a row-copy wait before it gives up (HP2D_TIMEOUT)
+    int own_r0, own_r1;          // rows whose cells enter the CFL maxima, ledgers and checks (a
+                                 // row slab's own rows; the others are halo rows of other slabs)
     unsigned int n_ctas;
     R stag_s2;
     const V4* stat;
@@ -469,7 +471,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     // map weights are read from shared memory where they are used
                     const R rr = MAP ? s_rs.at(a.rain, r, j[h], ny, nx) : RS.depth;
                     hh = hh + rr;
-                    const bool own = own_lane[h] && own_row;
+                    const bool own = own_lane[h] && own_row && r >= a.own_r0 && r < a.own_r1;
                     // uniform rain volume comes from the count of finite cells at the end
                     if (MAP && own && isfinite(hh)) rain_acc_r.add(rr);
                     if (INF) {
@@ -648,6 +650,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             }
             const int rm2 = r - 2;
             const bool frow = rm2 >= r0 && rm2 < r_end;
+            const bool mine = rm2 >= a.own_r0 && rm2 < a.own_r1;   // enters the reductions
 #pragma unroll
             for (int h = 0; h < CPL; ++h) {
                 if (own_lane[h] && frow) {
@@ -670,11 +673,11 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         hf3 = ho;
                         a.hf3[o] = ho;
                         a.qo[o] = qq;
-                        out_acc_r.add(qq * K.dt);
+                        if (mine) out_acc_r.add(qq * K.dt);
                         // the next step's clamp is skipped when an outlet cell (outside the
                         // infiltrating soils) stays negative after the next rain
                         // (Hydrological_Model.m:45-50); only outlet cells can end negative
-                        if (!(a.ga && (mt2[h] & 255u) != 255u) &&
+                        if (mine && !(a.ga && (mt2[h] & 255u) != 255u) &&
                             hn + (MAP ? s_rsn.at(a.rain, rm2, j[h], ny, nx) : s_rsn.depth) < R(-1e-11))
                             s_negn = 1;   // rare: kept in shared memory, not a register
                     }
@@ -690,12 +693,12 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     }
                     // a non-finite depth (NaN walls included, counted against the run's start)
                     // or one below -depth_tolerance
-                    nbad += (hn >= negtol) ? 0u : 1u;
+                    nbad += (hn >= negtol || !mine) ? 0u : 1u;
                     const R dm = dm2[h];
                     if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
                     // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
                     R vras = R(0);   // velocity raster: largest |face velocity| (refreshing_timestep.m:109-111)
-                    if (!quiet) {
+                    if (!quiet && mine) {
                         const R big = R(1e9);
                         const R vr = qxl2[h] == R(0) ? qxl2[h] : qdiv(qxl2[h], hfx2[h] < K.tol ? big : hfx2[h]);
                         const R vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
@@ -876,11 +879,17 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         const double delta = time_save - sc->tsp;
         sc->tsp = time_save;
         double tcr = sc->time_step * 60.0;   // refreshing_timestep.m:361-365
+        sc->last_vbits = vbits;
+        sc->last_cbits = cbits;
+        sc->last_refreshed = 0;
+        sc->last_unstable = 0;
         if ((delta > 0 || sc->k == 1) &&
             (sc->refresh_every <= 1 || sc->k == 1 || (sc->k - 1) % sc->refresh_every == 0)) {
             tcr = finalize_dt(vm, cm, a.res, a.alfa_min, a.alfa_max, a.min_dt, sc->max_dt, a.inc,
                               a.flag_timestep);
             sc->vmax_last = vm;
+            sc->last_refreshed = 1;
+            sc->last_unstable = tcr == a.min_dt;
             if (tcr == a.min_dt) {   // refreshing_timestep.m:357-359 (unstable)
                 sc->unstable += 1;
                 if (sc->dt_floor_stop) {
@@ -1281,7 +1290,8 @@ k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsign
 // keeps), and flags a non-finite depth in a cell of finite elevation (bad_domain).
 template <typename R>
 __global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>::V4* stat, int ny, int nx,
-                            RainDesc rain, int ga, double res, double tol_mm, double thr_mm, StepScalars* sc) {
+                            RainDesc rain, int ga, double res, double tol_mm, double thr_mm, StepScalars* sc,
+                            int own_r0, int own_r1) {
     const size_t n = size_t(ny) * nx;
     RainStep<R> RS;
     RS.make(rain, sc->rain_a, sc->rain_b);
@@ -1290,6 +1300,8 @@ __global__ void k_skip_flag(const typename Vec<R>::V4* st, const typename Vec<R>
     for (size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
         const R hc = st[c].x;
         const auto sr = stat[c];
+        const int ci = int(c / nx);
+        if (ci < own_r0 || ci >= own_r1) continue;   // a row slab counts its own rows only
         if (isfinite(hc)) ++fin;
         else {
             atomicAdd(&sc->n_bad0, 1ull);

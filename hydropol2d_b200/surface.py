@@ -280,6 +280,34 @@ class SurfaceFlow:
         """Test hook: the next ``attempts`` attempts of step ``k`` are rejected."""
         self._check(self._L.hp2d_inject_step_fault(self._h, int(k), int(attempts)))
 
+    # ---------------------------------------------------------------- row slabs
+    def set_owned_rows(self, row0: int, row1: int):
+        """This context holds one slab of a larger grid: rows [row0, row1) are its own, the rest
+        halo rows (hydropol2d_b200.slabs drives it)."""
+        self._check(self._L.hp2d_set_owned_rows(self._h, int(row0), int(row1)))
+
+    def step_maxima(self) -> tuple[int, int, int]:
+        """The last step's ordered speed^2 and celerity bits and the next step's clamp skip."""
+        v, c, s = C.c_uint64(), C.c_uint64(), C.c_int32()
+        self._check(self._L.hp2d_step_maxima(self._h, C.byref(v), C.byref(c), C.byref(s)))
+        return v.value, c.value, s.value
+
+    def apply_refresh(self, speed2_bits: int, celerity_bits: int, clamp_skip: int):
+        self._check(self._L.hp2d_apply_refresh(self._h, int(speed2_bits), int(celerity_bits), int(clamp_skip)))
+
+    def get_rows(self, row0: int, nrows: int) -> np.ndarray:
+        """State records {h, q_x, q_y, dmax} of rows [row0, row0 + nrows), (nrows, nx, 4)."""
+        out = np.empty((int(nrows), self.nx, 4), dtype=self.dtype)
+        self._check(self._L.hp2d_copy_rows(self._h, int(row0), int(nrows), out.ctypes.data_as(C.c_void_p), 0))
+        return out
+
+    def set_rows(self, row0: int, block: np.ndarray):
+        block = np.ascontiguousarray(block, dtype=self.dtype)
+        if block.ndim != 3 or block.shape[1:] != (self.nx, 4):
+            raise ValueError("rows must be an (nrows, nx, 4) array of state records")
+        self._check(self._L.hp2d_copy_rows(self._h, int(row0), block.shape[0],
+                                           block.ctypes.data_as(C.c_void_p), 1))
+
     # ---------------------------------------------------------------- outputs
     def download(self, field: str) -> np.ndarray:
         out = np.empty((self.ny, self.nx), dtype=np.float64)

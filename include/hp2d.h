@@ -353,6 +353,23 @@ hp2d_status hp2d_set_wait_limit(hp2d_ctx* ctx, int64_t polls);
  * rejected as if a depth had gone non-finite, so that the retry path runs on demand. */
 hp2d_status hp2d_inject_step_fault(hp2d_ctx* ctx, int64_t k, int32_t attempts);
 
+/* ---- one grid in row slabs (one context per slab; no counterpart in the reference) ---- */
+/* The context holds rows of a larger grid: its own rows [row0, row1) and up to two halo rows on
+ * each side that neighbouring slabs own (the draining limiter's dependency radius).  Its fused
+ * steps reduce the CFL maxima, the volume ledgers and the depth checks over the own rows only;
+ * after every step the caller combines the slabs' maxima (hp2d_step_maxima: the ordered bits of
+ * the largest speed^2 and wave-celerity term, and the next step's clamp skip), gives every slab
+ * the combined values (hp2d_apply_refresh redoes the step's time-step refresh with them), and
+ * copies each slab's two edge rows into its neighbours' halo rows (hp2d_copy_rows; the buffer is
+ * host or device memory).  The slabs then step as one grid, bit for bit.  No infiltration, rain
+ * maps, map records or retries in this mode (hydropol2d_b200.slabs drives it). */
+hp2d_status hp2d_set_owned_rows(hp2d_ctx* ctx, int32_t row0, int32_t row1);
+hp2d_status hp2d_step_maxima(hp2d_ctx* ctx, uint64_t* speed2_bits, uint64_t* celerity_bits, int32_t* clamp_skip);
+hp2d_status hp2d_apply_refresh(hp2d_ctx* ctx, uint64_t speed2_bits, uint64_t celerity_bits, int32_t clamp_skip);
+/* rows [row0, row0 + nrows) of the current state records ({h, q_x, q_y, dmax}, 4 values of the
+ * context's precision per cell) to buffer (into_state = 0) or from it (1) */
+hp2d_status hp2d_copy_rows(hp2d_ctx* ctx, int32_t row0, int32_t nrows, void* buffer, int32_t into_state);
+
 /* Temporal blocking (no counterpart in the reference; opt-in): steps_per_block = K in 2..4 makes
  * hp2d_fused_steps advance K steps per launch at the time step of the last refresh, which then
  * runs only on step 1 and on the steps k with (k - 1) % K == 0 (refreshing_timestep.m:17-368
