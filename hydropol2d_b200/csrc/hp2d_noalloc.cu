@@ -184,6 +184,14 @@ hp2d_status hp2d_cfl_dt_noalloc(int32_t ny, int32_t nx, double resolution, const
         s = g_noalloc_ptr[dev];
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the call ends with a read-back and a stream synchronisation, neither of which a stream
+    // under capture allows: refuse before anything enters the caller's capture
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return fail(HP2D_CUDA_ERROR, "cudaStreamIsCapturing", e);
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(HP2D_INVALID_ARG, "the stream is being captured: hp2d_cfl_dt_noalloc reads its result back "
+                                      "and synchronises the stream");
     const int nblocks = (ny + kNoAllocRowsPerBlock - 1) / kNoAllocRowsPerBlock;
     k_cfl_partials_noalloc<<<nblocks, kNoAllocThreads, 0, st>>>(ny, nx, resolution, params->depth_tolerance, q_x, q_y,
                                                                hf, params->flag_adaptive_timestepping,

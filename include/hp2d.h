@@ -438,7 +438,8 @@ hp2d_status hp2d_ensemble_run(hp2d_ensemble* ens, int64_t max_steps, int64_t* st
  *   q_x, q_y   ny*nx limited face discharge per unit width [m^2/s] (native fields 1, 2)
  *   hf         3*ny*nx face flow depth [m]: pages x, y and outlet, as Hf(:,:,1:3)
  *   stream     cudaStream_t to run on (NULL = default stream); the call ends by copying
- *              the two maxima to host memory and synchronising this stream
+ *              the two maxima to host memory and synchronising this stream, so a stream
+ *              under capture is refused with HP2D_INVALID_ARG (nothing enters the capture)
  *   time_step  [out] new time step [min]; max_velocity [out, nullable] [m/s]
  * On failure hp2d_noalloc_error() gives the message. */
 hp2d_status hp2d_cfl_dt_noalloc(int32_t ny, int32_t nx, double resolution, const hp2d_params* params,

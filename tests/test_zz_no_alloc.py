@@ -110,3 +110,37 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     st = L.hp2d_cfl_dt_noalloc(65537, 4, 1.0, C.byref(p), dummy, dummy, dummy, None, C.byref(ts), None)
     assert _abi.STATUS[st] == "HP2D_INVALID_ARG"
     assert "65536 rows" in L.hp2d_noalloc_error().decode()
+
+
+def test_noalloc_refuses_a_stream_under_capture():
+    """The call reads its result back and synchronises, which a capturing stream does not allow:
+    it refuses with HP2D_INVALID_ARG before touching the stream, and the capture stays valid."""
+    import torch
+    from hydropol2d_b200 import SurfaceFlow, _abi, build
+    from hydropol2d_b200 import synthetic as S
+    build.build()
+    L = _abi.lib()
+    case = S.vtilt_case(48, 32, 10.0)
+    sf = SurfaceFlow(*case.shape, case.resolution, "fp32", **case.params)
+    case.apply(sf)
+    sf.fused_steps(10)
+    qx, qy, hf = _inputs_from_context(sf, case)
+    first = _noalloc_dt(L, case, sf, qx, qy, hf)   # resolves the scratch outside any capture
+    x = torch.zeros(4, device="cuda:0")
+    g = torch.cuda.CUDAGraph()
+    ts = C.c_double()
+    with torch.cuda.graph(g):
+        stream = torch.cuda.current_stream().cuda_stream
+        st = L.hp2d_cfl_dt_noalloc(*case.shape, case.resolution, C.byref(sf.params), C.c_void_p(qx.data_ptr()),
+                                   C.c_void_p(qy.data_ptr()), C.c_void_p(hf.data_ptr()), C.c_void_p(stream),
+                                   C.byref(ts), None)
+        x.add_(1.0)
+    assert _abi.STATUS[st] == "HP2D_INVALID_ARG"
+    assert "captured" in L.hp2d_noalloc_error().decode()
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    assert x.cpu().tolist() == [2.0] * 4
+    assert _noalloc_dt(L, case, sf, qx, qy, hf) == first   # still usable afterwards
+    del g
+    sf.close()
