@@ -575,6 +575,24 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_split = {"setup_s": t1 - t0, "steps_s": t2 - t1, "readback_s": e2e_s - (t2 - t0)}
     n_out = sf.n_outlets
+    # host-copy rates of the boundary: a state upload (depth + two flux pages, FP64) and a map
+    # read-back (FP64), from and into page-locked and pageable host arrays (best of 3)
+    host_copies = {}
+    h_pg, of_pg, out_pg = np.array(h_mm), np.array(of), np.empty((ny, nx))
+    for route, (hh, oo, dst) in {"page_locked": (h_mm, of, depth_out),
+                                 "pageable": (h_pg, of_pg, out_pg)}.items():
+        up, down = [], []
+        for _ in range(3):
+            a = time.perf_counter()
+            sf.set_state(hh, oo)
+            b = time.perf_counter()
+            sf.download_into("depth", dst)
+            c = time.perf_counter()
+            up.append(b - a)
+            down.append(c - b)
+        host_copies[route] = {"state_upload_gbs": 24 * cells / min(up) / 1e9,
+                              "map_readback_gbs": 8 * cells / min(down) / 1e9}
+    del h_pg, of_pg, out_pg
     sf.close()
     # H2D per run: elevation and roughness (FP64) + the 4-byte meta word built on the host
     # (20 B/cell), depth and two flux pages (FP64, 24 B/cell).  D2H: the outlet hydrograph (4 B per
@@ -659,7 +677,8 @@ def main():
                 "d2h_bytes_per_step": d2h_per_step, "steps": args.steps, **e2e_split,
                 "includes": "context creation, static + 60-minute state upload from pinned host arrays, "
                             "per-step hydrograph and clock readback, final depth and dmax readback into "
-                            "pinned host arrays"},
+                            "pinned host arrays",
+                "host_copies": host_copies},
         "urban_c2": urban,
         "ensemble": ens,
         "gpu_launches": args.steps,

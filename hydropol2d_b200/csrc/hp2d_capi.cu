@@ -21,6 +21,7 @@
 #include <string>
 #include <mutex>
 #include <stdexcept>
+#include <thread>
 #include <vector>
 
 #include <cuda.h>
@@ -70,6 +71,110 @@ template <typename T> struct Dev {
         n = 0;
     }
     ~Dev() { free(); }
+};
+
+// Copies between a caller's host array and device memory.  Page-locked (or registered) caller
+// memory moves in one cudaMemcpyAsync at the link rate.  Pageable arrays of at least kMin bytes
+// are staged through this context's page-locked chunks by kLanes host threads, each with its
+// own stream and two chunks, so that one chunk's host memcpy overlaps the other's DMA; smaller
+// pageable arrays go in one copy, which the driver stages itself.  The chunks are allocated on
+// the first staged copy and kept with the context.
+struct HostStage {
+    static constexpr size_t kChunk = size_t(8) << 20;
+    static constexpr size_t kMin = size_t(32) << 20;
+    static constexpr int kLanes = 4;
+    struct Lane {
+        void* pin[2] = {nullptr, nullptr};
+        cudaStream_t s = nullptr;
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        cudaError_t err = cudaSuccess;
+    };
+    Lane lanes[kLanes];
+    bool ready = false;
+
+    ~HostStage() {
+        for (Lane& l : lanes) {
+            if (l.s) cudaStreamSynchronize(l.s);
+            for (int b = 0; b < 2; ++b) {
+                if (l.pin[b]) cudaFreeHost(l.pin[b]);
+                if (l.ev[b]) cudaEventDestroy(l.ev[b]);
+            }
+            if (l.s) cudaStreamDestroy(l.s);
+        }
+    }
+    static bool page_locked(const void* p) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+    }
+    void setup() {
+        if (ready) return;
+        for (Lane& l : lanes) {
+            HP_CK(cudaStreamCreateWithFlags(&l.s, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; ++b) {
+                HP_CK(cudaMallocHost(&l.pin[b], kChunk));
+                HP_CK(cudaEventCreateWithFlags(&l.ev[b], cudaEventDisableTiming));
+            }
+        }
+        ready = true;
+    }
+    // host -> device (to_device) or device -> host; returns after the data has landed.  Work
+    // queued on `main` before the call completes first.
+    void copy(void* dev, void* host, size_t bytes, bool to_device, cudaStream_t main, int device) {
+        if (bytes == 0) return;
+        const cudaMemcpyKind kind = to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+        if (bytes < kMin || page_locked(host)) {
+            HP_CK(to_device ? cudaMemcpyAsync(dev, host, bytes, kind, main) : cudaMemcpyAsync(host, dev, bytes, kind, main));
+            HP_CK(cudaStreamSynchronize(main));
+            return;
+        }
+        setup();
+        HP_CK(cudaStreamSynchronize(main));
+        const size_t nchunks = (bytes + kChunk - 1) / kChunk;
+        auto lane_work = [&](int t) {
+            Lane& l = lanes[t];
+            l.err = cudaSetDevice(device);
+            int use = 0, pb = -1;
+            size_t poff = 0, plen = 0;
+            for (size_t c = size_t(t); c < nchunks && l.err == cudaSuccess; c += kLanes) {
+                const size_t off = c * kChunk, len = std::min(kChunk, bytes - off);
+                const int b = use++ & 1;
+                char* d = static_cast<char*>(dev) + off;
+                char* h = static_cast<char*>(host) + off;
+                if (to_device) {   // the chunk's last DMA must be done before it is refilled
+                    if ((l.err = cudaEventSynchronize(l.ev[b])) != cudaSuccess) break;
+                    std::memcpy(l.pin[b], h, len);
+                    if ((l.err = cudaMemcpyAsync(d, l.pin[b], len, kind, l.s)) != cudaSuccess) break;
+                    if ((l.err = cudaEventRecord(l.ev[b], l.s)) != cudaSuccess) break;
+                } else {           // this chunk's DMA runs while the previous one is copied out
+                    if ((l.err = cudaMemcpyAsync(l.pin[b], d, len, kind, l.s)) != cudaSuccess) break;
+                    if ((l.err = cudaEventRecord(l.ev[b], l.s)) != cudaSuccess) break;
+                    if (pb >= 0) {
+                        if ((l.err = cudaEventSynchronize(l.ev[pb])) != cudaSuccess) break;
+                        std::memcpy(static_cast<char*>(host) + poff, l.pin[pb], plen);
+                    }
+                    pb = b;
+                    poff = off;
+                    plen = len;
+                }
+            }
+            if (!to_device && pb >= 0 && l.err == cudaSuccess) {
+                l.err = cudaEventSynchronize(l.ev[pb]);
+                if (l.err == cudaSuccess) std::memcpy(static_cast<char*>(host) + poff, l.pin[pb], plen);
+            }
+            const cudaError_t e = cudaStreamSynchronize(l.s);
+            if (l.err == cudaSuccess) l.err = e;
+        };
+        std::vector<std::thread> pool;
+        const int used = int(std::min<size_t>(kLanes, nchunks));
+        for (int t = 1; t < used; ++t) pool.emplace_back(lane_work, t);
+        lane_work(0);
+        for (auto& th : pool) th.join();
+        for (int t = 0; t < used; ++t) HP_CK(lanes[t].err);
+    }
 };
 
 // smallest x >= 0 whose correctly rounded square root reaches R(0.01): the stagnant
@@ -281,6 +386,10 @@ template <typename R> struct Impl : Base {
     }
 
     cudaStream_t st() const { return ctx->stream; }
+    HostStage stage;   // staging of pageable caller arrays
+    void h2d(void* dev, const void* host, size_t bytes) {
+        stage.copy(dev, const_cast<void*>(host), bytes, true, st(), ctx->device);
+    }
     void push_sc() { HP_CK(cudaMemcpyAsync(sc.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, st())); HP_CK(cudaStreamSynchronize(st())); }
     void pull_sc() { HP_CK(cudaMemcpyAsync(&hs, sc.p, sizeof(hs), cudaMemcpyDeviceToHost, st())); HP_CK(cudaStreamSynchronize(st())); }
 
@@ -384,8 +493,8 @@ template <typename R> struct Impl : Base {
             Dev<uint32_t> dm_;
             if (z_keep.n != n) z_keep.alloc(n);   // kept: setters that need the DEM fetch it
             dr_.alloc(n); dm_.alloc(n);
-            HP_CK(cudaMemcpyAsync(z_keep.p, z, n * sizeof(double), cudaMemcpyHostToDevice, st()));
-            HP_CK(cudaMemcpyAsync(dr_.p, rough, n * sizeof(double), cudaMemcpyHostToDevice, st()));
+            h2d(z_keep.p, z, n * sizeof(double));
+            h2d(dr_.p, rough, n * sizeof(double));
             upload(dm_.p, host_meta);
             // the unfused entry points' copies are extracted from the records on first use
             dzx.free(); dzy.free(); n2.free();
@@ -509,14 +618,14 @@ template <typename R> struct Impl : Base {
     hp2d_status set_state(const double* d, const double* outflow, const double* Imm) {
         pull_sc();
         {   // records built on the device from the caller's arrays
-            Dev<double> dd, dq;
-            dd.alloc(n);
-            HP_CK(cudaMemcpyAsync(dd.p, d, n * sizeof(double), cudaMemcpyHostToDevice, st()));
+            Dev<double> dq;
+            double* dd = readback_buffer();   // the read-back buffer doubles as upload staging
+            h2d(dd, d, n * sizeof(double));
             if (outflow) {
                 dq.alloc(2 * n);
-                HP_CK(cudaMemcpyAsync(dq.p, outflow, 2 * n * sizeof(double), cudaMemcpyHostToDevice, st()));
+                h2d(dq.p, outflow, 2 * n * sizeof(double));
             }
-            k_build_state<R><<<blocks_for(n), kThreads, 0, st()>>>(n, dd.p, outflow ? dq.p : nullptr, res,
+            k_build_state<R><<<blocks_for(n), kThreads, 0, st()>>>(n, dd, outflow ? dq.p : nullptr, res,
                                                                     st4[hs.cur].p);
             HP_CK(cudaGetLastError());
             HP_CK(cudaStreamSynchronize(st()));
@@ -1791,8 +1900,7 @@ template <typename R> struct Impl : Base {
     }
     void copy_out(const double* dev, double* out) {
         HP_CK(cudaGetLastError());
-        HP_CK(cudaMemcpyAsync(out, dev, n * sizeof(double), cudaMemcpyDeviceToHost, st()));
-        HP_CK(cudaStreamSynchronize(st()));
+        stage.copy(const_cast<double*>(dev), out, n * sizeof(double), false, st(), ctx->device);
     }
     void fetch_scaled(const R* src, double scale, double* out) {
         double* d = readback_buffer();
