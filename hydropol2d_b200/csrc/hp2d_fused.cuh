@@ -51,8 +51,13 @@ constexpr int kStages = HP2D_STAGES;   // shared-memory ring depth of the row pi
 #endif
 constexpr int kRowUnroll = HP2D_ROW_UNROLL;   // row-loop unroll (register renaming of the window)
 #ifndef HP2D_FACE_ILP
-#define HP2D_FACE_ILP 0   // 1: the faces of a row as interleaved, branch-free momentum updates
+#define HP2D_FACE_ILP 0   // 1: interleaved faces in every instantiation, -1: in none
 #endif
+// The faces of a row as interleaved, branch-free momentum updates (face_geom + face_momentum)
+// rather than one face_flux after the other: faster on the infiltration and rain-map
+// instantiations (19.4 vs 15.7 GCUPS on the 2048^2 Green-Ampt grid with 64 x 64 rain maps),
+// slower on the plain ones (37.6 vs 39.1 wet, 92.6 vs 96.5 on the 60-minute dam-break).
+template <int INF, bool MAP> constexpr bool kFaceIlp = HP2D_FACE_ILP > 0 || (HP2D_FACE_ILP == 0 && (INF != 0 || MAP));
 
 // dynamic shared memory of k_fused_step: per warp kStages x (2 records x 32*CPL cells)
 template <typename R, int CPL = 1> constexpr size_t fused_smem_bytes(int nt) {
@@ -569,7 +574,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     for (int h = 0; h < CPL; ++h)
                         if (!(j[h] >= 1 && j[h] + 1 < nx)) qxa[h] = qxb[h] = R(0);
                 }
-#if HP2D_FACE_ILP
+                if constexpr (kFaceIlp<INF, MAP>) {
                 // (B) and (C) interleaved: the geometry of the 2 x CPL faces, then -- unless no
                 // lane of the warp has a wet one -- their momentum updates without branches
                 R Sx[CPL], Sy[CPL], ya[CPL], yb[CPL];
@@ -601,7 +606,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                                                          a.scheme, ya[h], yb[h]);
                     }
                 }
-#else
+                } else {
 #pragma unroll
                 for (int h = 0; h < CPL; ++h)
                     if (col_ok[h] && rok)
@@ -620,7 +625,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         face_flux<R, false, SCH>(hT1[h], hT0[h], S[h].y, X[h].z, S[h].z, K, a.flag_critical, hfy0[h],
                                                  qyu0[h], a.scheme, ya, yb);
                     }
-#endif
+                }
                 // (D) donor scale of (r-1, j)
                 R qxu1_left[CPL];
                 left_of<R, CPL>(qxu1, qxu1_left, lane);

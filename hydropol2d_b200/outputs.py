@@ -12,6 +12,12 @@ names them, and the save_map_hydro_<store>.mat chunks of save_output_maps.m.
 * ``write_map_chunks``: the depth records [mm] in files of ``saver_memory_maps`` maps, variable
   ``Maps.Hydro.d`` (ny, nx, k) (save_output_maps.m:565-580).  The reference saves MAT 7.3
   (HDF5); these are MAT 5 files, which MATLAB's ``load`` reads the same way.
+* ``write_timeseries_netcdf``: one time series of maps in one NetCDF file with the variables,
+  dimensions and CF attributes of initializeTimeSeriesNetCDF / appendTimeSliceToNetCDF
+  (post_processing.m:2811-3154, :3236-3248): x, y (cell centres, y ascending, so the maps' rows
+  are flipped), time, a scalar crs, and the data variable (time, y, x) in single precision.
+  The reference writes the netcdf4 (HDF5) flavour with deflate; this writes the classic 64-bit
+  offset flavour (no HDF5 library here), which every NetCDF reader takes.
 """
 from __future__ import annotations
 
@@ -198,10 +204,70 @@ def write_map_chunks(directory: str, depths_mm, saver_memory_maps: int = 12, fir
     return out
 
 
-def export_run(sf, directory: str, geo: GeoRef, time_records=None, depth_wse: float = 0.01) -> list[str]:
+def write_timeseries_netcdf(path: str, maps, times, geo: GeoRef, var_name: str = "flood_depth",
+                            long_name: str = "Flood depth", units: str = "m",
+                            time_units: str = "hours since simulation start", calendar: str = "none",
+                            fill_value: float = float("nan")) -> str:
+    """``maps``: (nt, ny, nx) in the variable's units, row 0 the northern row; ``times`` in
+    ``time_units``.  Projected coordinates (metres) from ``geo``."""
+    from scipy.io import netcdf_file
+    maps = np.asarray(maps, dtype=np.float64)
+    if maps.ndim != 3:
+        raise ValueError("maps must be (nt, ny, nx)")
+    nt, ny, nx = maps.shape
+    times = np.asarray(times, dtype=np.float64).reshape(-1)
+    if times.size != nt:
+        raise ValueError("one time per map")
+    # intrinsicToWorld of the cell centres of a map-cells reference whose columns start north
+    x = geo.x_ul + (np.arange(1, nx + 1) - 0.5) * geo.res
+    y = geo.y_ul - (np.arange(1, ny + 1) - 0.5) * geo.res
+    flip = ny >= 2 and y[1] < y[0]
+    if flip:
+        y = y[::-1]
+    if os.path.exists(path):
+        os.remove(path)
+    f = netcdf_file(path, "w", version=2)
+    try:
+        f.createDimension("x", nx)
+        f.createDimension("y", ny)
+        f.createDimension("time", nt)
+        vx = f.createVariable("x", "d", ("x",))
+        vy = f.createVariable("y", "d", ("y",))
+        vt = f.createVariable("time", "d", ("time",))
+        crs = f.createVariable("crs", "i", ())
+        var = f.createVariable(var_name, "f", ("time", "y", "x"))
+        vx[:] = x
+        vy[:] = y
+        vt[:] = times
+        crs.data[()] = 0   # (assignValue indexes a 0-d array with [:] under numpy 2)
+        for v, std, lng, ax in ((vx, "projection_x_coordinate", "x coordinate of projection", "X"),
+                                (vy, "projection_y_coordinate", "y coordinate of projection", "Y")):
+            v.standard_name, v.long_name, v.units, v.axis = std, lng, "m", ax
+        vt.standard_name, vt.long_name, vt.units, vt.calendar, vt.axis = "time", "time", time_units, calendar, "T"
+        crs.grid_mapping_name = "transverse_mercator"
+        crs.long_name = "projected"
+        if geo.epsg is not None:
+            crs.epsg_code = f"EPSG:{int(geo.epsg)}"
+        var._FillValue = np.float32(fill_value)
+        var.long_name, var.units = long_name, units
+        var.coordinates = "x y time"
+        var.grid_mapping = "crs"
+        for i in range(nt):   # appendTimeSliceToNetCDF: single precision, rows flipped
+            z = maps[i].astype(np.float32)
+            var[i] = z[::-1] if flip else z
+        f.title = f"{long_name} time series"
+        f.source = "HydroPol2D export"
+    finally:
+        f.close()
+    return path
+
+
+def export_run(sf, directory: str, geo: GeoRef, time_records=None, depth_wse: float = 0.01,
+               netcdf: bool = False) -> list[str]:
     """All of the above for a ``SurfaceFlow`` after its run: the map records (when kept), named
     by ``time_records`` [min] as post_processing.m names record i (else by the clock of the
-    step that took it), the maximum depth, and the velocity and hazard maxima (when tracked)."""
+    step that took it), the maximum depth, and the velocity and hazard maxima (when tracked);
+    with ``netcdf`` also the records' time series (Flood_Depths_timeseries.nc, hours)."""
     from ._abi import HP2DError
     out = []
     recs = [sf.download_map_record(i) for i in range(sf.map_records())]
@@ -210,6 +276,10 @@ def export_run(sf, directory: str, geo: GeoRef, time_records=None, depth_wse: fl
         times = [t for _, t in recs] if time_records is None else list(time_records)[:len(recs)]
         out += export_depth_records(directory, geo, depths, times)
         out += write_map_chunks(directory, depths)
+        if netcdf:   # post_processing.m:1397-1410, :1527-1547 (flag_wse = 0)
+            out.append(write_timeseries_netcdf(os.path.join(directory, "Flood_Depths_timeseries.nc"),
+                                               np.stack(depths) / 1000.0, np.asarray(times, dtype=float) / 60.0,
+                                               geo))
     vmax = hz = None
     try:
         vmax, hz = sf.download("vmax"), sf.download("hazard_max")

@@ -41,3 +41,25 @@ def test_export_run(tmp_path, hp2d_lib):
     r, _ = O.read_geotiff(os.path.join(str(tmp_path), "Flood_Depths_t_0.033333_h.tif"))
     assert np.array_equal(r, rec / 1000.0)
     g.close()
+
+
+def test_export_run_netcdf_time_series(tmp_path, hp2d_lib):
+    from scipy.io import netcdf_file
+    from hydropol2d_b200 import SurfaceFlow
+    case = S.dambreak_case(48, 128, 5.0, seed=3, hours=0.1)
+    g = SurfaceFlow(*case.shape, case.resolution, "fp32", **case.params)
+    case.apply(g)
+    records = np.array([1.0, 2.0, 3.0, 4.5])
+    g.set_map_records(records, 8)
+    g.run()
+    geo = O.GeoRef(x_ul=300000.0, y_ul=7500000.0, res=case.resolution, epsg=31983)
+    files = O.export_run(g, str(tmp_path), geo, time_records=records, netcdf=True)
+    nc = [f for f in files if f.endswith("Flood_Depths_timeseries.nc")]
+    assert len(nc) == 1
+    with netcdf_file(nc[0], "r", mmap=False) as f:
+        assert list(f.variables["time"][:]) == list(records / 60.0)
+        z = np.array(f.variables["flood_depth"][:])[:, ::-1, :]
+        for i in range(4):
+            rec, _ = g.download_map_record(i)
+            assert np.array_equal(z[i], (rec / 1000.0).astype(np.float32))
+    g.close()

@@ -75,3 +75,31 @@ def test_depth_records_and_chunks(tmp_path):
     assert m.shape == (3, 4, 12) and m[0, 0, 0] == 12.0 and m[0, 0, 11] == 23.0
     last = loadmat(chunks[2], simplify_cells=True)["Maps"]["Hydro"]["d"]
     assert last.shape == (3, 4, 2)
+
+
+def test_timeseries_netcdf_layout(tmp_path):
+    """Dimensions, coordinates (cell centres, y ascending), flipped rows, single precision, the
+    fill value and the CF attributes of initializeTimeSeriesNetCDF (post_processing.m:2811-3154)."""
+    from scipy.io import netcdf_file
+    from hydropol2d_b200.outputs import GeoRef, write_timeseries_netcdf
+    rng = np.random.default_rng(4)
+    maps = rng.uniform(0, 2, (3, 5, 7))
+    maps[1, 0, 0] = np.nan
+    geo = GeoRef(x_ul=1000.0, y_ul=5000.0, res=10.0, epsg=31983)
+    p = write_timeseries_netcdf(str(tmp_path / "Flood_Depths_timeseries.nc"), maps, [0.5, 1.0, 1.5], geo)
+    with netcdf_file(p, "r", mmap=False) as f:
+        assert f.dimensions == {"x": 7, "y": 5, "time": 3}
+        assert np.allclose(f.variables["x"][:], 1005.0 + 10.0 * np.arange(7))
+        assert np.allclose(f.variables["y"][:], 4955.0 + 10.0 * np.arange(5))   # ascending
+        assert list(f.variables["time"][:]) == [0.5, 1.0, 1.5]
+        v = f.variables["flood_depth"]
+        assert v.dimensions == ("time", "y", "x") and v.data.dtype.newbyteorder("=") == np.float32
+        got = np.array(v[:])
+        assert np.array_equal(got[:, ::-1, :], maps.astype(np.float32), equal_nan=True)   # north row first again
+        assert np.isnan(got[1, -1, 0])
+        assert v.units == b"m" and v.grid_mapping == b"crs" and v.coordinates == b"x y time"
+        assert np.isnan(v._FillValue)
+        assert f.variables["time"].units == b"hours since simulation start"
+        assert f.variables["crs"].epsg_code == b"EPSG:31983"
+        assert f.variables["x"].standard_name == b"projection_x_coordinate"
+        assert f.title == b"Flood depth time series" and f.source == b"HydroPol2D export"
