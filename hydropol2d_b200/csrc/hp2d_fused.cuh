@@ -371,10 +371,17 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
         R hT1[CPL], hT2[CPL], qxu1[CPL], qyu1[CPL], hfx1[CPL], hfx2[CPL], hfy1[CPL], hfy2[CPL];
         R sc2[CPL], qxl2[CPL], qyl2[CPL], dm1[CPL], dm2[CPL];
         R qyp1[CPL];   // schemes 2/3: previous q_y of the row before
+        // velocity of the face below row r-3, computed by the (F) of row r-3: after the shift it
+        // is the face above row r-2 (qyl2 / hfy2 then hold the values it was computed from), so
+        // the next (F) takes it instead of dividing again; vcar_ok (warp-uniform) says whether
+        // the last row's (F) computed it
+        R vcar[CPL];
+        bool vcar_ok = false;
         unsigned mt1[CPL], mt2[CPL];
 #pragma unroll
         for (int h = 0; h < CPL; ++h) {
             qyp1[h] = R(0);
+            vcar[h] = R(0);
             hT1[h] = hT2[h] = qxu1[h] = qyu1[h] = R(0);
             hfx1[h] = hfx2[h] = hfy1[h] = hfy2[h] = R(0);
             sc2[h] = R(1);
@@ -547,6 +554,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                         mt2[h] = mt1[h]; mt1[h] = meta[h];
                         if (SCH) qyp1[h] = X[h].z;
                     }
+                    vcar_ok = false;
                     continue;
                 }
             }
@@ -706,8 +714,11 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     if (!quiet && mine) {
                         const R big = R(1e9);
                         const R vr = qxl2[h] == R(0) ? qxl2[h] : qdiv(qxl2[h], hfx2[h] < K.tol ? big : hfx2[h]);
-                        const R vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
+                        R vu;
+                        if (vcar_ok) vu = vcar[h];
+                        else vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
                         const R vb = qyl1[h] == R(0) ? qyl1[h] : qdiv(qyl1[h], hfy1[h] < K.tol ? big : hfy1[h]);
+                        vcar[h] = vb;
                         if (INFL) vras = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb));
                         const R rc = j[h] == 0 ? R(0.5) * vr : vr;
                         const R uc = R(0.5) * (vu + vb);
@@ -744,6 +755,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     }
                 }
             }
+            vcar_ok = !quiet && mine && frow;
             if (flg && lane == 0) dfl[r - 2] = 0;   // rewritten: no longer known dry
             // (G) shift the window down one row
 #pragma unroll
