@@ -37,7 +37,7 @@ NATIVE = {
 EXPORTS = [
     "hp2d_create", "hp2d_destroy", "hp2d_last_error", "hp2d_create_error",
     "hp2d_upload_static", "hp2d_set_soil", "hp2d_set_soil_vg", "hp2d_set_state", "hp2d_set_clock", "hp2d_set_rain_clock",
-    "hp2d_set_rain_uniform", "hp2d_set_rain_maps", "hp2d_set_rain_gauges", "hp2d_set_inflow", "hp2d_set_stage",
+    "hp2d_set_rain_uniform", "hp2d_set_rain_maps", "hp2d_set_rain_maps_end_stamped", "hp2d_set_rain_gauges", "hp2d_set_inflow", "hp2d_set_stage",
     "hp2d_set_reservoirs", "hp2d_set_hazard_tracking", "hp2d_set_dry_skip",
     "hp2d_set_map_records", "hp2d_set_map_records_host", "hp2d_map_records", "hp2d_download_map_record", "hp2d_hydrology_step", "hp2d_li_step",
     "hp2d_cfl_dt", "hp2d_track_maxima", "hp2d_fused_steps", "hp2d_fused_steps_timed",
@@ -157,6 +157,8 @@ def lib() -> C.CDLL:
                              P(C.c_int32), P(C.c_int32), P(C.c_int32)], C.c_int),
         "hp2d_set_rain_uniform": ([vp, C.c_int32, dp, dp], C.c_int),
         "hp2d_set_rain_maps": ([vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_float), C.c_double], C.c_int),
+        "hp2d_set_rain_maps_end_stamped": ([vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_float), P(C.c_double),
+                                            C.c_double], C.c_int),
         "hp2d_hydrology_step": ([vp, C.c_double], C.c_int),
         "hp2d_li_step": ([vp, C.c_double], C.c_int),
         "hp2d_cfl_dt": ([vp, dp, dp], C.c_int),

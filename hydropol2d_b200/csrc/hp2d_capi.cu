@@ -713,6 +713,43 @@ template <typename R> struct Impl : Base {
         maps.alloc(cnt);
         upload(maps.p, std::vector<float>(rate, rate + cnt));
         rain.n_maps = nm; rain.my = my; rain.mx = mx; rain.map_dt = map_dt; rain.maps = maps.p;
+        rain.map_t = nullptr;
+        rain.n_uniform = 0;
+        invalidate_graph();
+        dirty = true;
+        return HP2D_OK;
+    }
+
+    // End-stamped input rain maps (flag_input_rainfall_map = 1): map m holds over
+    // [t_end[m-1], t_end[m]), the first one from t_end[0] - dt_force
+    Dev<double> map_edges;
+    hp2d_status set_rain_maps_end_stamped(int32_t nm, int32_t my, int32_t mx, const float* rate, const double* t_end,
+                                          double dt_force) {
+        if (nm <= 0 || my <= 0 || mx <= 0 || !rate || !t_end || !(dt_force >= 0)) {
+            ctx->err = "bad input rain maps";
+            return HP2D_INVALID_ARG;
+        }
+        std::vector<double> e(size_t(nm) + 1);
+        e[0] = t_end[0] - dt_force;
+        for (int q = 0; q < nm; ++q) e[size_t(q) + 1] = t_end[q];
+        for (int q = 0; q < nm; ++q) {
+            if (!(e[size_t(q) + 1] >= e[q]) || !std::isfinite(e[q]) || !std::isfinite(e[size_t(q) + 1])) {
+                ctx->err = "map end times must be finite and non-decreasing";
+                return HP2D_INVALID_ARG;
+            }
+            // an interval shorter than a step could make a step's rain span three maps
+            if (e[size_t(q) + 1] > e[q] && (e[size_t(q) + 1] - e[q]) * 60.0 < ctx->p.max_time_step) {
+                ctx->err = "rain map interval shorter than max_time_step";
+                return HP2D_INVALID_ARG;
+            }
+        }
+        size_t cnt = size_t(nm) * my * mx;
+        maps.alloc(cnt);
+        upload(maps.p, std::vector<float>(rate, rate + cnt));
+        map_edges.alloc(e.size());
+        upload(map_edges.p, e);
+        rain.n_maps = nm; rain.my = my; rain.mx = mx; rain.map_dt = 0.0; rain.maps = maps.p;
+        rain.map_t = map_edges.p;
         rain.n_uniform = 0;
         invalidate_graph();
         dirty = true;
@@ -738,6 +775,7 @@ template <typename R> struct Impl : Base {
         HP_CK(cudaGetLastError());
         HP_CK(cudaStreamSynchronize(st()));
         rain.n_maps = nt; rain.my = ny; rain.mx = nx; rain.map_dt = dt; rain.maps = maps.p;
+        rain.map_t = nullptr;
         rain.n_uniform = 0;
         invalidate_graph();
         dirty = true;
@@ -2511,6 +2549,11 @@ hp2d_status hp2d_set_rain_gauges(hp2d_ctx* ctx, int32_t n_gauges, const double* 
 
 hp2d_status hp2d_set_rain_clock(hp2d_ctx* ctx, double rain_t0, double rain_t1, double t_previous) {
     return with_impl(ctx, [&](auto& m) { return m.set_rain_clock(rain_t0, rain_t1, t_previous); });
+}
+
+hp2d_status hp2d_set_rain_maps_end_stamped(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx, const float* rate,
+                                           const double* t_end, double dt_force) {
+    return with_impl(ctx, [&](auto& m) { return m.set_rain_maps_end_stamped(n_maps, my, mx, rate, t_end, dt_force); });
 }
 
 hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx, const float* rate, double map_dt) {

@@ -331,6 +331,7 @@ struct RainDesc {
     int n_maps, my, mx;
     double map_dt;           // [min]
     const float* maps;       // n_maps * my * mx
+    const double* map_t;     // null: map m over [m, m+1) x map_dt; else over [map_t[m], map_t[m+1]) [min]
 };
 
 // Integral [mm/h x min] over [a, b] of the uniform series: rate q holds from t_start[q] up to
@@ -473,8 +474,9 @@ __device__ __host__ inline unsigned outlet_ord(unsigned meta) { return (meta & k
 
 // Rain of one step over the clock interval [a, b] [min]: a uniform depth, or the (at most
 // two) rate maps overlapping the interval with their overlaps (map m holds over
-// [m, m+1) x map_dt, nothing after the last map; update_spatial_BC.m:1287-1359).  Depths
-// are rate [mm/h] x overlap [min] / 60 [mm], in metres.
+// [m, m+1) x map_dt, or over [map_t[m], map_t[m+1]) for end-stamped input maps, nothing
+// after the last map; update_spatial_BC.m:1287-1359).  Depths are rate [mm/h] x
+// overlap [min] / 60 [mm], in metres.
 template <typename R> struct RainStep {
     R depth;       // uniform series [m]
     int nm;        // maps overlapping the interval (0..2)
@@ -486,9 +488,21 @@ template <typename R> struct RainStep {
         m[0] = m[1] = 0;
         w[0] = w[1] = R(0);
         if (!rd.n_maps || !(b > a)) return;
-        const int m0 = max(0, int(floor(a / rd.map_dt)) - 1);
+        int m0;
+        if (rd.map_t) {   // the first map that ends after a
+            int lo = 0, hi = rd.n_maps;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (rd.map_t[mid + 1] > a) hi = mid;
+                else lo = mid + 1;
+            }
+            m0 = lo;
+        } else {
+            m0 = max(0, int(floor(a / rd.map_dt)) - 1);
+        }
         for (int q = m0; q < rd.n_maps && nm < 2; ++q) {
-            const double lo = q * rd.map_dt, hi = (q + 1) * rd.map_dt;
+            const double lo = rd.map_t ? rd.map_t[q] : q * rd.map_dt;
+            const double hi = rd.map_t ? rd.map_t[q + 1] : (q + 1) * rd.map_dt;
             if (lo >= b) break;
             const double ov = fmin(b, hi) - fmax(a, lo);
             if (ov > 0.0) {

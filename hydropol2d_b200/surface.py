@@ -209,6 +209,21 @@ class SurfaceFlow:
         r = _f64(rate).ravel()
         self._check(self._L.hp2d_set_rain_uniform(self._h, int(t.size), _dp(t), _dp(r)))
 
+    def set_rain_maps_end_stamped(self, maps, t_end, dt_force: float | None = None):
+        """Input rain maps [mm/h] (n, my, mx), map m over [t_end[m-1], t_end[m]) [min], the first
+        from t_end[0] - dt_force (default t_end[1] - t_end[0], or 0 for one map)."""
+        m = np.ascontiguousarray(maps, dtype=np.float32)
+        if m.ndim == 2:
+            m = m[None]
+        te = np.ascontiguousarray(t_end, dtype=np.float64).reshape(-1)
+        if te.size != m.shape[0]:
+            raise ValueError("one end time per map")
+        if dt_force is None:
+            dt_force = float(te[1] - te[0]) if te.size >= 2 and te[1] > te[0] else 0.0
+        self._check(self._L.hp2d_set_rain_maps_end_stamped(self._h, m.shape[0], m.shape[1], m.shape[2],
+                                                           m.ctypes.data_as(C.POINTER(C.c_float)), _dp(te),
+                                                           float(dt_force)))
+
     def set_rain_maps(self, maps, map_dt: float):
         m = np.ascontiguousarray(maps, dtype=np.float32)
         nm, my, mx = m.shape

@@ -202,6 +202,16 @@ hp2d_status hp2d_set_rain_uniform(hp2d_ctx* ctx, int32_t n, const double* t_star
                                   const double* rate);
 hp2d_status hp2d_set_rain_maps(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx,
                                const float* rate, double map_dt);
+/* Input rain maps (flags.flag_input_rainfall_map = 1; update_spatial_BC.m:497-517 with
+ * localAverageInputRainMapOverStep :1287-1359): end-stamped rate maps [mm/h], map m holding
+ * over [t_end[m-1], t_end[m]) [min] and the first one from t_end[0] - dt_force (the reference's
+ * Input_Rainfall.time and dt_force, by default t_end[1] - t_end[0]), nothing after the last.
+ * The maps are given already aligned to the grid (my x mx, bilinearly sampled as above; at
+ * my = ny, mx = nx each cell takes its own value): hydropol2d_b200.raster_rain reads GeoTIFF
+ * rasters and aligns them as raster_cutter.m does.  Each non-empty interval must be at least
+ * params.max_time_step long. */
+hp2d_status hp2d_set_rain_maps_end_stamped(hp2d_ctx* ctx, int32_t n_maps, int32_t my, int32_t mx,
+                                           const float* rate, const double* t_end, double dt_force);
 
 /* Rain from gauges (flags.flag_spatial_rainfall = 1; update_spatial_BC.m:494-517 with
  * Rainfall_Interpolator.m / idw_function.m): n_gauges at eastings/northings x_gauge, y_gauge

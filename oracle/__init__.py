@@ -75,6 +75,8 @@ def _load():
                                    P(C.c_int32), dp], C.c_int),
             "oracle_set_rain_uniform": ([vp, C.c_int32, dp, dp], C.c_int),
             "oracle_set_rain_maps": ([vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_float), C.c_double], C.c_int),
+            "oracle_set_rain_maps_end_stamped": ([vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_float), P(C.c_double),
+                                                  C.c_double], C.c_int),
             "oracle_hydrology_step": ([vp, C.c_double], C.c_int),
             "oracle_li_step": ([vp, C.c_double], C.c_int),
             "oracle_cfl_dt": ([vp, C.c_double, dp, dp], C.c_int),
@@ -213,6 +215,17 @@ class KernelFormOracle:
         m = np.ascontiguousarray(maps, dtype=np.float32)
         nm, my, mx = m.shape
         self._L.oracle_set_rain_maps(self._h, nm, my, mx, m.ctypes.data_as(C.POINTER(C.c_float)), float(map_dt))
+
+    def set_rain_maps_end_stamped(self, maps, t_end, dt_force=None):
+        m = np.ascontiguousarray(maps, dtype=np.float32)
+        if m.ndim == 2:
+            m = m[None]
+        te = np.ascontiguousarray(t_end, dtype=np.float64).reshape(-1)
+        if dt_force is None:
+            dt_force = float(te[1] - te[0]) if te.size >= 2 and te[1] > te[0] else 0.0
+        nm, my, mx = m.shape
+        self._L.oracle_set_rain_maps_end_stamped(self._h, nm, my, mx, m.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 _dp(te), float(dt_force))
 
     def hydrology_step(self, time_step):
         self._L.oracle_hydrology_step(self._h, float(time_step))

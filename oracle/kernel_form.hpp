@@ -150,6 +150,7 @@ public:
     std::vector<double> rain_t, rain_r;
     int n_maps = 0, my = 0, mx = 0;
     double map_dt = 5.0;
+    std::vector<double> map_t;   // empty: map m over [m, m+1) x map_dt; else [map_t[m], map_t[m+1])
     std::vector<float> maps;
     // state
     std::vector<R> h, qx, qy, I, T, dmax, arrival;
@@ -289,8 +290,9 @@ public:
     // the piecewise-constant rate over it (localAverageRateOverStep x interval,
     // update_spatial_BC.m:1131-1184; maps :1287-1359) / 60 -> mm, here in metres.  Uniform
     // rates hold from rain_t[q] up to rain_t[q+1] (the last for ever); map m holds over
-    // [m, m+1) x map_dt and nothing after the last map; an interval overlaps at most two maps
-    // (map_dt >= max_time_step, checked by the library).
+    // [m, m+1) x map_dt (or over [map_t[m], map_t[m+1]) for end-stamped input maps,
+    // update_spatial_BC.m:497-517) and nothing after the last map; an interval overlaps at most
+    // two maps (every map interval >= max_time_step, checked by the library).
     struct StepRain {
         R depth = R(0);        // uniform [m]
         int nm = 0;
@@ -313,9 +315,15 @@ public:
             s.depth = R(acc / 60000.0);
         }
         if (n_maps > 0 && b > a) {
-            const int m0 = std::max(0, int(std::floor(a / map_dt)) - 1);
+            int m0 = 0;
+            if (!map_t.empty()) {   // the first map that ends after a
+                while (m0 < n_maps && !(map_t[size_t(m0) + 1] > a)) ++m0;
+            } else {
+                m0 = std::max(0, int(std::floor(a / map_dt)) - 1);
+            }
             for (int q = m0; q < n_maps && s.nm < 2; ++q) {
-                const double lo = q * map_dt, hi = (q + 1) * map_dt;
+                const double lo = map_t.empty() ? q * map_dt : map_t[size_t(q)];
+                const double hi = map_t.empty() ? (q + 1) * map_dt : map_t[size_t(q) + 1];
                 if (lo >= b) break;
                 const double ov = std::fmin(b, hi) - std::fmax(a, lo);
                 if (ov > 0.0) {

@@ -586,6 +586,49 @@ def average_rate_over_step(times_end, values, t0: float, t1: float) -> float:
     return acc / (t1 - t0)
 
 
+def advance_end_stamped_cursor(times, t_now: float, cursor: int) -> int:
+    """localAdvanceEndStampedCursor (update_spatial_BC.m:1095-1129), 1-based as in MATLAB."""
+    n = len(times)
+    cursor = min(max(1, cursor), n)
+    while cursor < n and t_now > times[cursor - 1]:
+        cursor += 1
+    return cursor
+
+
+def average_input_rain_map_over_step(times_end, maps, t0: float, t1: float, cursor: int = 1,
+                                     dt_force: float | None = None):
+    """localAverageInputRainMapOverStep (update_spatial_BC.m:1287-1359) on maps already read and
+    aligned ((n, ny, nx) [mm/h]): the time-averaged rate map over [t0, t1] and the new cursor.
+    Map i holds from times_end[i-1] (times_end[0] - dt_force for the first) to times_end[i];
+    dt_force defaults to localEstimateConstantDt (:1240-1253)."""
+    times = np.asarray(times_end, dtype=np.float64)
+    maps = np.asarray(maps, dtype=np.float64)
+    zero = np.zeros(maps.shape[1:])
+    if times.size == 0 or t1 <= t0:
+        return zero, cursor
+    dt_total = t1 - t0
+    cursor = advance_end_stamped_cursor(times, t0, cursor)
+    if dt_force is None:
+        dt_force = times[1] - times[0] if times.size >= 2 else 0.0
+        if not np.isfinite(dt_force) or dt_force <= 0:
+            dt_force = 0.0
+    ts = times[0] - dt_force if cursor == 1 else times[cursor - 2]
+    te = times[cursor - 1]
+    if t0 >= ts and t1 <= te:   # fast path: the step inside one forcing interval
+        return maps[cursor - 1].copy(), cursor
+    acc = zero.copy()
+    for i in range(cursor, times.size + 1):
+        ts = times[0] - dt_force if i == 1 else times[i - 2]
+        te = times[i - 1]
+        ov = max(0.0, min(t1, te) - max(t0, ts))
+        if ov > 0:
+            acc = acc + ov * maps[i - 1]
+        if te >= t1:
+            cursor = i
+            break
+    return acc / dt_total, cursor
+
+
 def idw_rain_maps(x_gauge, y_gauge, rates, ny: int, nx: int, res: float, x_ul: float = 0.0,
                   y_ul: float = 0.0) -> np.ndarray:
     """Rainfall_Interpolator.m + idw_function.m (p = 2, Euclidean norm, no radius) for every

@@ -128,6 +128,21 @@ int oracle_set_rain_maps(oracle_model* m, int32_t nm, int32_t my, int32_t mx, co
                          double map_dt) {
     return dispatch(m, [&](auto& M) {
         M.n_maps = nm; M.my = my; M.mx = mx; M.map_dt = map_dt;
+        M.map_t.clear();
+        M.maps.assign(rate, rate + size_t(nm) * my * mx);
+        return 0;
+    });
+}
+
+// end-stamped input maps: map q over [t_end[q-1], t_end[q]), the first from t_end[0] - dt_force
+// (localAverageInputRainMapOverStep, update_spatial_BC.m:1287-1359)
+int oracle_set_rain_maps_end_stamped(oracle_model* m, int32_t nm, int32_t my, int32_t mx, const float* rate,
+                                     const double* t_end, double dt_force) {
+    return dispatch(m, [&](auto& M) {
+        M.n_maps = nm; M.my = my; M.mx = mx; M.map_dt = 0.0;
+        M.map_t.assign(size_t(nm) + 1, 0.0);
+        M.map_t[0] = t_end[0] - dt_force;
+        for (int q = 0; q < nm; ++q) M.map_t[size_t(q) + 1] = t_end[q];
         M.maps.assign(rate, rate + size_t(nm) * my * mx);
         return 0;
     });

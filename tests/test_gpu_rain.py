@@ -93,3 +93,65 @@ def test_maps_shorter_than_the_largest_step_are_rejected(hp2d_lib):
     with pytest.raises(HP2DError):
         g.set_rain_maps(np.zeros((2, 4, 4), np.float32), 0.1)   # 6 s < max_time_step 10 s
     g.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_end_stamped_input_maps(precision, hp2d_lib, oracle_lib):
+    """Input rain maps (flag_input_rainfall_map): uneven end-stamped intervals, the first from
+    t_end[0] - dt_force > 0, full-resolution maps (each cell its own value) and coarse ones; the
+    run goes past the last map."""
+    case = random_terrain(40, 72, seed=4, walls=True)
+    case.rain_uniform = None
+    rng = np.random.default_rng(6)
+    t_end = np.array([0.5, 0.8, 1.3, 1.6])   # [0.3, 0.5), [0.5, 0.8), ...: all >= 10 s
+    for maps in (rng.uniform(0, 200, (4, 40, 72)).astype(np.float32),
+                 rng.uniform(0, 200, (4, 7, 9)).astype(np.float32)):
+        g, o = make_pair(case, precision)
+        g.set_rain_maps_end_stamped(maps, t_end, 0.2)
+        o.set_rain_maps_end_stamped(maps, t_end, 0.2)
+        for chunk in (3, 40, 100, 200):
+            g.fused_steps(chunk)
+            o.fused_steps(chunk)
+            assert_same_state(g, o, FIELDS, f"{maps.shape} after chunk {chunk}")
+            assert_same_clock(g, o)
+        assert g.diag()["t"] > 1.6
+        g.close()
+
+
+def test_input_rain_rasters_from_files(tmp_path, hp2d_lib, oracle_lib):
+    """GeoTIFF rate rasters at four times the grid's cell size, read and aligned as
+    raster_cutter.m does, on the GPU and in the oracle: the same bits."""
+    from hydropol2d_b200 import raster_rain as RR
+    from hydropol2d_b200.outputs import GeoRef, write_geotiff
+    case = random_terrain(48, 64, seed=8, walls=True)
+    case.rain_uniform = None
+    dem = GeoRef(x_ul=500000.0, y_ul=7000000.0, res=case.resolution)
+    rng = np.random.default_rng(8)
+    paths = []
+    for m in range(3):
+        p = str(tmp_path / f"rain_{m}.tif")
+        write_geotiff(p, rng.uniform(0, 150, (14, 18)), GeoRef(dem.x_ul - 7.0, dem.y_ul + 3.0, 4 * dem.res))
+        paths.append(p)
+    g, o = make_pair(case, "fp32")
+    mg = RR.set_input_rain(g, paths, [0.4, 0.8, 1.2], dem, case.z)
+    mo = RR.set_input_rain(o, paths, [0.4, 0.8, 1.2], dem, case.z)
+    assert np.array_equal(mg, mo) and mg.shape == (3, 48, 64) and np.all(mg >= 0)
+    g.fused_steps(300)
+    o.fused_steps(300)
+    assert_same_state(g, o, FIELDS)
+    assert_same_clock(g, o)
+    assert g.diag()["rain_volume"] > 0
+    g.close()
+
+
+def test_end_stamped_intervals_shorter_than_the_largest_step_are_rejected(hp2d_lib):
+    from hydropol2d_b200 import HP2DError, SurfaceFlow
+    case = small_vtilt(16, 16)
+    g = SurfaceFlow(*case.shape, case.resolution, "fp32", **case.params)
+    case.apply(g)
+    with pytest.raises(HP2DError):
+        g.set_rain_maps_end_stamped(np.zeros((2, 4, 4), np.float32), [0.5, 0.6], 0.5)   # 6 s
+    with pytest.raises(HP2DError):
+        g.set_rain_maps_end_stamped(np.zeros((2, 4, 4), np.float32), [0.5, 0.4], 0.5)   # decreasing
+    g.set_rain_maps_end_stamped(np.zeros((2, 4, 4), np.float32), [0.5, 0.5], 0.5)        # empty interval: fine
+    g.close()
