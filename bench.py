@@ -275,6 +275,16 @@ def run_surrogate(args):
 
 
 # ---------------------------------------------------------------- profiling workloads
+_WL_SHAPE = [0, 0]   # profiling workloads: cells per lane and rows per warp (0: the library's)
+
+
+def _apply_shape(g) -> None:
+    if _WL_SHAPE[0]:
+        g.set_layout(_WL_SHAPE[0])
+    if _WL_SHAPE[1]:
+        g.set_tuning(_WL_SHAPE[1])
+
+
 def workload_wet(steps: int, tb: int = 1) -> str:
     """The V-tilted catchment geometry on 2048 x 2048 cells (dx 10 m) plus a 0.5 m random field,
     5 cm of water everywhere and 60 mm/h of rain: every cell takes the full local-inertial path
@@ -290,6 +300,7 @@ def workload_wet(steps: int, tb: int = 1) -> str:
                   rain_uniform=None if tb > 1 else (np.array([0.0]), np.array([60.0])))
     g = SurfaceFlow(2048, 2048, 10.0, "fp32", **p)
     case.apply(g)
+    _apply_shape(g)
     if tb > 1:
         g.set_temporal_blocking(tb)
     g.fused_steps(steps)
@@ -307,6 +318,7 @@ def workload_dambreak(ny: int, steps: int, advance_min: float, state: str | None
     case = S.dambreak_case(ny, 8192, 5.0, seed=11)
     g = SurfaceFlow(ny, 8192, 5.0, "fp32", **case.params)
     case.apply(g)
+    _apply_shape(g)
     if state and Path(state).exists():
         z = np.load(state)
         g.set_state(z["h"].astype(np.float64) * 1000.0,
@@ -335,6 +347,7 @@ def workload_urban(n: int, steps: int, timed: int) -> str:
     case = S.urban_case(n, 2.0, seed=7, hours=2.0)
     g = SurfaceFlow(n, n, 2.0, "fp32", **case.params)
     case.apply(g)
+    _apply_shape(g)
     g.fused_steps(steps)
     ms = g.fused_steps_timed(timed)
     g.close()
@@ -395,6 +408,7 @@ def run_workload(args):
     from hydropol2d_b200 import build
     build.build()
     w = args.workload
+    _WL_SHAPE[:] = [args.layout, args.rpw]
     if w == "wet":
         line = workload_wet(args.steps, args.tb)
     elif w == "dambreak":
@@ -441,6 +455,8 @@ def main():
     ap.add_argument("--state", default=None)
     ap.add_argument("--timed", type=int, default=240)
     ap.add_argument("--tb", type=int, default=1, help="profiling workloads: steps per temporal block")
+    ap.add_argument("--layout", type=int, default=0, help="profiling workloads: cells per lane (1 or 2)")
+    ap.add_argument("--rpw", type=int, default=0, help="profiling workloads: rows per warp")
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--launches", type=int, default=64)
