@@ -57,9 +57,10 @@ RECORD_BYTES_PER_CELL = 48.0
 RECORD_BYTES_PER_CELL_GA = 64.0
 ALG_BYTES_PER_CELL_GA = 49.0   # + I read/write 8 B + soil class 1 B
 # DRAM bytes per cell of one launch in the headline window, measured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of k_fused_step, three launches) on the same
-# dam-break with 2048 rows advanced to the 60-minute mark, scaled per cell
-NCU_DRAM_BYTES_PER_CELL = None
+# (dram__bytes_read.sum + dram__bytes_write.sum of k_fused_step, three launches: 240.2 MB per
+# launch over 2048 x 8192 cells) on the same dam-break with 2048 rows advanced to the 60-minute
+# mark (28 % wet), scaled per cell; the bench grid's window is 29 % wet
+NCU_DRAM_BYTES_PER_CELL = 14.32
 
 
 def dist_env():
@@ -578,7 +579,9 @@ def main():
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sf = SurfaceFlow(ny, nx, DX, "fp32", device=local, **case.params)
+    ta = time.perf_counter()
     sf.upload_static(z_p, n_p, case.outlet_rows, case.outlet_cols)
+    tb = time.perf_counter()
     sf.set_state(h_mm, of)
     sf.set_clock(dw["t"], dw["time_step"], dw["k"])
     t1 = time.perf_counter()
@@ -589,7 +592,8 @@ def main():
     sf.download_into("depth", depth_out)
     sf.download_into("dmax", dmax_out)
     e2e_s = time.perf_counter() - t0
-    e2e_split = {"setup_s": t1 - t0, "steps_s": t2 - t1, "readback_s": e2e_s - (t2 - t0)}
+    e2e_split = {"setup_s": t1 - t0, "create_s": ta - t0, "static_s": tb - ta, "state_s": t1 - tb,
+                 "steps_s": t2 - t1, "readback_s": e2e_s - (t2 - t0)}
     n_out = sf.n_outlets
     # host-copy rates of the boundary: a state upload (depth + two flux pages, FP64) and a map
     # read-back (FP64), from and into page-locked and pageable host arrays (best of 3)

@@ -124,6 +124,9 @@ def test_noalloc_refuses_a_stream_under_capture():
     sf = SurfaceFlow(*case.shape, case.resolution, "fp32", **case.params)
     case.apply(sf)
     sf.fused_steps(10)
+    ts = sf.diag()["time_step"]
+    sf.hydrology_step(ts)
+    sf.li_step(ts)   # the unfused step materialises the face depths the call reads
     qx, qy, hf = _inputs_from_context(sf, case)
     first = _noalloc_dt(L, case, sf, qx, qy, hf)   # resolves the scratch outside any capture
     x = torch.zeros(4, device="cuda:0")
