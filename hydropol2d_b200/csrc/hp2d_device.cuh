@@ -352,26 +352,6 @@ __device__ __host__ inline double uniform_integral(const RainDesc& rd, double a,
 template <typename R>
 __device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i, int j, int ny, int nx);
 
-// One axis of map_rate's bilinear sample: the lower map index, the upper one and the weight of
-// the upper one, for grid index k of n along an axis of m map cells.
-template <typename R> struct MapAxis {
-    int k0, k1;
-    R w;
-    __device__ void make(int k, int n, int m) { make_scaled(k, R(double(m) / n), m); }
-    // scale = R(double(m) / n), computed once
-    __device__ void make_scaled(int k, R scale, int m) {
-        const R half = R(0.5);
-        R fk = (R(k) + half) * scale - half;
-        fk = fmin(fmax(fk, R(0)), R(m - 1));
-        k0 = (int)floor(fk);
-        k1 = min(k0 + 1, m - 1);
-        w = fk - R(k0);
-    }
-};
-template <typename R>
-__device__ __forceinline__ R map_rate_split(const RainDesc& rd, const float* f, const MapAxis<R>& y,
-                                            const MapAxis<R>& x);
-
 // ---------------- inflow hydrographs (flag_inflow, update_spatial_BC.m:359-395) ----------
 // Gauge g's rate [mm/h] holds from t_start[q] up to t_start[q+1] (the last for ever); a
 // step adds to every cell of the gauge the integral over the step's rain interval / 60
@@ -532,17 +512,6 @@ template <typename R> struct RainStep {
             }
         }
     }
-    // depth [m] the step adds at a cell of row `rw` and column `cw` (map_rate's arithmetic with
-    // its row and column halves computed once per row and once per lane)
-    __device__ R at(const RainDesc& rd, const MapAxis<R>& rw, const MapAxis<R>& cw) const {
-        if (!rd.n_maps) return depth;
-        if (nm == 0) return R(0);
-        R r = w[0] * map_rate_split<R>(rd, rd.maps + size_t(m[0]) * rd.my * rd.mx, rw, cw);
-#pragma unroll 1
-        for (int q = 1; q < nm; ++q)
-            r = r + w[q] * map_rate_split<R>(rd, rd.maps + size_t(m[q]) * rd.my * rd.mx, rw, cw);
-        return r;
-    }
     // depth [m] the step adds at cell (i, j)
     __device__ R at(const RainDesc& rd, int i, int j, int ny, int nx) const {
         if (!rd.n_maps) return depth;
@@ -555,16 +524,6 @@ template <typename R> struct RainStep {
     }
 };
 
-
-template <typename R>
-__device__ __forceinline__ R map_rate_split(const RainDesc& rd, const float* f, const MapAxis<R>& y,
-                                            const MapAxis<R>& x) {
-    R f00 = R(f[y.k0 * rd.mx + x.k0]), f01 = R(f[y.k0 * rd.mx + x.k1]);
-    R f10 = R(f[y.k1 * rd.mx + x.k0]), f11 = R(f[y.k1 * rd.mx + x.k1]);
-    R top = (R(1) - x.w) * f00 + x.w * f01;
-    R bot = (R(1) - x.w) * f10 + x.w * f11;
-    return (R(1) - y.w) * top + y.w * bot;
-}
 
 template <typename R>
 __device__ __forceinline__ R map_rate(const RainDesc& rd, const float* f, int i, int j, int ny, int nx) {

@@ -187,13 +187,8 @@ __device__ __forceinline__ void left_of(const R (&v)[CPL], R (&out)[CPL], int la
 #ifndef HP2D_MINB_F32_PAIR
 #define HP2D_MINB_F32_PAIR 4
 #endif
-#ifndef HP2D_MINB_F32_PAIR_HEAVY
-#define HP2D_MINB_F32_PAIR_HEAVY HP2D_MINB_F32_PAIR   // the same with infiltration or rain maps
-#endif
-template <typename R, int CPL = 1, bool HEAVY = false> struct FusedOcc {
-    static constexpr int minb = CPL == 1 ? HP2D_MINB_F32 : (HEAVY ? HP2D_MINB_F32_PAIR_HEAVY : HP2D_MINB_F32_PAIR);
-};
-template <int CPL, bool HEAVY> struct FusedOcc<double, CPL, HEAVY> { static constexpr int minb = CPL == 1 ? 3 : 2; };
+template <typename R, int CPL = 1> struct FusedOcc { static constexpr int minb = CPL == 1 ? HP2D_MINB_F32 : HP2D_MINB_F32_PAIR; };
+template <int CPL> struct FusedOcc<double, CPL> { static constexpr int minb = CPL == 1 ? 3 : 2; };
 
 // One CTA-sized work item of the fused step: warps blk*NT/32 .. of the grid described by
 // `a`.  k_fused_step runs item blockIdx.x of one grid; k_ens_step runs items of many grids
@@ -433,16 +428,6 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             fence_proxy_async_smem();   // reads of the ring by an earlier item come first
             for (int k = 0; k < kStages && k <= last_k; ++k) issue(k);
         }
-        // rain maps: the column half of each cell's bilinear sample, once per lane
-        MapAxis<R> mcol[CPL] = {};
-        R map_sy = R(0);
-        if constexpr (MAP) {
-            if (a.rain.n_maps) {
-                map_sy = R(double(a.rain.my) / ny);
-#pragma unroll
-                for (int h = 0; h < CPL; ++h) mcol[h].make(j[h], nx, a.rain.mx);
-            }
-        }
         V2 nG[CPL];
 #pragma unroll
         for (int h = 0; h < CPL; ++h) {
@@ -483,10 +468,6 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             R hT0[CPL];
             unsigned meta[CPL];
             bool all_dry = true;
-            MapAxis<R> mrow{};   // the row half of the rain maps' sample
-            if constexpr (MAP) {
-                if (a.rain.n_maps) mrow.make_scaled(r, map_sy, a.rain.my);
-            }
 #pragma unroll
             for (int h = 0; h < CPL; ++h) {
                 const V2 Gs = nG[h];
@@ -500,8 +481,7 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                     // a pending map record keeps the depth this step starts from
                     if (s_rec >= 0 && own_lane[h] && own_row) a.rec.snap[size_t(s_rec) * (size_t(ny) * nx) + c] = hh;
                     // map weights are read from shared memory where they are used
-                    R rr = RS.depth;
-                    if constexpr (MAP) rr = s_rs.at(a.rain, mrow, mcol[h]);
+                    const R rr = MAP ? s_rs.at(a.rain, r, j[h], ny, nx) : RS.depth;
                     hh = hh + rr;
                     const bool own = own_lane[h] && own_row && r >= a.own_r0 && r < a.own_r1;
                     // uniform rain volume comes from the count of finite cells at the end
@@ -1223,7 +1203,7 @@ __global__ void k_struct_prime(const FusedArgs<R> a) {
 }
 
 template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false, int SCH = 0>
-__global__ void __launch_bounds__(NT, FusedOcc<R, CPL, (INF != 0 || MAP)>::minb) k_fused_step(const FusedArgs<R> a) {
+__global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb) k_fused_step(const FusedArgs<R> a) {
     fused_item<R, NT, INF, MAP, CPL, INFL, SCH>(a, blockIdx.x);
 }
 
@@ -1284,7 +1264,7 @@ __global__ void k_ens_plan(const FusedArgs<R>* __restrict__ members, int n_membe
 }
 
 template <typename R, int NT, int INF, bool MAP, int CPL = 1, bool INFL = false, int SCH = 0>
-__global__ void __launch_bounds__(NT, FusedOcc<R, CPL, (INF != 0 || MAP)>::minb)
+__global__ void __launch_bounds__(NT, FusedOcc<R, CPL>::minb)
 k_ens_step(const FusedArgs<R>* __restrict__ members, int n_members, const unsigned* __restrict__ prefix,
            EnsQueue* q) {
     __shared__ FusedArgs<R> s_a;
