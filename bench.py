@@ -226,6 +226,34 @@ def ensemble_leg(device: int, n_members: int = 256) -> dict | None:
                       "member reaches its routing_time; max over ranks"}
 
 
+def accuracy_leg(device: int, n_members: int = 12) -> dict:
+    """The north star's peak-depth gate (<= 1 cm against FP64) measured on ensemble members at
+    256 x 256: each member run to its end time in FP32 and in FP64 (the FP64 path is bit-exact
+    with the FP64 oracle), per forcing kind the largest per-member peak-depth error and the
+    largest share of cells beyond 1 cm."""
+    from hydropol2d_b200 import SurfaceFlow, synthetic as S
+    kinds: dict = {}
+    for i in range(n_members):
+        spec = S.ensemble_member_spec(i, lo=256, hi=256)
+        c = S.ensemble_member(i, lo=256, hi=256)
+        peaks = []
+        for prec in ("fp32", "fp64"):
+            sf = SurfaceFlow(*c.shape, c.resolution, prec, device=device, **c.params)
+            c.apply(sf)
+            sf.run()
+            peaks.append(sf.download("dmax") / 1000.0)
+            sf.close()
+        err = np.abs(peaks[0] - peaks[1])
+        err = err[np.isfinite(err)]
+        k = kinds.setdefault(spec["kind"], {"members": 0, "max_peak_err_m": 0.0, "max_cells_over_1cm_pct": 0.0,
+                                            "members_within_1cm": 0})
+        k["members"] += 1
+        k["max_peak_err_m"] = max(k["max_peak_err_m"], float(err.max()))
+        k["max_cells_over_1cm_pct"] = max(k["max_cells_over_1cm_pct"], 100.0 * float(np.mean(err > 0.01)))
+        k["members_within_1cm"] += int(err.max() <= 0.01)
+    return {"gate": "peak depth within 1 cm of FP64", "size": "256 x 256", "by_kind": kinds}
+
+
 def urban_leg(device: int, n: int = 2048, peak: float | None = None) -> dict:
     """Configuration 2: urban rain-on-grid 2048 x 2048 (dx 2 m) with Green-Ampt soils and 64 x 64
     rain maps changing every 5 minutes, run over its whole 2 simulated hours (every launch timed)."""
@@ -444,6 +472,7 @@ def main():
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-member ensemble leg")
     ap.add_argument("--no-urban", action="store_true", help="skip the urban Green-Ampt leg")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 peak-depth leg")
     ap.add_argument("--window-min", type=float, default=WINDOW_MIN,
                     help="clock [min] the headline window starts at")
     ap.add_argument("--hours", type=float, default=3.0, help="simulated hours of the dam-break run")
@@ -659,6 +688,7 @@ def main():
             dist.destroy_process_group()
         return
 
+    acc = None if args.no_accuracy or world > 1 else accuracy_leg(local)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         v, sample, cores = cpu_port_gcups(15.0)
@@ -700,6 +730,7 @@ def main():
                             "pinned host arrays",
                 "host_copies": host_copies},
         "urban_c2": urban,
+        "accuracy": acc,
         "ensemble": ens,
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),
