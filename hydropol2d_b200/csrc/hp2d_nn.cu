@@ -95,18 +95,48 @@ int* err_ptr() {
     return p;
 }
 
+int sm_count() {
+    static int n[8] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 8) return 148;
+    if (!n[dev] && cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) n[dev] = 148;
+    return n[dev];
+}
+
+// a grid of more tiles than SMs runs persistently (k_gemm_bf16_pt), a smaller one one tile per CTA
+template <int BN, int KB, bool IM2COL>
+hp2d_status launch_tiles(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int kt, int per, int mtiles,
+                         int ntiles, int splits, void* C, int ldc, const float* bias, int epi, int* err, ConvGeom g,
+                         cudaStream_t st) {
+    static bool attr_set[2][8] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smem = gemm_smem_bytes<BN, KB>();
+    const long total = long(mtiles) * ntiles * splits;
+    const int sms = sm_count();
+    const bool pt = total > sms;
+    if (dev < 8 && !attr_set[pt][dev]) {
+        const cudaError_t e = pt ? cudaFuncSetAttribute(k_gemm_bf16_pt<BN, KB, IM2COL>,
+                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))
+                                 : cudaFuncSetAttribute(k_gemm_bf16<BN, KB, IM2COL>,
+                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return launched("cudaFuncSetAttribute");
+        attr_set[pt][dev] = true;
+    }
+    if (pt) {
+        k_gemm_bf16_pt<BN, KB, IM2COL><<<sms, kPtThreads, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi, err, g,
+                                                                      mtiles, ntiles, splits);
+        return launched("k_gemm_bf16_pt");
+    }
+    k_gemm_bf16<BN, KB, IM2COL><<<dim3(mtiles, ntiles, splits), 128, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias,
+                                                                               epi, err, g);
+    return launched("k_gemm_bf16");
+}
+
 template <int BN>
 hp2d_status gemm_bn(int M, int N, int K, const void* A, int lda, const void* B, int ldb, void* C, int ldc,
                     const float* bias, int epi, int split_k, cudaStream_t st) {
-    static bool attr_set[8] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const size_t smem = gemm_smem_bytes<BN>();
-    if (dev < 8 && !attr_set[dev]) {
-        if (cudaFuncSetAttribute(k_gemm_bf16<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-            return launched("cudaFuncSetAttribute");
-        attr_set[dev] = true;
-    }
     CUtensorMap ma, mb;
     if (!make_map(&ma, A, M, K, lda, kBM) || !make_map(&mb, B, N, K, ldb, BN))
         return fail("cuTensorMapEncodeTiled rejected an operand (alignment or pitch)");
@@ -115,24 +145,13 @@ hp2d_status gemm_bn(int M, int N, int K, const void* A, int lda, const void* B, 
     const int splits = (kt + per - 1) / per;   // every split gets at least one k tile
     int* err = err_ptr();
     if (!err) return fail("cannot resolve the error flag", HP2D_CUDA_ERROR);
-    dim3 grid((M + kBM - 1) / kBM, (N + BN - 1) / BN, splits);
-    k_gemm_bf16<BN><<<grid, 128, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi, err, ConvGeom{0, 0, 0});
-    return launched("k_gemm_bf16");
+    return launch_tiles<BN, kBK, false>(ma, mb, M, N, kt, per, (M + kBM - 1) / kBM, (N + BN - 1) / BN, splits, C,
+                                        ldc, bias, epi, err, ConvGeom{0, 0, 0}, st);
 }
 
 template <int BN, int KB>
 hp2d_status conv_bn(const void* x, int B, int H, int W, int Cin, const void* w, int ldw, int Co, const float* bias,
                     void* y, int ldy, int epi, cudaStream_t st) {
-    static bool attr_set[8] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const size_t smem = gemm_smem_bytes<BN, KB>();
-    if (dev < 8 && !attr_set[dev]) {
-        if (cudaFuncSetAttribute(k_gemm_bf16<BN, KB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
-            cudaSuccess)
-            return launched("cudaFuncSetAttribute");
-        attr_set[dev] = true;
-    }
     CUtensorMap ma, mb;
     if (!make_map_nhwc(&ma, x, B, H, W, Cin, KB) || !make_map(&mb, w, Co, 9 * Cin, ldw, BN, KB))
         return fail("cuTensorMapEncodeTiled rejected an operand (alignment or pitch)");
@@ -140,10 +159,8 @@ hp2d_status conv_bn(const void* x, int B, int H, int W, int Cin, const void* w, 
     if (!err) return fail("cannot resolve the error flag", HP2D_CUDA_ERROR);
     const int M = B * H * W;
     const int kt = 9 * Cin / KB;
-    dim3 grid(M / kBM, (Co + BN - 1) / BN, 1);
-    k_gemm_bf16<BN, KB, true><<<grid, 128, smem, st>>>(ma, mb, M, Co, kt, kt, y, ldy, bias, epi, err,
-                                                       ConvGeom{H, W, Cin / KB});
-    return launched("k_gemm_bf16 (implicit convolution)");
+    return launch_tiles<BN, KB, true>(ma, mb, M, Co, kt, kt, M / kBM, (Co + BN - 1) / BN, 1, y, ldy, bias, epi, err,
+                                      ConvGeom{H, W, Cin / KB}, st);
 }
 
 template <int KB>

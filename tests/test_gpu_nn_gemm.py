@@ -99,3 +99,55 @@ def test_implicit_conv_matches_im2col_gemm(B, H, W, C, Co):
     nn.check()
     ref = y_ref.clamp_min(0)
     assert bool(((yb.float() - ref).abs() <= ref.abs() * 2 ** -8 + 1e-5).all())
+
+
+@pytest.mark.parametrize("M,N,K,epi,split", [(128 * 300, 64, 192, "f32", 1), (20000, 320, 320, "f32", 1),
+                                             (40000, 96, 256, "bf16_bias_relu", 1), (128 * 80, 256, 64 * 12, "f32_atomic", 3),
+                                             (30000, 32, 128, "f32_bias", 1)])
+def test_persistent_gemm_many_tiles(M, N, K, epi, split):
+    """Grids of more tiles than SMs run the persistent kernel (two TMEM accumulators, the
+    epilogue of one tile overlapping the next): ragged M and N, every epilogue kind, split-K."""
+    from hydropol2d_b200 import nn
+    g = torch.Generator().manual_seed(M + N + K)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).cuda()
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16).cuda()
+    bias = torch.randn(N, generator=g).cuda()
+    dt = torch.bfloat16 if epi.startswith("bf16") else torch.float32
+    C = torch.zeros((M, N), dtype=dt, device="cuda") if epi == "f32_atomic" else \
+        torch.full((M, N), float("nan"), dtype=dt, device="cuda")
+    if epi == "f32_atomic":
+        nn.gemm(A, B, C, epi, split_k=split)
+    else:
+        nn.gemm(A, B, C, epi, bias=bias if "bias" in epi else None)
+    nn.check()
+    ref = _ref(A, B)
+    if "bias" in epi:
+        ref = ref + bias.cpu()
+    if epi == "bf16_bias_relu":
+        ref = ref.clamp_min(0)
+    got = C.float().cpu()
+    tol = 1e-4 * np.sqrt(K) * 4 + (ref.abs() * 2 ** -8 if dt == torch.bfloat16 else 0)
+    assert bool(((got - ref).abs() <= tol).all()), (got - ref).abs().max().item()
+
+
+@pytest.mark.parametrize("B,H,W,C,Co", [(4, 128, 128, 32, 64), (2, 64, 64, 64, 128), (1, 128, 256, 32, 32)])
+def test_persistent_implicit_conv_against_cpu(B, H, W, C, Co):
+    """Implicit convolutions of more tiles than SMs (the persistent kernel, per-tile image
+    geometry) against a CPU convolution of the same BF16 inputs."""
+    from hydropol2d_b200 import nn
+    g = torch.Generator().manual_seed(B * H + C)
+    x = torch.randn(B, H, W, C, generator=g).to(torch.bfloat16)
+    kp = -(-9 * C // 64) * 64
+    w = torch.zeros(Co, kp)
+    w[:, :9 * C] = torch.randn(Co, 9 * C, generator=g) * 0.1
+    w16 = w.to(torch.bfloat16)
+    bias = torch.randn(Co, generator=g)
+    y = torch.empty(B * H * W, Co, device="cuda")
+    nn.conv3x3(x.cuda(), w16.cuda(), Co, y, "f32_bias", bias=bias.cuda())
+    nn.check()
+    # reference: weights [Co, tap(dy, dx), C] as the library lays them out
+    wt = w16.float()[:, :9 * C].reshape(Co, 3, 3, C).permute(0, 3, 1, 2)
+    ref = torch.nn.functional.conv2d(x.float().permute(0, 3, 1, 2), wt, bias, padding=1)
+    ref = ref.permute(0, 2, 3, 1).reshape(B * H * W, Co)
+    d = (y.cpu() - ref).abs().max().item()
+    assert d <= 1e-4 * np.sqrt(9 * C) * 4, d
