@@ -1,5 +1,6 @@
 // Kernels of the learned screening network (include/hp2d_nn.h): the tcgen05 GEMM host
 // side (tensor maps, tile choice) and the memory-bound layers around it.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -104,29 +105,36 @@ int sm_count() {
     return n[dev];
 }
 
-// a grid of more tiles than SMs runs persistently (k_gemm_bf16_pt), a smaller one one tile per CTA
+// a grid of more tiles than the persistent kernel's resident CTAs runs persistently
+// (k_gemm_bf16_pt), a smaller one one tile per CTA
 template <int BN, int KB, bool IM2COL>
 hp2d_status launch_tiles(const CUtensorMap& ma, const CUtensorMap& mb, int M, int N, int kt, int per, int mtiles,
                          int ntiles, int splits, void* C, int ldc, const float* bias, int epi, int* err, ConvGeom g,
                          cudaStream_t st) {
-    static bool attr_set[2][8] = {};
+    // per device: attributes set and the persistent kernel's resident CTAs per SM (by registers and
+    // shared memory, and by TMEM: 2 x BN of its 512 columns per CTA)
+    static int per_sm[8] = {};
     int dev = 0;
     cudaGetDevice(&dev);
+    if (dev >= 8) return fail("device index beyond 7");
     const size_t smem = gemm_smem_bytes<BN, KB>();
-    const long total = long(mtiles) * ntiles * splits;
-    const int sms = sm_count();
-    const bool pt = total > sms;
-    if (dev < 8 && !attr_set[pt][dev]) {
-        const cudaError_t e = pt ? cudaFuncSetAttribute(k_gemm_bf16_pt<BN, KB, IM2COL>,
-                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))
-                                 : cudaFuncSetAttribute(k_gemm_bf16<BN, KB, IM2COL>,
-                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess) return launched("cudaFuncSetAttribute");
-        attr_set[pt][dev] = true;
+    if (!per_sm[dev]) {
+        if (cudaFuncSetAttribute(k_gemm_bf16<BN, KB, IM2COL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem)) != cudaSuccess ||
+            cudaFuncSetAttribute(k_gemm_bf16_pt<BN, KB, IM2COL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem)) != cudaSuccess)
+            return launched("cudaFuncSetAttribute");
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_gemm_bf16_pt<BN, KB, IM2COL>, kPtThreads, smem) !=
+            cudaSuccess)
+            return launched("cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        per_sm[dev] = std::max(1, std::min(occ, 512 / (2 * BN)));
     }
-    if (pt) {
-        k_gemm_bf16_pt<BN, KB, IM2COL><<<sms, kPtThreads, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi, err, g,
-                                                                      mtiles, ntiles, splits);
+    const long total = long(mtiles) * ntiles * splits;
+    const int grid_pt = sm_count() * per_sm[dev];
+    if (total > grid_pt) {
+        k_gemm_bf16_pt<BN, KB, IM2COL><<<grid_pt, kPtThreads, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi,
+                                                                          err, g, mtiles, ntiles, splits);
         return launched("k_gemm_bf16_pt");
     }
     k_gemm_bf16<BN, KB, IM2COL><<<dim3(mtiles, ntiles, splits), 128, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias,
@@ -238,7 +246,8 @@ __global__ void k_im2col_t(const uint16_t* __restrict__ x, int B, int H, int W, 
 __global__ void k_transpose(const uint16_t* __restrict__ in, int rows, int cols, int ldi, uint16_t* __restrict__ out,
                             int ldo) {
     __shared__ uint16_t tile[32][33];
-    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    // row tiles on x (up to 2^31 - 1 of them: batches of large images), column tiles on y
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     for (int i = threadIdx.y; i < 32; i += blockDim.y) {
         const int r = r0 + i, c = c0 + threadIdx.x;
         tile[i][threadIdx.x] = (r < rows && c < cols) ? in[int64_t(r) * ldi + c] : 0;
@@ -490,7 +499,8 @@ hp2d_status hp2d_nn_im2col3x3(const uint16_t* x, int32_t B, int32_t H, int32_t W
 hp2d_status hp2d_nn_transpose(const uint16_t* in, int32_t rows, int32_t cols, int32_t ldi, uint16_t* out, int32_t ldo,
                               void* stream) {
     if (!in || !out || rows <= 0 || cols <= 0 || ldi < cols || ldo < rows) return fail("transpose: bad shape");
-    dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+    if ((cols + 31) / 32 > 65535) return fail("transpose: more than 65535 column tiles");
+    dim3 grid((rows + 31) / 32, (cols + 31) / 32);
     k_transpose<<<grid, dim3(32, 8), 0, S(stream)>>>(in, rows, cols, ldi, out, ldo);
     return launched("transpose");
 }
