@@ -124,11 +124,17 @@ hp2d_status launch_tiles(const CUtensorMap& ma, const CUtensorMap& mb, int M, in
             cudaFuncSetAttribute(k_gemm_bf16_pt<BN, KB, IM2COL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)) != cudaSuccess)
             return launched("cudaFuncSetAttribute");
-        int occ = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_gemm_bf16_pt<BN, KB, IM2COL>, kPtThreads, smem) !=
-            cudaSuccess)
-            return launched("cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-        per_sm[dev] = std::max(1, std::min(occ, 512 / (2 * BN)));
+        // the largest shared-memory carveout, so that CTAs of several tiles can share an SM
+        cudaFuncSetAttribute(k_gemm_bf16_pt<BN, KB, IM2COL>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncAttributes fa{};
+        int smem_sm = 0;
+        if (cudaFuncGetAttributes(&fa, k_gemm_bf16_pt<BN, KB, IM2COL>) != cudaSuccess ||
+            cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+            return launched("cudaFuncGetAttributes");
+        const int regs = ((fa.numRegs + 7) / 8) * 8;
+        const int by_regs = 65536 / std::max(1, regs * kPtThreads);
+        const int by_smem = smem_sm / int(smem + fa.sharedSizeBytes + 1024);
+        per_sm[dev] = std::max(1, std::min({by_regs, by_smem, 512 / (2 * BN), 4}));
     }
     const long total = long(mtiles) * ntiles * splits;
     const int grid_pt = sm_count() * per_sm[dev];
