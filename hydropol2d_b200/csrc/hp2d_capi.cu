@@ -177,6 +177,34 @@ struct HostStage {
     }
 };
 
+// f(begin, end) over [0, n) on up to 16 host threads (one for small n): the per-cell host loops of
+// the set-up calls, whose first touch of fresh pages dominates on large grids
+template <typename F> void host_parallel(size_t n, F f) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (n < (size_t(1) << 20) || hw == 1) {
+        f(size_t(0), n);
+        return;
+    }
+    const size_t chunk = (n + hw - 1) / hw;
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < hw; ++t) {
+        const size_t a = t * chunk, b = std::min(n, a + chunk);
+        if (a < b) pool.emplace_back(f, a, b);
+    }
+    f(size_t(0), std::min(n, chunk));
+    for (auto& th : pool) th.join();
+}
+// allocator whose value-initialisation is a no-op, so that a large vector is filled once, in parallel
+template <typename T> struct NoInitAlloc : std::allocator<T> {
+    template <typename U> struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <typename U> NoInitAlloc(const NoInitAlloc<U>&) {}
+    template <typename U> void construct(U* p) { ::new (static_cast<void*>(p)) U; }
+    template <typename U, typename... A> void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+
 // smallest x >= 0 whose correctly rounded square root reaches R(0.01): the stagnant
 // test sqrt(s2) < 0.01 of refreshing_timestep.m:184 is then s2 < x exactly
 template <typename R> R stagnant_threshold() {
@@ -301,7 +329,7 @@ template <typename R> struct Impl : Base {
     StepScalars hs{};
     Dev<double> vol;
     // host copies needed to rebuild records
-    std::vector<uint32_t> host_meta;
+    std::vector<uint32_t, NoInitAlloc<uint32_t>> host_meta;   // meta word per cell (host mirror)
     std::vector<uint8_t> host_soil;
     std::vector<R> host_tr;
     // van Genuchten infiltration: classes, globals, water-table depth per cell, DEM copy
@@ -358,7 +386,8 @@ template <typename R> struct Impl : Base {
         sc.alloc(1);
         vol.alloc(1);
         bit_words = (nx + 31) / 32;
-        host_meta.assign(n, 255u);
+        host_meta.resize(n);
+        host_parallel(n, [&](size_t a, size_t b) { std::fill(host_meta.begin() + a, host_meta.begin() + b, 255u); });
         std::memset(&hs, 0, sizeof(hs));
         hs.t_min = c->p.min_time_step / 60.0;
         hs.time_step = c->p.min_time_step / 60.0;   // HydroPol2D_preprocessing.m:2469
@@ -393,10 +422,9 @@ template <typename R> struct Impl : Base {
     void push_sc() { HP_CK(cudaMemcpyAsync(sc.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, st())); HP_CK(cudaStreamSynchronize(st())); }
     void pull_sc() { HP_CK(cudaMemcpyAsync(&hs, sc.p, sizeof(hs), cudaMemcpyDeviceToHost, st())); HP_CK(cudaStreamSynchronize(st())); }
 
-    template <typename T> void upload(T* dst, const std::vector<T>& v) {
+    template <typename T, typename A> void upload(T* dst, const std::vector<T, A>& v) {
         if (v.empty()) return;
-        HP_CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st()));
-        HP_CK(cudaStreamSynchronize(st()));
+        h2d(dst, v.data(), v.size() * sizeof(T));
     }
     template <typename T> std::vector<T> fetch(const T* src, size_t count) {
         std::vector<T> v(count);
@@ -469,7 +497,9 @@ template <typename R> struct Impl : Base {
         std::sort(outs.begin(), outs.end(), [](auto& x, auto& y) { return x.first < y.first; });
         outs.erase(std::unique(outs.begin(), outs.end(), [](auto& x, auto& y) { return x.first == y.first; }), outs.end());
         n_out = int(outs.size());
-        for (size_t k = 0; k < n; ++k) host_meta[k] &= 255u;   // outlets and inflow cells are set anew
+        host_parallel(n, [&](size_t a, size_t b) {   // outlets and inflow cells are set anew
+            for (size_t k = a; k < b; ++k) host_meta[k] &= 255u;
+        });
         inflow.n_gauges = 0;
         inflow.n_stage = 0;
         inflow_cells_h = BcCells{};
@@ -543,7 +573,9 @@ template <typename R> struct Impl : Base {
         host_soil.assign(cls, cls + n);
         host_tr.resize(ncls);
         for (int c = 0; c < ncls; ++c) host_tr[c] = t[c].tr;
-        for (size_t k = 0; k < n; ++k) host_meta[k] = (host_meta[k] & ~255u) | cls[k];
+        host_parallel(n, [&](size_t a, size_t b) {
+            for (size_t k = a; k < b; ++k) host_meta[k] = (host_meta[k] & ~255u) | cls[k];
+        });
         write_meta();
         soil.alloc(n);
         upload(soil.p, host_soil);
@@ -600,7 +632,9 @@ template <typename R> struct Impl : Base {
             host_zwt[k] = R(std::max(sd - gwd, 0.0));
         }
         host_soil.assign(cls, cls + n);
-        for (size_t k = 0; k < n; ++k) host_meta[k] = (host_meta[k] & ~255u) | cls[k];
+        host_parallel(n, [&](size_t a, size_t b) {
+            for (size_t k = a; k < b; ++k) host_meta[k] = (host_meta[k] & ~255u) | cls[k];
+        });
         write_meta();
         soil.alloc(n);
         upload(soil.p, host_soil);
