@@ -137,7 +137,9 @@ hp2d_status launch_tiles(const CUtensorMap& ma, const CUtensorMap& mb, int M, in
         per_sm[dev] = std::max(1, std::min({by_regs, by_smem, 512 / (2 * BN), 4}));
     }
     const long total = long(mtiles) * ntiles * splits;
-    const int grid_pt = sm_count() * per_sm[dev];
+    // split-K partial sums (atomic epilogue) run one CTA per SM: measured faster in the training
+    // step's weight-gradient GEMMs than several CTAs adding into the same outputs
+    const int grid_pt = sm_count() * (epi == EPI_F32_ATOMIC ? 1 : per_sm[dev]);
     if (total > grid_pt) {
         k_gemm_bf16_pt<BN, KB, IM2COL><<<grid_pt, kPtThreads, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi,
                                                                           err, g, mtiles, ntiles, splits);
