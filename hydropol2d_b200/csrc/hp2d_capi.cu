@@ -422,9 +422,13 @@ template <typename R> struct Impl : Base {
     void push_sc() { HP_CK(cudaMemcpyAsync(sc.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, st())); HP_CK(cudaStreamSynchronize(st())); }
     void pull_sc() { HP_CK(cudaMemcpyAsync(&hs, sc.p, sizeof(hs), cudaMemcpyDeviceToHost, st())); HP_CK(cudaStreamSynchronize(st())); }
 
+    // the library's own host vectors: one copy (the driver stages pageable memory itself; the
+    // context's staging chunks are for the caller's large arrays, whose page-locked allocation
+    // would cost more than it saves here)
     template <typename T, typename A> void upload(T* dst, const std::vector<T, A>& v) {
         if (v.empty()) return;
-        h2d(dst, v.data(), v.size() * sizeof(T));
+        HP_CK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st()));
+        HP_CK(cudaStreamSynchronize(st()));
     }
     template <typename T> std::vector<T> fetch(const T* src, size_t count) {
         std::vector<T> v(count);
