@@ -82,27 +82,27 @@ hp2d_status launched(const char* what) {
     return HP2D_OK;
 }
 
+// the current device's copy of the kernels' error flag (resolved once per device)
 int* err_ptr() {
-    static int* p = nullptr;
-    static int dev = -1;
+    static std::mutex mu;
+    static int* ptr[64] = {};
     int d = 0;
-    cudaGetDevice(&d);
-    if (!p || d != dev) {
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[d]) {
         void* q = nullptr;
         if (cudaGetSymbolAddress(&q, g_nn_err_flag) != cudaSuccess) return nullptr;
-        p = static_cast<int*>(q);
-        dev = d;
+        ptr[d] = static_cast<int*>(q);
     }
-    return p;
+    return ptr[d];
 }
 
-int sm_count() {
-    static int n[8] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 8) return 148;
-    if (!n[dev] && cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) n[dev] = 148;
-    return n[dev];
+std::mutex g_launch_init_mutex;   // first-use set-up of the GEMM launches, per device
+
+int sm_count(int dev) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    return n;
 }
 
 // a grid of more tiles than the persistent kernel's resident CTAs runs persistently
@@ -113,11 +113,14 @@ hp2d_status launch_tiles(const CUtensorMap& ma, const CUtensorMap& mb, int M, in
                          cudaStream_t st) {
     // per device: attributes set and the persistent kernel's resident CTAs per SM (by registers and
     // shared memory, and by TMEM: 2 x BN of its 512 columns per CTA)
-    static int per_sm[8] = {};
+    constexpr int kDevs = 64;
+    static int per_sm[kDevs] = {};
+    static int sms[kDevs] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 8) return fail("device index beyond 7");
+    if (dev < 0 || dev >= kDevs) return fail("device index beyond 63");
     const size_t smem = gemm_smem_bytes<BN, KB>();
+    std::unique_lock<std::mutex> lock(g_launch_init_mutex);
     if (!per_sm[dev]) {
         if (cudaFuncSetAttribute(k_gemm_bf16<BN, KB, IM2COL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)) != cudaSuccess ||
@@ -135,11 +138,14 @@ hp2d_status launch_tiles(const CUtensorMap& ma, const CUtensorMap& mb, int M, in
         const int by_regs = 65536 / std::max(1, regs * kPtThreads);
         const int by_smem = smem_sm / int(smem + fa.sharedSizeBytes + 1024);
         per_sm[dev] = std::max(1, std::min({by_regs, by_smem, 512 / (2 * BN), 4}));
+        sms[dev] = sm_count(dev);
     }
+    const int ctas = per_sm[dev], n_sms = sms[dev];
+    lock.unlock();
     const long total = long(mtiles) * ntiles * splits;
     // split-K partial sums (atomic epilogue) run one CTA per SM: measured faster in the training
     // step's weight-gradient GEMMs than several CTAs adding into the same outputs
-    const int grid_pt = sm_count() * (epi == EPI_F32_ATOMIC ? 1 : per_sm[dev]);
+    const int grid_pt = n_sms * (epi == EPI_F32_ATOMIC ? 1 : ctas);
     if (total > grid_pt) {
         k_gemm_bf16_pt<BN, KB, IM2COL><<<grid_pt, kPtThreads, smem, st>>>(ma, mb, M, N, kt, per, C, ldc, bias, epi,
                                                                           err, g, mtiles, ntiles, splits);
