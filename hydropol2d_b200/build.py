@@ -22,8 +22,11 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
     "-Xcompiler", "-fPIC",
 ]
-# device code of one translation unit compiled in parallel by nvcc itself
-SPLIT = ["--split-compile=0"]
+# No --split-compile: with it the device code of a kernel depended on how nvcc partitioned the
+# translation unit among the build machine's threads, and two builds of the same source ran the
+# 2048^2 Green-Ampt + rain-map step at 15 or 19 GCUPS and the wet step at 39 or 37; whole-unit
+# builds run at 21 and 39 every time.
+SPLIT: list[str] = []
 
 
 def sources() -> list[Path]:

@@ -59,19 +59,30 @@ struct Base {
 template <typename T> struct Dev {
     T* p = nullptr;
     size_t n = 0;
+    bool owned = true;   // false: a view into another allocation
     void alloc(size_t count) {
         free();
         if (count == 0) return;
         HP_CK(cudaMalloc(&p, count * sizeof(T)));
         n = count;
+        owned = true;
+    }
+    void view(T* q, size_t count) {
+        free();
+        p = q;
+        n = count;
+        owned = false;
     }
     void free() {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
         p = nullptr;
         n = 0;
+        owned = true;
     }
     ~Dev() { free(); }
 };
+
+
 
 // Copies between a caller's host array and device memory.  Page-locked (or registered) caller
 // memory moves in one cudaMemcpyAsync at the link rate.  Pageable arrays of at least kMin bytes
@@ -286,7 +297,15 @@ template <typename R> struct Impl : Base {
     double res;
     // fused-path records
     Dev<V4> stat, st4[2];
+    Dev<unsigned char> rec_slab;   // stat, st4[0], st4[1]
     Dev<V2> gs2[2];
+    Dev<unsigned char> soil_slab;  // gs2[0], gs2[1] in one allocation
+    void alloc_soil_records() {
+        if (gs2[0].p) return;
+        const size_t stride = (n * sizeof(V2) + 255u) & ~size_t(255u);
+        soil_slab.alloc(2 * stride);
+        for (int b = 0; b < 2; ++b) gs2[b].view(reinterpret_cast<V2*>(soil_slab.p + b * stride), n);
+    }
     Dev<R> arrival;
     Dev<SoilClass<R>> classes;
     int n_classes = 0;
@@ -380,8 +399,13 @@ template <typename R> struct Impl : Base {
         nx = c->g.nx;
         n = size_t(ny) * nx;
         res = c->g.resolution;
-        stat.alloc(n);
-        for (int b = 0; b < 2; ++b) st4[b].alloc(n);
+        {
+            // the static records and both state buffers in one allocation
+            const size_t stride = (n * sizeof(V4) + 255u) & ~size_t(255u);
+            rec_slab.alloc(3 * stride);
+            stat.view(reinterpret_cast<V4*>(rec_slab.p), n);
+            for (int b = 0; b < 2; ++b) st4[b].view(reinterpret_cast<V4*>(rec_slab.p + (b + 1) * stride), n);
+        }
         arrival.alloc(n);
         sc.alloc(1);
         vol.alloc(1);
@@ -588,7 +612,7 @@ template <typename R> struct Impl : Base {
         if (gs2[0].p) g = fetch(gs2[hs.cur].p, n);
         else for (size_t k = 0; k < n; ++k) g[k] = V2{R(0), R(0)};
         for (size_t k = 0; k < n; ++k) g[k].y = soil_y(k);
-        for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
+        alloc_soil_records();
         upload(gs2[hs.cur].p, g);
         invalidate_graph();
         dirty = true;
@@ -646,7 +670,7 @@ template <typename R> struct Impl : Base {
         if (gs2[0].p) g = fetch(gs2[hs.cur].p, n);
         else for (size_t k = 0; k < n; ++k) g[k] = V2{R(0), R(0)};
         for (size_t k = 0; k < n; ++k) g[k].y = soil_y(k);
-        for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
+        alloc_soil_records();
         upload(gs2[hs.cur].p, g);
         invalidate_graph();
         dirty = true;
@@ -669,7 +693,7 @@ template <typename R> struct Impl : Base {
             HP_CK(cudaStreamSynchronize(st()));
         }
         if (Imm || gs2[0].p) {
-            for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
+            alloc_soil_records();
             std::vector<V2> g(n);
             std::vector<V2> old;
             if (!Imm) old = fetch(gs2[hs.cur].p, n);
