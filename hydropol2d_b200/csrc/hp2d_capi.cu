@@ -59,25 +59,16 @@ struct Base {
 template <typename T> struct Dev {
     T* p = nullptr;
     size_t n = 0;
-    bool owned = true;   // false: a view into another allocation
     void alloc(size_t count) {
         free();
         if (count == 0) return;
         HP_CK(cudaMalloc(&p, count * sizeof(T)));
         n = count;
-        owned = true;
-    }
-    void view(T* q, size_t count) {
-        free();
-        p = q;
-        n = count;
-        owned = false;
     }
     void free() {
-        if (p && owned) cudaFree(p);
+        if (p) cudaFree(p);
         p = nullptr;
         n = 0;
-        owned = true;
     }
     ~Dev() { free(); }
 };
@@ -297,14 +288,9 @@ template <typename R> struct Impl : Base {
     double res;
     // fused-path records
     Dev<V4> stat, st4[2];
-    Dev<unsigned char> rec_slab;   // stat, st4[0], st4[1]
     Dev<V2> gs2[2];
-    Dev<unsigned char> soil_slab;  // gs2[0], gs2[1] in one allocation
     void alloc_soil_records() {
-        if (gs2[0].p) return;
-        const size_t stride = (n * sizeof(V2) + 255u) & ~size_t(255u);
-        soil_slab.alloc(2 * stride);
-        for (int b = 0; b < 2; ++b) gs2[b].view(reinterpret_cast<V2*>(soil_slab.p + b * stride), n);
+        for (int b = 0; b < 2; ++b) if (!gs2[b].p) gs2[b].alloc(n);
     }
     Dev<R> arrival;
     Dev<SoilClass<R>> classes;
@@ -399,13 +385,8 @@ template <typename R> struct Impl : Base {
         nx = c->g.nx;
         n = size_t(ny) * nx;
         res = c->g.resolution;
-        {
-            // the static records and both state buffers in one allocation
-            const size_t stride = (n * sizeof(V4) + 255u) & ~size_t(255u);
-            rec_slab.alloc(3 * stride);
-            stat.view(reinterpret_cast<V4*>(rec_slab.p), n);
-            for (int b = 0; b < 2; ++b) st4[b].view(reinterpret_cast<V4*>(rec_slab.p + (b + 1) * stride), n);
-        }
+        stat.alloc(n);
+        for (int b = 0; b < 2; ++b) st4[b].alloc(n);
         arrival.alloc(n);
         sc.alloc(1);
         vol.alloc(1);
