@@ -51,12 +51,11 @@ constexpr int kStages = HP2D_STAGES;   // shared-memory ring depth of the row pi
 #endif
 constexpr int kRowUnroll = HP2D_ROW_UNROLL;   // row-loop unroll (register renaming of the window)
 #ifndef HP2D_FACE_ILP
-#define HP2D_FACE_ILP 0   // 1: interleaved faces in every instantiation, -1: in none
+#define HP2D_FACE_ILP 1   // 1: interleaved faces in every instantiation, 0: infiltration / rain maps only, -1: none
 #endif
 // The faces of a row as interleaved, branch-free momentum updates (face_geom + face_momentum)
-// rather than one face_flux after the other: faster on the infiltration and rain-map
-// instantiations (19.4 vs 15.7 GCUPS on the 2048^2 Green-Ampt grid with 64 x 64 rain maps),
-// slower on the plain ones (37.6 vs 39.1 wet, 92.6 vs 96.5 on the 60-minute dam-break).
+// rather than one face_flux after the other: measured faster on every workload (wet 2048^2 40.2
+// vs 39.1 GCUPS, 60-minute dam-break 98.3 vs 96.3, Green-Ampt + rain maps 21.4 vs 21.0).
 template <int INF, bool MAP> constexpr bool kFaceIlp = HP2D_FACE_ILP > 0 || (HP2D_FACE_ILP == 0 && (INF != 0 || MAP));
 
 // dynamic shared memory of k_fused_step: per warp kStages x (2 records x 32*CPL cells)
