@@ -207,6 +207,13 @@ template <typename T> struct NoInitAlloc : std::allocator<T> {
     }
 };
 
+// meta words of a grid without soil classes (255 everywhere, filled first): the outlet ordinal + 1
+// in bits 8..30 of the outlet cells (cells sorted, one entry per cell)
+__global__ void k_outlet_meta_scatter(const int32_t* __restrict__ cells, int n_out, uint32_t* __restrict__ meta) {
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n_out; o += gridDim.x * blockDim.x)
+        meta[cells[o]] = 255u | (uint32_t(o + 1) << 8);
+}
+
 // smallest x >= 0 whose correctly rounded square root reaches R(0.01): the stagnant
 // test sqrt(s2) < 0.01 of refreshing_timestep.m:184 is then s2 < x exactly
 template <typename R> R stagnant_threshold() {
@@ -534,7 +541,17 @@ template <typename R> struct Impl : Base {
             dr_.alloc(n); dm_.alloc(n);
             h2d(z_keep.p, z, n * sizeof(double));
             h2d(dr_.p, rough, n * sizeof(double));
-            upload(dm_.p, host_meta);
+            if (host_soil.empty()) {   // the same words as the host mirror, built on the device
+                Dev<int32_t> dc;
+                dc.alloc(size_t(std::max(n_out, 1)));
+                if (n_out) upload(dc.p, cells);
+                fill(dm_.p, n, 255u);
+                if (n_out) k_outlet_meta_scatter<<<(n_out + kThreads - 1) / kThreads, kThreads, 0, st()>>>(dc.p, n_out, dm_.p);
+                HP_CK(cudaGetLastError());
+                HP_CK(cudaStreamSynchronize(st()));
+            } else {
+                upload(dm_.p, host_meta);
+            }
             // the unfused entry points' copies are extracted from the records on first use
             dzx.free(); dzy.free(); n2.free();
             k_build_static<R><<<blocks_for(n), kThreads, 0, st()>>>(ny, nx, z_keep.p, dr_.p, dm_.p, stat.p, nullptr,
