@@ -1907,7 +1907,7 @@ template <typename R> struct Impl : Base {
         prologue();
         Snapshot snap;
         take(snap);
-        const int cands[] = {16, 24, 32, 40, 48, 64, 96, 128};
+        const int cands[] = {16, 24, 32, 40, 44, 48, 56, 64, 96, 128};
         if (!rpw_chosen) rows_per_warp = default_rows(cells_per_lane);
         rpw_chosen = true;
         const int keep = rows_per_warp, keep_cpl = cells_per_lane;
