@@ -57,6 +57,11 @@ constexpr int kRowUnroll = HP2D_ROW_UNROLL;   // row-loop unroll (register renam
 // rather than one face_flux after the other: measured faster on every workload (wet 2048^2 40.2
 // vs 39.1 GCUPS, 60-minute dam-break 98.3 vs 96.3, Green-Ampt + rain maps 21.4 vs 21.0).
 template <int INF, bool MAP> constexpr bool kFaceIlp = HP2D_FACE_ILP > 0 || (HP2D_FACE_ILP == 0 && (INF != 0 || MAP));
+// Phase (F) without a per-lane branch around each cell's body (stores and reductions masked
+// instead), so that the CPL cells interleave: wet 2048^2 41.6 vs 40.8 GCUPS, 60-minute dam-break
+// 115.5 vs 111.8, 128-member ensemble 44.6 vs 43.0; the Green-Ampt + rain-map instantiation ran
+// 20.3 vs 21.2 with it and keeps the branch.
+template <int INF, bool MAP> constexpr bool kFlatF = INF == 0 && !MAP;
 
 // dynamic shared memory of k_fused_step: per warp kStages x (2 records x 32*CPL cells)
 template <typename R, int CPL = 1> constexpr size_t fused_smem_bytes(int nt) {
@@ -663,68 +668,80 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
             const int rm2 = r - 2;
             const bool frow = rm2 >= r0 && rm2 < r_end;
             const bool mine = rm2 >= a.own_r0 && rm2 < a.own_r1;   // enters the reductions
-#pragma unroll
-            for (int h = 0; h < CPL; ++h) {
-                if (own_lane[h] && frow) {
-                    const size_t c2 = size_t(rm2) * nx + j[h];
-                    // a control structure's transfers join the depth after the fluxes
-                    // (Local_Inertial_Model_D4.m:318-344, :390)
-                    R h_in = hT2[h];
-                    if (INFL && (mt2[h] & kInflowBit)) {
-                        const int ss = a.inflow.cell_struct[(mt2[h] >> 8) & 0x7FFFFFu];
-                        if (ss >= 0) h_in = h_in + a.strct.extra[ss];
-                    }
-                    R hn = quiet ? h_in + R(0) : continuity(h_in, qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
-                    const R negtol = -K.tol;
-                    R hf3 = R(0);
-                    const unsigned ord = outlet_ord(mt2[h]);
-                    if (ord) {
-                        const int o = int(ord) - 1;
-                        R ho;
-                        const R qq = outlet_sink(hn, a.outlet_coef[o], a.outlet_type, K, ho);
-                        hf3 = ho;
-                        a.hf3[o] = ho;
-                        a.qo[o] = qq;
-                        if (mine) out_acc_r.add(qq * K.dt);
-                        // the next step's clamp is skipped when an outlet cell (outside the
-                        // infiltrating soils) stays negative after the next rain
-                        // (Hydrological_Model.m:45-50); only outlet cells can end negative
-                        if (mine && !(a.ga && (mt2[h] & 255u) != 255u) &&
-                            hn + (MAP ? s_rsn.at(a.rain, rm2, j[h], ny, nx) : s_rsn.depth) < R(-1e-11))
-                            s_negn = 1;   // rare: kept in shared memory, not a register
-                    }
-                    // stage hydrograph: the cell's depth becomes the gauge's stage
-                    // (update_spatial_BC.m:332-341, after the step's refreshing_timestep)
-                    if (INFL && (mt2[h] & kInflowBit)) {
-                        const int sg = a.inflow.cell_stage[(mt2[h] >> 8) & 0x7FFFFFu];
-                        if (sg >= 0) {
-                            const R sv = a.inflow.stage_now[sg];
-                            atomicAdd(&s_stage, double(sv) - double(hn));
-                            hn = sv;
+            if constexpr (kFlatF<INF, MAP>) {
+                // The cells of the lane are computed without a per-lane branch (an apron lane's values
+                // are computed and dropped: `act` masks every store and every reduction), so that the
+                // compiler can interleave the CPL cells' arithmetic; frow is the same for the warp.
+                if (frow) {
+                    R hn_[CPL], hf3_[CPL];
+    #pragma unroll
+                    for (int h = 0; h < CPL; ++h) {
+                        const bool act = own_lane[h];
+                        const size_t c2 = size_t(rm2) * nx + j[h];
+                        // a control structure's transfers join the depth after the fluxes
+                        // (Local_Inertial_Model_D4.m:318-344, :390)
+                        R h_in = hT2[h];
+                        if (INFL && act && (mt2[h] & kInflowBit)) {
+                            const int ss = a.inflow.cell_struct[(mt2[h] >> 8) & 0x7FFFFFu];
+                            if (ss >= 0) h_in = h_in + a.strct.extra[ss];
                         }
+                        R hn = quiet ? h_in + R(0) : continuity(h_in, qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
+                        const R negtol = -K.tol;
+                        R hf3 = R(0);
+                        const unsigned ord = outlet_ord(mt2[h]);
+                        if (act && ord) {
+                            const int o = int(ord) - 1;
+                            R ho;
+                            const R qq = outlet_sink(hn, a.outlet_coef[o], a.outlet_type, K, ho);
+                            hf3 = ho;
+                            a.hf3[o] = ho;
+                            a.qo[o] = qq;
+                            if (mine) out_acc_r.add(qq * K.dt);
+                            // the next step's clamp is skipped when an outlet cell (outside the
+                            // infiltrating soils) stays negative after the next rain
+                            // (Hydrological_Model.m:45-50); only outlet cells can end negative
+                            if (mine && !(a.ga && (mt2[h] & 255u) != 255u) &&
+                                hn + (MAP ? s_rsn.at(a.rain, rm2, j[h], ny, nx) : s_rsn.depth) < R(-1e-11))
+                                s_negn = 1;   // rare: kept in shared memory, not a register
+                        }
+                        // stage hydrograph: the cell's depth becomes the gauge's stage
+                        // (update_spatial_BC.m:332-341, after the step's refreshing_timestep)
+                        if (INFL && act && (mt2[h] & kInflowBit)) {
+                            const int sg = a.inflow.cell_stage[(mt2[h] >> 8) & 0x7FFFFFu];
+                            if (sg >= 0) {
+                                const R sv = a.inflow.stage_now[sg];
+                                atomicAdd(&s_stage, double(sv) - double(hn));
+                                hn = sv;
+                            }
+                        }
+                        // a non-finite depth (NaN walls included, counted against the run's start)
+                        // or one below -depth_tolerance
+                        nbad += (hn >= negtol || !mine || !act) ? 0u : 1u;
+                        if (act && dm2[h] < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
+                        hn_[h] = hn;
+                        hf3_[h] = hf3;
                     }
-                    // a non-finite depth (NaN walls included, counted against the run's start)
-                    // or one below -depth_tolerance
-                    nbad += (hn >= negtol || !mine) ? 0u : 1u;
-                    const R dm = dm2[h];
-                    if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
-                    // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
-                    R vras = R(0);   // velocity raster: largest |face velocity| (refreshing_timestep.m:109-111)
+                    // refreshing_timestep.m:61-89, :139-150, :181-238 for these cells
+                    R vras[CPL];   // velocity raster: largest |face velocity| (refreshing_timestep.m:109-111)
+    #pragma unroll
+                    for (int h = 0; h < CPL; ++h) vras[h] = R(0);
                     if (!quiet && mine) {
                         const R big = R(1e9);
-                        const R vr = qxl2[h] == R(0) ? qxl2[h] : qdiv(qxl2[h], hfx2[h] < K.tol ? big : hfx2[h]);
-                        R vu;
-                        if (vcar_ok) vu = vcar[h];
-                        else vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
-                        const R vb = qyl1[h] == R(0) ? qyl1[h] : qdiv(qyl1[h], hfy1[h] < K.tol ? big : hfy1[h]);
-                        vcar[h] = vb;
-                        if (INFL) vras = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb));
-                        const R rc = j[h] == 0 ? R(0.5) * vr : vr;
-                        const R uc = R(0.5) * (vu + vb);
-                        const R s2 = rc * rc + uc * uc;
-                        s2max = fmax(s2max, s2);
-                        if (s2 >= a.stag_s2) {
-                            const R dts = fmax(fmax(hfx2[h], hfy2[h]), hf3);
+    #pragma unroll
+                        for (int h = 0; h < CPL; ++h) {
+                            const bool act = own_lane[h];
+                            const R vr = qxl2[h] == R(0) ? qxl2[h] : qdiv(qxl2[h], hfx2[h] < K.tol ? big : hfx2[h]);
+                            R vu;
+                            if (vcar_ok) vu = vcar[h];
+                            else vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
+                            const R vb = qyl1[h] == R(0) ? qyl1[h] : qdiv(qyl1[h], hfy1[h] < K.tol ? big : hfy1[h]);
+                            vcar[h] = vb;
+                            if (INFL) vras[h] = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb));
+                            const R rc = j[h] == 0 ? R(0.5) * vr : vr;
+                            const R uc = R(0.5) * (vu + vb);
+                            const R s2 = rc * rc + uc * uc;
+                            if (act) s2max = fmax(s2max, s2);
+                            const R dts = fmax(fmax(hfx2[h], hfy2[h]), hf3_[h]);
                             R cval;
                             if (a.adaptive == 1) {
                                 cval = K.g * fmax(dts, R(0));
@@ -732,25 +749,126 @@ __device__ __forceinline__ bool fused_item(const FusedArgs<R>& a, const unsigned
                                 const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
                                 cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
                             }
-                            cmaxv = fmax(cmaxv, cval);
+                            if (act && s2 >= a.stag_s2) cmaxv = fmax(cmaxv, cval);
                         }
                     }
-                    V4 o4;
-                    o4.x = hn;
-                    o4.y = qxl2[h];
-                    o4.z = qyl2[h];
-                    o4.w = hn > dm ? hn : dm;   // save_output_maps.m:598, max(d_t, dmax)
-                    sout[c2] = o4;
-                    // running maxima of the velocity raster and of depth x velocity
-                    // (save_output_maps.m:588-604, snisb_velocity_hazard_snapshot :832-848)
-                    if (INFL && a.vmax) {
-                        const R vo = a.vmax[c2];
-                        a.vmax[c2] = vras > vo ? vras : vo;
-                        const R hd = fmax(hn, R(0));
-                        R hz = hd * vras;
-                        if (hd < R(0.01) || !isfinite(hz)) hz = R(0);
-                        const R ho = a.hzmax[c2];
-                        a.hzmax[c2] = isnan(hn) ? hn : (hz > ho ? hz : ho);
+    #pragma unroll
+                    for (int h = 0; h < CPL; ++h) {
+                        if (!own_lane[h]) continue;
+                        const size_t c2 = size_t(rm2) * nx + j[h];
+                        const R hn = hn_[h];
+                        const R dm = dm2[h];
+                        V4 o4;
+                        o4.x = hn;
+                        o4.y = qxl2[h];
+                        o4.z = qyl2[h];
+                        o4.w = hn > dm ? hn : dm;   // save_output_maps.m:598, max(d_t, dmax)
+                        sout[c2] = o4;
+                        // running maxima of the velocity raster and of depth x velocity
+                        // (save_output_maps.m:588-604, snisb_velocity_hazard_snapshot :832-848)
+                        if (INFL && a.vmax) {
+                            const R vo = a.vmax[c2];
+                            a.vmax[c2] = vras[h] > vo ? vras[h] : vo;
+                            const R hd = fmax(hn, R(0));
+                            R hz = hd * vras[h];
+                            if (hd < R(0.01) || !isfinite(hz)) hz = R(0);
+                            const R ho = a.hzmax[c2];
+                            a.hzmax[c2] = isnan(hn) ? hn : (hz > ho ? hz : ho);
+                        }
+                    }
+                }
+            } else {
+            // the infiltration and rain-map instantiations keep the per-lane branch around the cell
+            // body (fewer live registers: measured faster there)
+    #pragma unroll
+                for (int h = 0; h < CPL; ++h) {
+                    if (own_lane[h] && frow) {
+                        const size_t c2 = size_t(rm2) * nx + j[h];
+                        // a control structure's transfers join the depth after the fluxes
+                        // (Local_Inertial_Model_D4.m:318-344, :390)
+                        R h_in = hT2[h];
+                        if (INFL && (mt2[h] & kInflowBit)) {
+                            const int ss = a.inflow.cell_struct[(mt2[h] >> 8) & 0x7FFFFFu];
+                            if (ss >= 0) h_in = h_in + a.strct.extra[ss];
+                        }
+                        R hn = quiet ? h_in + R(0) : continuity(h_in, qxl2_left[h], qxl2[h], qyl2[h], qyl1[h], K);
+                        const R negtol = -K.tol;
+                        R hf3 = R(0);
+                        const unsigned ord = outlet_ord(mt2[h]);
+                        if (ord) {
+                            const int o = int(ord) - 1;
+                            R ho;
+                            const R qq = outlet_sink(hn, a.outlet_coef[o], a.outlet_type, K, ho);
+                            hf3 = ho;
+                            a.hf3[o] = ho;
+                            a.qo[o] = qq;
+                            if (mine) out_acc_r.add(qq * K.dt);
+                            // the next step's clamp is skipped when an outlet cell (outside the
+                            // infiltrating soils) stays negative after the next rain
+                            // (Hydrological_Model.m:45-50); only outlet cells can end negative
+                            if (mine && !(a.ga && (mt2[h] & 255u) != 255u) &&
+                                hn + (MAP ? s_rsn.at(a.rain, rm2, j[h], ny, nx) : s_rsn.depth) < R(-1e-11))
+                                s_negn = 1;   // rare: kept in shared memory, not a register
+                        }
+                        // stage hydrograph: the cell's depth becomes the gauge's stage
+                        // (update_spatial_BC.m:332-341, after the step's refreshing_timestep)
+                        if (INFL && (mt2[h] & kInflowBit)) {
+                            const int sg = a.inflow.cell_stage[(mt2[h] >> 8) & 0x7FFFFFu];
+                            if (sg >= 0) {
+                                const R sv = a.inflow.stage_now[sg];
+                                atomicAdd(&s_stage, double(sv) - double(hn));
+                                hn = sv;
+                            }
+                        }
+                        // a non-finite depth (NaN walls included, counted against the run's start)
+                        // or one below -depth_tolerance
+                        nbad += (hn >= negtol || !mine) ? 0u : 1u;
+                        const R dm = dm2[h];
+                        if (dm < K.thr && hn >= K.thr) a.arrival[c2] = t_arr;
+                        // refreshing_timestep.m:61-89, :139-150, :181-238 for this cell
+                        R vras = R(0);   // velocity raster: largest |face velocity| (refreshing_timestep.m:109-111)
+                        if (!quiet && mine) {
+                            const R big = R(1e9);
+                            const R vr = qxl2[h] == R(0) ? qxl2[h] : qdiv(qxl2[h], hfx2[h] < K.tol ? big : hfx2[h]);
+                            R vu;
+                            if (vcar_ok) vu = vcar[h];
+                            else vu = qyl2[h] == R(0) ? qyl2[h] : qdiv(qyl2[h], hfy2[h] < K.tol ? big : hfy2[h]);
+                            const R vb = qyl1[h] == R(0) ? qyl1[h] : qdiv(qyl1[h], hfy1[h] < K.tol ? big : hfy1[h]);
+                            vcar[h] = vb;
+                            if (INFL) vras = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb));
+                            const R rc = j[h] == 0 ? R(0.5) * vr : vr;
+                            const R uc = R(0.5) * (vu + vb);
+                            const R s2 = rc * rc + uc * uc;
+                            s2max = fmax(s2max, s2);
+                            if (s2 >= a.stag_s2) {
+                                const R dts = fmax(fmax(hfx2[h], hfy2[h]), hf3);
+                                R cval;
+                                if (a.adaptive == 1) {
+                                    cval = K.g * fmax(dts, R(0));
+                                } else {
+                                    const R wc = fmax(sqrt(K.g * fmax(dts, R(0))), R(1e-10));
+                                    cval = fmax(fmax(fabs(vr), fabs(vu)), fabs(vb)) + wc;
+                                }
+                                cmaxv = fmax(cmaxv, cval);
+                            }
+                        }
+                        V4 o4;
+                        o4.x = hn;
+                        o4.y = qxl2[h];
+                        o4.z = qyl2[h];
+                        o4.w = hn > dm ? hn : dm;   // save_output_maps.m:598, max(d_t, dmax)
+                        sout[c2] = o4;
+                        // running maxima of the velocity raster and of depth x velocity
+                        // (save_output_maps.m:588-604, snisb_velocity_hazard_snapshot :832-848)
+                        if (INFL && a.vmax) {
+                            const R vo = a.vmax[c2];
+                            a.vmax[c2] = vras > vo ? vras : vo;
+                            const R hd = fmax(hn, R(0));
+                            R hz = hd * vras;
+                            if (hd < R(0.01) || !isfinite(hz)) hz = R(0);
+                            const R ho = a.hzmax[c2];
+                            a.hzmax[c2] = isnan(hn) ? hn : (hz > ho ? hz : ho);
+                        }
                     }
                 }
             }
